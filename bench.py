@@ -1,0 +1,346 @@
+"""Benchmark of the elastic staggered-grid time loop on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--config config2|config1|config3]
+
+One bench step is one complete forward modelling run of the configuration:
+zero the state, nt time steps (velocity + stress passes, source injection,
+receiver sampling), inputs already resident in HBM.  Default workload
+(config2): 3D homogeneous SSG-CPML 200^3, dx=10 m, dt=1 ms, 1000 time steps,
+20-cell CPML, double-couple (30/60/90) 15 Hz Ricker2 source, 50x50 receivers,
+fp32.  The state (~0.9 GB) is larger than L2, so no L2 flush is needed.
+
+Metric: Gcell-updates/s = cells * time steps / device time (max over ranks,
+whole job).  Multi-GPU runs are independent replicas (one shot per GPU):
+the forward loop of one model has no data-path exchange.
+
+`e2e` is the same metric through the public drop-in API with host buffers:
+each step copies the model (vp, vs, rho) from pinned host memory into the
+solver, runs the nt steps and reads the seismogram back into pinned memory.
+
+`--impl reference` times the reference's scheme on the host CPU: the
+SeisWave_Taichi Taichi package is not installable here, so its CPU arm is the
+C++/OpenMP restatement of the same kernels (oracle/), run on every host core
+on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+FALLBACK_HBM_GBS = 6650.0
+
+# DRAM bytes per time step (velocity + stress pass) from ncu, scaled to the
+# full workload; summaries under profiles/.  None until captured.
+NCU_TRAFFIC_PER_STEP = {}
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks/throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"),
+                               parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def build_solver(cfg, torch):
+    from seiswave_taichi_b200.Elastic3D_SSG_Tensor import ElasticWAVE
+    w = ElasticWAVE(cfg["vs"], cfg["vp"], cfg["rho"], cfg["dx"], cfg["dy"], cfg["dz"], cfg["dt"],
+                    cfg["isx"], cfg["isy"], cfg["isz"], cfg["rsx"], cfg["rsy"], cfg["rsz"], cfg["MT"],
+                    cfg["src_scale"], cfg["nt"], cfg["accuracy"], cfg["freq"], torch.float32)
+    w.SetADEPML3D(cfg["surface"], cfg["pml"])
+    return w
+
+
+def build_solver2d(cfg, torch):
+    from seiswave_taichi_b200.Elastic2D_CPML import ElasticWAVE
+    w = ElasticWAVE(cfg["vs"], cfg["vp"], cfg["rho"], cfg["dx"], cfg["dz"], cfg["dt"], cfg["isx"],
+                    cfg["isz"], cfg["rsx"], cfg["rsz"], cfg["nt"], cfg["accuracy"], cfg["freq"],
+                    torch.float32)
+    w.SetADEPML2D(cfg["surface"], cfg["pml"])
+    return w
+
+
+def algorithmic_bytes(cfg, npml=20):
+    """Fused minimum bytes per time step: every wavefield read and written
+    once, the material read once, and each CPML memory variable read and
+    written once on its slabs: 3D 84*N + 48*(S_x+S_y+S_z), 2D 52*N + 32*(S_x+S_z),
+    S_d = 2*npml*(product of the other two extents)."""
+    shape = cfg["shape"]
+    ncell = int(np.prod(shape))
+    if len(shape) == 3:
+        nx, ny, nz = shape
+        S = 2 * npml * (ny * nz + nx * nz + nx * ny)
+        return 84 * ncell + 48 * S
+    nx, nz = shape
+    S = 2 * npml * (nz + nx)
+    return 52 * ncell + 32 * S
+
+
+def cpu_baseline(cfg, min_seconds=10.0, max_steps=60):
+    """The oracle on all host cores, on a bounded sample (whole grid, the
+    first few time steps) of the same workload."""
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    O.set_threads(threads)
+    if len(cfg["shape"]) == 3:
+        o = O.Oracle3D("TENSOR", cfg["vs"], cfg["vp"], cfg["rho"], cfg["dx"], cfg["dy"], cfg["dz"], cfg["dt"],
+                       cfg["isx"], cfg["isy"], cfg["isz"], cfg["rsx"], cfg["rsy"], cfg["rsz"], cfg["nt"],
+                       cfg["accuracy"], cfg["freq"], cfg["surface"], cfg["pml"], MT=cfg["MT"],
+                       src_scale=cfg["src_scale"])
+        step = lambda it, n: o.run(it, n)
+    else:
+        o = O.Oracle2D(cfg["vs"], cfg["vp"], cfg["rho"], cfg["dx"], cfg["dz"], cfg["dt"], cfg["isx"], cfg["isz"],
+                       int(cfg["rsx"].reshape(-1)[0]), int(cfg["rsz"].reshape(-1)[0]), cfg["nt"],
+                       cfg["accuracy"], cfg["freq"], cfg["surface"], cfg["pml"])
+        step = lambda it, n: o.run("VS", it, n)
+    step(0, 1)  # first touch of the state pages
+    ncell = int(np.prod(cfg["shape"]))
+    t0 = time.perf_counter()
+    done = 0
+    while done < max_steps and (time.perf_counter() - t0) < min_seconds:
+        step(1 + done, 1)
+        done += 1
+    el = time.perf_counter() - t0
+    return {"value": ncell * done / el / 1e9, "unit": "Gcell-updates/s", "cores": threads, "kind": "port",
+            "sample": f"time steps 1..{done} of the full {'x'.join(map(str, cfg['shape']))} grid "
+                      f"({el:.1f} s, C++/OpenMP oracle restating the reference kernels)"}
+
+
+def get_config(name):
+    from seiswave_taichi_b200 import synthetic as S
+    if name == "config2":
+        return S.config2()
+    if name == "config1":
+        return S.config1()
+    if name == "config3":
+        return S.config3()
+    raise SystemExit(f"unknown config {name}")
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    cfg = get_config(args.config)
+    samples = []
+    for s in range(args.warmup + args.steps):
+        b = cpu_baseline(cfg, min_seconds=4.0, max_steps=20)
+        if s >= args.warmup:
+            samples.append(b)
+    v = float(np.mean([b["value"] for b in samples]))
+    cb = dict(samples[-1])
+    cb["value"] = v
+    ncell = int(np.prod(cfg["shape"]))
+    line = {
+        "impl": "reference", "metric": "Gcell-updates/s", "value": v, "unit": "Gcell-updates/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ncell * cfg["nt"] / (v * 1e9) * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": cfg["name"], "grid": list(cfg["shape"]), "time_steps": cfg["nt"],
+                   "accuracy": cfg["accuracy"]},
+        "cpu_baseline": cb,
+        "e2e": {"value": v, "unit": "Gcell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="config2", choices=["config2", "config1", "config3"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args(argv)
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    cfg = get_config(args.config)
+    three_d = len(cfg["shape"]) == 3
+    w = build_solver(cfg, torch) if three_d else build_solver2d(cfg, torch)
+    nt = cfg["nt"]
+    ncell = int(np.prod(cfg["shape"]))
+    stream = torch.cuda.current_stream()
+
+    def one_run():
+        w.reset()
+        w.run(nt)
+
+    for _ in range(args.warmup):
+        one_run()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            one_run()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms_total = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms_total], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total = float(t.item())
+    ms_step = ms_total / args.steps
+    value = world * ncell * nt * args.steps / (ms_total * 1e-3) / 1e9
+
+    # roofline of one time step (velocity + stress pass)
+    peak, peak_kind = peaks()
+    alg = algorithmic_bytes(cfg)
+    ms_per_tstep = ms_step / nt
+    achieved = alg / (ms_per_tstep * 1e-3) / 1e9
+    traffic = NCU_TRAFFIC_PER_STEP.get(cfg["name"])
+
+    # end to end through the public API with host buffers
+    pin = {k: torch.from_numpy(np.ascontiguousarray(cfg[k])).pin_memory() for k in ("vp", "vs", "rho")}
+    out = torch.empty(tuple(w.data.shape), dtype=w.data.dtype).pin_memory()
+    h2d = sum(t.numel() * t.element_size() for t in pin.values())
+    d2h = out.numel() * out.element_size()
+
+    def e2e_run():
+        w.set_model(pin["vp"], pin["vs"], pin["rho"])
+        w.reset()
+        w.run(nt)
+        out.copy_(w.data, non_blocking=True)
+
+    for _ in range(2):
+        e2e_run()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_run()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * ncell * nt * args.steps / (e2e_ms * 1e-3) / 1e9
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(cfg)
+
+    launches_per_run = 2 * nt + (1 if three_d else 0)
+    if rank == 0:
+        line = {
+            "metric": "Gcell-updates/s", "value": value, "unit": "Gcell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": cfg["name"], "grid": list(cfg["shape"]), "time_steps": nt,
+                       "accuracy": cfg["accuracy"], "parallelism": f"replicas{world}",
+                       "l2": "state larger than L2 (no flush needed)" if three_d else
+                             "state fits in L2 (2D 400^2); %HBM not meaningful"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "kernel": "k3_velocity + k3_stress (one time step)" if three_d else
+                                   "k2_velocity + k2_stress (one time step)",
+                         "algorithmic_bytes_per_launch": alg, "ms_per_launch": ms_per_tstep,
+                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                                        else "fallback 6650 GB/s"},
+            "e2e": {"value": e2e_value, "unit": "Gcell-updates/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches_per_run * args.steps,
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,197 @@
+/*
+ * seiswave.h -- C ABI of libseiswave.so, the B200 (sm_100a) elastic
+ * staggered-grid finite-difference time loop.
+ *
+ * The reference (SeisWave_Taichi) is pure Python/Taichi and has no FFI of its
+ * own; each entry point below replaces one Taichi kernel or host routine of
+ * the reference's ElasticWAVE classes (paths relative to the reference
+ * project), and the Python package seiswave_taichi_b200 binds them through
+ * ctypes with the reference's class names and signatures.
+ *
+ * Ownership: every array is allocated by the caller (PyTorch in the Python
+ * package) and borrowed by the plan; nothing here frees caller memory.  A plan
+ * owns only its small internal scratch (step counters, CUDA graphs), released
+ * by sw_plan_destroy.  Device arrays are C-contiguous, last index fastest:
+ * (nx, nz) in 2D, (nx, ny, nz) in 3D.
+ *
+ * Errors: every call returns SW_OK (0) or a negative SW_ERR_* code; the
+ * message of the last failure on the calling thread is sw_last_error().
+ * Nothing calls exit() or traps on the device.
+ *
+ * Threading: work is enqueued on the caller's stream (a cudaStream_t passed as
+ * void*, NULL = legacy default stream).  A plan is not thread-safe; use one plan
+ * per stream.  No call blocks the host except sw_check_finite.
+ */
+#ifndef SEISWAVE_H
+#define SEISWAVE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define SW_API __attribute__((visibility("default")))
+#else
+#define SW_API
+#endif
+
+#define SW_ABI_VERSION 1
+#define SW_MAX_ORDER 8 /* largest half-stencil length N (accuracy) */
+
+/* status codes */
+#define SW_OK 0
+#define SW_ERR_ARG (-1)          /* invalid descriptor or argument */
+#define SW_ERR_CUDA (-2)         /* a CUDA runtime call failed */
+#define SW_ERR_NONFINITE (-3)    /* a wavefield holds NaN or Inf */
+#define SW_ERR_UNSUPPORTED (-4)  /* valid request this build does not implement */
+#define SW_ERR_TIMEOUT (-5)      /* a bounded device wait gave up */
+
+/* element types */
+#define SW_F32 0
+#define SW_F64 1
+
+/* 2D schemes: Elastic2D_CPML.py update_SSG_VS :128, update_SSG_SV :203, update_RSG :277 */
+#define SW2D_SSG_VS 0
+#define SW2D_SSG_SV 1
+#define SW2D_RSG 2
+
+/* 3D schemes: Elastic3D_SSG_CPML.py update_SSG :144 (point force),
+ * Elastic3D_SSG_Tensor.py update_SSG :166 (moment tensor),
+ * Elastic3D_SSG_SPML.py update_SSG_SPML :160 (split-field PML) */
+#define SW3D_CPML_FORCE 0
+#define SW3D_CPML_TENSOR 1
+#define SW3D_SPML 2
+
+/* source kinds */
+#define SW_SRC_NONE 0
+#define SW_SRC_FORCE 1  /* v[src] += dt*w/rho[src] after the velocity phase */
+#define SW_SRC_MOMENT 2 /* sigma_ab[src] += w*(-M_ab) before the velocity phase */
+#define SW_SRC_RSG4 3   /* 2D RSG: vz[isx+a,isz+b] += dt*w/(8 rho), a,b in {-1,0} */
+
+/* One axis of the absorbing boundary, built on the host exactly as the
+ * reference's SetADEPML2D/SetADEPML3D (Elastic2D_CPML.py:392-528,
+ * Elastic3D_SSG_Tensor.py:361-568) builds it. */
+typedef struct sw_pml_axis {
+  int32_t lo;          /* memory-variable slab: indices [0, lo) ...            */
+  int32_t hi;          /* ... and [n-hi, n) of this axis; elsewhere the CPML
+                          correction is the identity and is not stored        */
+  const void* coef;    /* 6*n values (field type): b, a, k at integer points,
+                          then b_half, a_half, k_half                          */
+  const void* damp;    /* 2*n values: d, d_half (split PML only, else NULL)    */
+  const uint8_t* flag; /* n bytes: bit0 = integer point lies inside the PML
+                          predicate (x<=xmin_pml or x>=xmax_pml), bit1 = half  */
+} sw_pml_axis;
+
+/* Receivers: data[it*nrec + r] = field[rec_index[r]] after step it. */
+typedef struct sw_receivers {
+  int32_t nrec;
+  int32_t field;             /* index into the descriptor's field[] array      */
+  const int64_t* index;      /* device, nrec linear cell indices               */
+  void* data;                /* device, (nt_max, nrec) traces (reference .data) */
+  int32_t dtype;             /* element type of data: SW_F32 or SW_F64         */
+} sw_receivers;
+
+typedef struct sw_source {
+  int32_t kind;              /* SW_SRC_*                                       */
+  int32_t i, j, k;           /* cell (k unused in 2D)                          */
+  const void* wavelet;       /* device, nt_max values (field type)             */
+  double mt[6];              /* moment tensor: xx yy zz xy xz yz (2D: xx zz xz in 0,2,4) */
+} sw_source;
+
+/* 2D: fields are vx vz sxx szz sxz; memory variables slab-compact:
+ * mem[0] = x direction, (4, lo+hi, nz): sxx_dx sxz_dx dvx_dx dvz_dx;
+ * mem[1] = z direction, (4, nx, lo+hi): sxz_dz szz_dz dvz_dz dvx_dz.
+ * The same arrays serve the VS, SV and RSG schemes, as in the reference. */
+typedef struct sw2d_desc {
+  int32_t scheme, dtype, nx, nz, order;
+  int32_t nt_max;
+  double dx, dz, dt;
+  double coef[SW_MAX_ORDER];
+  void* field[5];            /* vx vz sxx szz sxz */
+  const void* rho;
+  const void* lam;
+  const void* mu;
+  sw_pml_axis pml[2];        /* x, z */
+  void* mem[2];
+  sw_source src;
+  sw_receivers rec;
+} sw2d_desc;
+
+/* 3D: fields are vx vy vz sxx syy szz sxy sxz syz.
+ * CPML memory variables slab-compact: mem[0] = x, (6, lo+hi, ny, nz):
+ *   sxx_dx sxy_dx sxz_dx dvx_dx dvy_dx dvz_dx;
+ * mem[1] = y, (6, nx, lo+hi, nz): sxy_dy syy_dy syz_dy dvy_dy dvx_dy dvz_dy;
+ * mem[2] = z, (6, nx, ny, lo+hi): sxz_dz syz_dz szz_dz dvz_dz dvx_dz dvy_dz.
+ * Split PML: split = (24, nx, ny, nz) split fields. */
+typedef struct sw3d_desc {
+  int32_t scheme, dtype, nx, ny, nz, order;
+  int32_t nt_max;
+  double dx, dy, dz, dt;
+  double coef[SW_MAX_ORDER];
+  void* field[9];            /* vx vy vz sxx syy szz sxy sxz syz */
+  const void* rho;
+  const void* lam;
+  const void* mu;
+  sw_pml_axis pml[3];        /* x, y, z */
+  void* mem[3];
+  void* split;
+  sw_source src;
+  sw_receivers rec;
+} sw3d_desc;
+
+typedef struct sw_plan sw_plan;
+
+/* Version of this ABI (SW_ABI_VERSION). */
+SW_API int sw_version(void);
+
+/* Message of the last failed call on this thread ("" if none). */
+SW_API const char* sw_last_error(void);
+
+/* Validate a 2D descriptor and build a plan.  Replaces the state set-up of
+ * Elastic2D_CPML.ElasticWAVE.__init__ (Elastic2D_CPML.py:11-91) and the
+ * profile upload of SetADEPML2D (:392-528); the caller keeps the arrays. */
+SW_API int sw2d_plan_create(const sw2d_desc* desc, sw_plan** plan);
+
+/* Same for 3D: Elastic3D_SSG_CPML.py:9-122, Elastic3D_SSG_Tensor.py:9-130,
+ * Elastic3D_SSG_SPML.py:8-138 and their SetADEPML3D. */
+SW_API int sw3d_plan_create(const sw3d_desc* desc, sw_plan** plan);
+
+/* Override the number of x planes one CTA streams in the 3D CPML passes
+ * (the autotuner's knob; the plan picks a default from the grid and SM count). */
+SW_API int sw_plan_set_tile(sw_plan* plan, int32_t x_chunk);
+
+/* sizeof of the ABI structs as this library was compiled: which = 0
+ * sw_pml_axis, 1 sw_receivers, 2 sw_source, 3 sw2d_desc, 4 sw3d_desc; -1 else.
+ * Lets a binding check its struct layout without touching a GPU. */
+SW_API int sw_abi_sizeof(int32_t which);
+
+/* Release the plan's own scratch and graphs. */
+SW_API int sw_plan_destroy(sw_plan* plan);
+
+/* One time step `it`: the reference's update_SSG_VS(it) / update_SSG_SV(it) /
+ * update_SSG(it) / update_SSG_SPML(it) (Elastic2D_CPML.py:128,203;
+ * Elastic3D_SSG_CPML.py:144; Elastic3D_SSG_Tensor.py:166;
+ * Elastic3D_SSG_SPML.py:160). */
+SW_API int sw_step(sw_plan* plan, int32_t it, void* stream);
+
+/* One time step with the source amplitude given by the caller instead of the
+ * plan's wavelet: update_RSG(it, source) (Elastic2D_CPML.py:277). */
+SW_API int sw_step_amp(sw_plan* plan, int32_t it, double amplitude, void* stream);
+
+/* Steps it0 .. it0+nsteps-1 back to back, the reference driver loop
+ * `for i in range(nt): obj.update_*(i)` (e.g. test2d_homegenous.py:55-56),
+ * replayed from a cached CUDA graph when use_graph != 0. */
+SW_API int sw_run(sw_plan* plan, int32_t it0, int32_t nsteps, int32_t use_graph, void* stream);
+
+/* Scan every wavefield for NaN/Inf; blocks on the stream.  *nonfinite is set
+ * to the number of non-finite values found (0 when the state is finite);
+ * returns SW_ERR_NONFINITE when it is non-zero. */
+SW_API int sw_check_finite(sw_plan* plan, void* stream, int64_t* nonfinite);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SEISWAVE_H */

@@ -1,0 +1,280 @@
+"""NumPy twin of the oracle (test infrastructure only).
+
+A second, independent transcription of two reference kernels, written with
+whole-array slices instead of loops:
+  * Elastic2D_CPML.update_SSG_VS   (src/Elastic2D_CPML.py:128-200)
+  * Elastic3D_SSG_Tensor.update_SSG (src/Elastic3D_SSG_Tensor.py:166-345)
+Every operation is an elementwise IEEE operation in the array dtype, in the
+reference's order, so on the same inputs it must agree bit for bit with the
+C++ oracle (sw_oracle.cpp).  Used on tiny grids only.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def _pred(vals, lo, hi):
+    return (vals <= lo) | (vals >= hi)
+
+
+class Twin2D:
+    def __init__(self, o):
+        """Build from an oracle.Oracle2D (shares its inputs, owns its state)."""
+        T = o.T
+        self.T = T
+        self.N = o.N
+        d = o.desc
+        self.dx, self.dz, self.dt = T(d.dx), T(d.dz), T(d.dt)
+        self.c = np.array([d.c[m] for m in range(o.N)], dtype=np.float64).astype(T)
+        self.rho, self.lam, self.mu = o.rho.copy(), o.lam.copy(), o.mu.copy()
+        z = lambda: np.zeros_like(o.vx)
+        self.vx, self.vz, self.sxx, self.szz, self.sxz = z(), z(), z(), z(), z()
+        self.mem = {k: z() for k in ("sxx_dx", "sxz_dx", "sxz_dz", "szz_dz", "dvx_dx", "dvx_dz",
+                                     "dvz_dx", "dvz_dz")}
+        (self.X, (self.xlo, self.xhi)), (self.Z, (self.zlo, self.zhi)) = o.axes
+        self.isx, self.isz, self.rsx, self.rsz = d.isx, d.isz, d.rsx, d.rsz
+        self.data = np.zeros_like(o.data)
+
+    def _d(self, f, I, J, axis, fwd):
+        T, N, c = self.T, self.N, self.c
+        v = np.zeros((I.stop - I.start, J.stop - J.start), T)
+        for m in range(N):
+            a, b = (m + 1, -m) if fwd else (m, -m - 1)
+            if axis == 0:
+                hi = f[I.start + a:I.stop + a, J]
+                lo = f[I.start + b:I.stop + b, J]
+            else:
+                hi = f[I, J.start + a:J.stop + a]
+                lo = f[I, J.start + b:J.stop + b]
+            v = v + c[m] * (hi - lo)
+        return v
+
+    def _mask(self, I, J, xhalf, zhalf):
+        T = self.T
+        i = np.arange(I.start, I.stop)
+        j = np.arange(J.start, J.stop)
+        x = (i - self.N).astype(T) * self.dx + (self.dx / T(2) if xhalf else T(0))
+        z = (j - self.N).astype(T) * self.dz + (self.dz / T(2) if zhalf else T(0))
+        return _pred(x, T(self.xlo), T(self.xhi))[:, None] | _pred(z, T(self.zlo), T(self.zhi))[None, :]
+
+    def _pml(self, name, d, bx, ax, kx, mask, I, J, along_x):
+        m = self.mem[name]
+        old = m[I, J]
+        if along_x:
+            b, a, k = bx[I][:, None], ax[I][:, None], kx[I][:, None]
+        else:
+            b, a, k = bx[J][None, :], ax[J][None, :], kx[J][None, :]
+        new = b * old + a * d
+        m[I, J] = np.where(mask, new, old)
+        return np.where(mask, d / k + new, d)
+
+    def step(self, it, w):
+        T, N, dt = self.T, self.N, self.dt
+        nx, nz = self.vx.shape
+        X, Z = self.X, self.Z
+        # vx
+        I, J = slice(N + 1, nx - N), slice(N + 1, nz - N)
+        dsxxdx = self._d(self.sxx, I, J, 0, False) / self.dx
+        dsxzdz = self._d(self.sxz, I, J, 1, False) / self.dz
+        mk = self._mask(I, J, False, False)
+        dsxxdx = self._pml("sxx_dx", dsxxdx, X["b"], X["a"], X["k"], mk, I, J, True)
+        dsxzdz = self._pml("sxz_dz", dsxzdz, Z["b"], Z["a"], Z["k"], mk, I, J, False)
+        self.vx[I, J] = self.vx[I, J] + (dsxxdx + dsxzdz) * dt / self.rho[I, J]
+        # vz
+        I, J = slice(N, nx - N - 1), slice(N, nz - N - 1)
+        r = self.rho
+        rh = T(0.25) * (r[I, J] + r[N:nx - N - 1, N + 1:nz - N] + r[N + 1:nx - N, N + 1:nz - N]
+                        + r[N + 1:nx - N, N:nz - N - 1])
+        dsxzdx = self._d(self.sxz, I, J, 0, True) / self.dx
+        dszzdz = self._d(self.szz, I, J, 1, True) / self.dz
+        mk = self._mask(I, J, True, True)
+        dsxzdx = self._pml("sxz_dx", dsxzdx, X["b_half"], X["a_half"], X["k_half"], mk, I, J, True)
+        dszzdz = self._pml("szz_dz", dszzdz, Z["b_half"], Z["a_half"], Z["k_half"], mk, I, J, False)
+        self.vz[I, J] = self.vz[I, J] + (dszzdz + dsxzdx) * dt / rh
+        # source
+        self.vz[self.isx, self.isz] += dt * T(w) / self.rho[self.isx, self.isz]
+        # sxx szz
+        I, J = slice(N, nx - N - 1), slice(N + 1, nz - N)
+        lhx = T(0.5) * (self.lam[I, J] + self.lam[N + 1:nx - N, J])
+        mhx = T(0.5) * (self.mu[I, J] + self.mu[N + 1:nx - N, J])
+        lpm = lhx + T(2) * mhx
+        dvxdx = self._d(self.vx, I, J, 0, True) / self.dx
+        dvzdz = self._d(self.vz, I, J, 1, False) / self.dz
+        mk = self._mask(I, J, True, False)
+        dvxdx = self._pml("dvx_dx", dvxdx, X["b_half"], X["a_half"], X["k_half"], mk, I, J, True)
+        dvzdz = self._pml("dvz_dz", dvzdz, Z["b"], Z["a"], Z["k"], mk, I, J, False)
+        self.sxx[I, J] = self.sxx[I, J] + (lpm * dvxdx + lhx * dvzdz) * dt
+        self.szz[I, J] = self.szz[I, J] + (lpm * dvzdz + lhx * dvxdx) * dt
+        # sxz
+        I, J = slice(N + 1, nx - N), slice(N, nz - N - 1)
+        mhz = T(0.5) * (self.mu[I, N + 1:nz - N] + self.mu[I, J])
+        dvzdx = self._d(self.vz, I, J, 0, False) / self.dx
+        dvxdz = self._d(self.vx, I, J, 1, True) / self.dz
+        mk = self._mask(I, J, False, True)
+        dvzdx = self._pml("dvz_dx", dvzdx, X["b"], X["a"], X["k"], mk, I, J, True)
+        dvxdz = self._pml("dvx_dz", dvxdz, Z["b_half"], Z["a_half"], Z["k_half"], mk, I, J, False)
+        self.sxz[I, J] = self.sxz[I, J] + mhz * (dvxdz + dvzdx) * dt
+        self.data[it] = self.vz[self.rsx, self.rsz]
+
+
+class Twin3DTensor:
+    def __init__(self, o):
+        """Build from an oracle.Oracle3D of scheme TENSOR."""
+        T = o.T
+        self.T = T
+        self.N = o.N
+        d = o.desc
+        self.h = (T(d.dx), T(d.dy), T(d.dz))
+        self.dt = T(d.dt)
+        self.c = np.array([d.c[m] for m in range(o.N)], dtype=np.float64).astype(T)
+        self.rho, self.lam, self.mu = o.rho.copy(), o.lam.copy(), o.mu.copy()
+        z = lambda: np.zeros_like(o.vx)
+        for f in ("vx", "vy", "vz", "sxx", "syy", "szz", "sxy", "sxz", "syz"):
+            setattr(self, f, z())
+        self.mem = {}
+        self.axes = o.axes
+        self.src = (d.isx, d.isy, d.isz)
+        self.mt = [np.float32(d.mt[q]) for q in range(6)]
+        self.rec = (o.rx, o.ry, o.rz)
+        self.data = np.zeros_like(o.data)
+
+    def _d(self, f, box, axis, fwd):
+        T, N, c = self.T, self.N, self.c
+        shp = tuple(s.stop - s.start for s in box)
+        v = np.zeros(shp, T)
+        for m in range(N):
+            a, b = (m + 1, -m) if fwd else (m, -m - 1)
+            hi = tuple(slice(s.start + (a if q == axis else 0), s.stop + (a if q == axis else 0))
+                       for q, s in enumerate(box))
+            lo = tuple(slice(s.start + (b if q == axis else 0), s.stop + (b if q == axis else 0))
+                       for q, s in enumerate(box))
+            v = v + c[m] * (f[hi] - f[lo])
+        return v
+
+    def _mask(self, box, half):
+        T = self.T
+        m = None
+        for q in range(3):
+            i = np.arange(box[q].start, box[q].stop)
+            x = (i - self.N).astype(T) * self.h[q] + (self.h[q] / T(2) if half[q] else T(0))
+            prof, (lo, hi) = self.axes[q]
+            p = _pred(x, T(lo), T(hi))
+            shape = [1, 1, 1]
+            shape[q] = -1
+            p = p.reshape(shape)
+            m = p if m is None else (m | p)
+        return m
+
+    def _pml(self, name, d, q, half, mask, box):
+        prof, _ = self.axes[q]
+        sfx = "_half" if half else ""
+        shape = [1, 1, 1]
+        shape[q] = -1
+        b = prof["b" + sfx][box[q]].reshape(shape)
+        a = prof["a" + sfx][box[q]].reshape(shape)
+        k = prof["k" + sfx][box[q]].reshape(shape)
+        if name not in self.mem:
+            self.mem[name] = np.zeros_like(self.vx)
+        m = self.mem[name]
+        old = m[box]
+        new = b * old + a * d
+        m[box] = np.where(mask, new, old)
+        return np.where(mask, d / k + new, d)
+
+    def step(self, it, w):
+        T, N, dt = self.T, self.N, self.dt
+        nx, ny, nz = self.vx.shape
+        dx, dy, dz = self.h
+        s = self.src
+        src = T(np.float32(w))
+        for f, q in (("sxx", 0), ("syy", 1), ("szz", 2), ("sxy", 3), ("sxz", 4), ("syz", 5)):
+            getattr(self, f)[s] += src * (-T(self.mt[q]))
+        S = lambda a, b: slice(a, b)
+        r, lam, mu = self.rho, self.lam, self.mu
+        # vx
+        B = (S(N, nx - N - 1), S(N + 1, ny - N), S(N + 1, nz - N))
+        d1 = self._d(self.sxx, B, 0, True) / dx
+        d2 = self._d(self.sxy, B, 1, False) / dy
+        d3 = self._d(self.sxz, B, 2, False) / dz
+        mk = self._mask(B, (1, 0, 0))
+        d1 = self._pml("sxx_dx", d1, 0, True, mk, B)
+        d2 = self._pml("sxy_dy", d2, 1, False, mk, B)
+        d3 = self._pml("sxz_dz", d3, 2, False, mk, B)
+        self.vx[B] = self.vx[B] + (d1 + d3 + d2) * dt / r[B]
+        # vy
+        B = (S(N + 1, nx - N), S(N, ny - N - 1), S(N + 1, nz - N))
+        Bj = (B[0], S(N + 1, ny - N), B[2])
+        rhy = T(0.5) * (r[B] + r[Bj])
+        d1 = self._d(self.sxy, B, 0, False) / dx
+        d2 = self._d(self.syy, B, 1, True) / dy
+        d3 = self._d(self.syz, B, 2, False) / dz
+        mk = self._mask(B, (0, 1, 0))
+        d1 = self._pml("sxy_dx", d1, 0, False, mk, B)
+        d2 = self._pml("syy_dy", d2, 1, True, mk, B)
+        d3 = self._pml("syz_dz", d3, 2, False, mk, B)
+        self.vy[B] = self.vy[B] + (d1 + d2 + d3) * dt / rhy
+        # vz
+        B = (S(N + 1, nx - N), S(N + 1, ny - N), S(N, nz - N - 1))
+        Bj = (B[0], S(N + 2, ny - N + 1), B[2])
+        Bij = (S(N + 2, nx - N + 1), S(N + 2, ny - N + 1), B[2])
+        Bi = (S(N + 2, nx - N + 1), B[1], B[2])
+        r4 = T(0.25) * (r[B] + r[Bj] + r[Bij] + r[Bi])
+        d1 = self._d(self.sxz, B, 0, False) / dx
+        d2 = self._d(self.syz, B, 1, False) / dy
+        d3 = self._d(self.szz, B, 2, True) / dz
+        mk = self._mask(B, (0, 0, 1))
+        d1 = self._pml("sxz_dx", d1, 0, False, mk, B)
+        d2 = self._pml("syz_dy", d2, 1, False, mk, B)
+        d3 = self._pml("szz_dz", d3, 2, True, mk, B)
+        self.vz[B] = self.vz[B] + (d1 + d2 + d3) * dt / r4
+        # normal stresses
+        B = (S(N + 1, nx - N), S(N + 1, ny - N), S(N + 1, nz - N))
+        Bi = (S(N + 2, nx - N + 1), B[1], B[2])
+        lhx = T(0.5) * (lam[B] + lam[Bi])
+        mhx = T(0.5) * (mu[B] + mu[Bi])
+        lpm = lhx + T(2) * mhx
+        e1 = self._d(self.vx, B, 0, False) / dx
+        e2 = self._d(self.vy, B, 1, False) / dy
+        e3 = self._d(self.vz, B, 2, False) / dz
+        mk = self._mask(B, (0, 0, 0))
+        e1 = self._pml("dvx_dx", e1, 0, False, mk, B)
+        e2 = self._pml("dvy_dy", e2, 1, False, mk, B)
+        e3 = self._pml("dvz_dz", e3, 2, False, mk, B)
+        self.sxx[B] = self.sxx[B] + (lpm * e1 + lhx * (e3 + e2)) * dt
+        self.syy[B] = self.syy[B] + (lpm * e2 + lhx * (e1 + e3)) * dt
+        self.szz[B] = self.szz[B] + (lpm * e3 + lhx * (e1 + e2)) * dt
+        # sxy
+        B = (S(N + 1, nx - N), S(N + 1, ny - N), S(N, nz - N))
+        Bj = (B[0], S(N + 2, ny - N + 1), B[2])
+        Bi = (S(N + 2, nx - N + 1), B[1], B[2])
+        m4 = T(0.25) * (mu[Bj] + mu[B] + mu[B] + mu[Bi])
+        e1 = self._d(self.vy, B, 0, True) / dx
+        e2 = self._d(self.vx, B, 1, True) / dy
+        mk = self._mask(B, (1, 1, 0))
+        e1 = self._pml("dvy_dx", e1, 0, True, mk, B)
+        e2 = self._pml("dvx_dy", e2, 1, True, mk, B)
+        self.sxy[B] = self.sxy[B] + m4 * (e2 + e1) * dt
+        # sxz
+        B = (S(N, nx - N - 1), S(N, ny - N), S(N, nz - N - 1))
+        Bi = (S(N + 1, nx - N), B[1], B[2])
+        Bj = (B[0], S(N + 1, ny - N + 1), B[2])
+        m4 = T(0.25) * (mu[B] + mu[Bi] + mu[B] + mu[Bj])
+        e1 = self._d(self.vz, B, 0, True) / dx
+        e2 = self._d(self.vx, B, 2, True) / dz
+        mk = self._mask(B, (1, 0, 1))
+        e1 = self._pml("dvz_dx", e1, 0, True, mk, B)
+        e2 = self._pml("dvx_dz", e2, 2, True, mk, B)
+        self.sxz[B] = self.sxz[B] + m4 * (e2 + e1) * dt
+        # syz
+        B = (S(N, nx - N), S(N, ny - N - 1), S(N, nz - N - 1))
+        Bj = (B[0], S(N + 1, ny - N), B[2])
+        Bk = (B[0], B[1], S(N + 1, nz - N))
+        m4 = T(0.25) * (mu[Bj] + mu[B] + mu[Bk] + mu[B])
+        e1 = self._d(self.vz, B, 1, True) / dy
+        e2 = self._d(self.vy, B, 2, True) / dz
+        mk = self._mask(B, (0, 1, 1))
+        e1 = self._pml("dvz_dy", e1, 1, True, mk, B)
+        e2 = self._pml("dvy_dz", e2, 2, True, mk, B)
+        self.syz[B] = self.syz[B] + m4 * (e1 + e2) * dt
+        rx, ry, rz = self.rec
+        self.data[it] = self.vx[rx, ry, rz].astype(np.float32)

@@ -1,0 +1,316 @@
+"""Shared implementation of the three 3D ElasticWAVE drop-ins.
+
+State layout on the device (C-contiguous, last index fastest, as a Taichi
+dense field):
+  vx vy vz sxx syy szz sxy sxz syz   (nx, ny, nz) each, field type
+  rho lam mu                          (nx, ny, nz) each
+  CPML memory variables               slab-compact, 6 per direction:
+      _mem[0] (6, Lx+Rx, ny, nz), _mem[1] (6, nx, Ly+Ry, nz), _mem[2] (6, nx, ny, Lz+Rz)
+  split-PML fields                    (24, nx, ny, nz)
+  data                                (nt, nrec) float32 receiver traces
+The reference's full-grid memory arrays (memory_sxx_dx, ...) are still readable
+as attributes; they are expanded from the slabs on access.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _native as N
+from . import pml as P
+from ._common import (as_device, as_numpy, compute_lam, compute_mu, device, receiver_table,
+                      sw_dtype, torch_dtype)
+
+FIELDS3 = ("vx", "vy", "vz", "sxx", "syy", "szz", "sxy", "sxz", "syz")
+
+# slab-compact memory variables: name -> (direction, component)
+MEM3 = {
+    "memory_sxx_dx": (0, 0), "memory_sxy_dx": (0, 1), "memory_sxz_dx": (0, 2),
+    "memory_dvx_dx": (0, 3), "memory_dvy_dx": (0, 4), "memory_dvz_dx": (0, 5),
+    "memory_sxy_dy": (1, 0), "memory_syy_dy": (1, 1), "memory_syz_dy": (1, 2),
+    "memory_dvy_dy": (1, 3), "memory_dvx_dy": (1, 4), "memory_dvz_dy": (1, 5),
+    "memory_sxz_dz": (2, 0), "memory_syz_dz": (2, 1), "memory_szz_dz": (2, 2),
+    "memory_dvz_dz": (2, 3), "memory_dvx_dz": (2, 4), "memory_dvy_dz": (2, 5),
+}
+
+SPLIT3 = ("vx_x", "vx_y", "vx_z", "vy_x", "vy_y", "vy_z", "vz_x", "vz_y", "vz_z",
+          "sxx_x", "sxx_y", "sxx_z", "syy_x", "syy_y", "syy_z",
+          "sxy_x", "sxy_y", "sxz_x", "sxz_z", "syz_y", "syz_z",
+          "szz_x", "szz_y", "szz_z")
+
+AXES = ("x", "y", "z")
+
+
+class Elastic3DBase:
+    """Common state, PML set-up and stepping of the 3D staggered-grid solvers."""
+
+    _scheme = N.SW3D_CPML_TENSOR
+
+    def _init_common(self, vs, vp, rho, dx, dy, dz, dt, isx, isy, isz, nt, accuracy, freq,
+                     fieldtype, coef64=False):
+        self._dt_torch = torch_dtype(fieldtype)
+        self._np_dtype = np.float64 if self._dt_torch == torch.float64 else np.float32
+        self._dev = device()
+        self.vs = as_device(vs, self._dt_torch, self._dev)
+        self.vp = as_device(vp, self._dt_torch, self._dev)
+        self.rho = as_device(rho, self._dt_torch, self._dev)
+        if self.vs.dim() != 3 or self.vp.shape != self.vs.shape or self.rho.shape != self.vs.shape:
+            raise ValueError("vs, vp and rho must be 3D arrays of one shape (nx, ny, nz)")
+        self.gridsize = tuple(int(s) for s in self.vs.shape)
+        self.dx, self.dy, self.dz = dx, dy, dz
+        self.xmin = self.ymin = self.zmin = 0
+        self.star = int(accuracy)
+        if not 1 <= self.star <= N.SW_MAX_ORDER:
+            raise ValueError(f"accuracy must be in 1..{N.SW_MAX_ORDER}")
+        nx, ny, nz = self.gridsize
+        if min(self.gridsize) < 2 * self.star + 3:
+            raise ValueError("grid too small for the stencil order")
+        self._coef64 = bool(coef64)
+        self.c = torch.as_tensor(self.diff_coff(self.star), device=self._dev)
+        self.xmax = self.xmin + dx * (nx - 1 - 2 * accuracy)
+        self.ymax = self.zmin + dy * (ny - 1 - 2 * accuracy)
+        self.zmax = self.zmin + dz * (nz - 1 - 2 * accuracy)
+        self.mu = self.Compute_mu(fieldtype)
+        self.lam = self.Compute_lam(fieldtype)
+        self.f0 = freq
+        self.dt = dt
+        self.isx, self.isy, self.isz = int(isx), int(isy), int(isz)
+        self.nt = int(nt)
+        z = lambda: torch.zeros(self.gridsize, dtype=self._dt_torch, device=self._dev)
+        for f in FIELDS3:
+            setattr(self, f, z())
+        for ax, n in zip(AXES, self.gridsize):
+            for name in P.PROFILE_NAMES:
+                base, _, half = name.partition("_")
+                attr = f"{base}_{ax}_half" if half else f"{base}_{ax}"
+                setattr(self, attr, torch.zeros(n, dtype=self._dt_torch, device=self._dev))
+        self.xmin_pml, self.xmax_pml = self.xmin, self.xmax
+        self.zmin_pml, self.zmax_pml = self.zmin, self.zmax
+        self._prof = None
+        self._plan = None
+        self._mem = [None, None, None]
+        self._split = None
+
+    # ---- reference helpers ------------------------------------------------
+    def Compute_mu(self, fieldtype=None):
+        """mu = rho*vs**2 (Elastic3D_SSG_Tensor.py:132-139)."""
+        return compute_mu(self.vs, self.rho)
+
+    def Compute_lam(self, fieldtype=None):
+        """lam = rho*(vp**2-2*vs**2) (Elastic3D_SSG_Tensor.py:141-149)."""
+        return compute_lam(self.vs, self.vp, self.rho)
+
+    def diff_coff(self, order):
+        """Elastic3D_SSG_Tensor.py:348-359 (float32 coefficients; float64 ones
+        when the solver was built with coef64=True)."""
+        c32 = P.diff_coff(order)
+        if getattr(self, "_coef64", False):
+            b = np.zeros(order)
+            b[0] = 1
+            A = np.array([[(2 * j + 1) ** (2 * i + 1) for j in range(order)] for i in range(order)], float)
+            return np.linalg.solve(A, b)
+        return c32
+
+    @staticmethod
+    def diff_coff_op(order):
+        return P.diff_coff_op(order)
+
+    # ---- PML set-up -------------------------------------------------------
+    def SetADEPML3D(self, pml_surface, parameter: dict):
+        """Elastic3D_SSG_Tensor.py:361-568 (identical in the CPML/SPML classes)."""
+        pml_surface = list(pml_surface)
+        if len(pml_surface) != 6:
+            raise ValueError("pml_surface is [xL, xR, yL, yR, zTop, zBottom]")
+        thick = (parameter["pml_x_thick"], parameter["pml_y_thick"], parameter["pml_z_thick"])
+        h = (self.dx, self.dy, self.dz)
+        profs = []
+        for a, ax in enumerate(AXES):
+            pr = P.axis_profile(self.gridsize[a], self.star, h[a], thick[a], bool(pml_surface[2 * a]),
+                                bool(pml_surface[2 * a + 1]), parameter["vp_max"], parameter["Rcoef"],
+                                parameter["alpha_max_pml"], parameter["kmax_pml"], parameter["theta"],
+                                self.dt, self._np_dtype)
+            profs.append(pr)
+            for name in P.PROFILE_NAMES:
+                base, _, half = name.partition("_")
+                attr = f"{base}_{ax}_half" if half else f"{base}_{ax}"
+                setattr(self, attr, torch.as_tensor(pr[name], device=self._dev))
+            setattr(self, f"{ax}min_pml", pr.pml_min)
+            setattr(self, f"{ax}max_pml", pr.pml_max)
+        self._prof = profs
+        self._pml_param = dict(parameter)
+        self._pml_surface = pml_surface
+        self._tables = []
+        for a in range(3):
+            pr = profs[a]
+            lo, hi = P.slab_extent(pr)
+            self._tables.append(dict(
+                lo=lo, hi=hi,
+                coef=torch.as_tensor(P.coef_table(pr, self._np_dtype), device=self._dev),
+                damp=torch.as_tensor(P.damp_table(pr, self._np_dtype), device=self._dev),
+                flag=torch.as_tensor(P.axis_flags(self.gridsize[a], self.star, h[a], pr.pml_min, pr.pml_max,
+                                                  self._np_dtype), device=self._dev),
+            ))
+        self._alloc_boundary_state()
+        self._plan = None
+
+    def _alloc_boundary_state(self):
+        nx, ny, nz = self.gridsize
+        if self._scheme == N.SW3D_SPML:
+            self._split = torch.zeros((24, nx, ny, nz), dtype=self._dt_torch, device=self._dev)
+            return
+        s = [t["lo"] + t["hi"] for t in self._tables]
+        shapes = [(6, s[0], ny, nz), (6, nx, s[1], nz), (6, nx, ny, s[2])]
+        self._mem = [torch.zeros(sh, dtype=self._dt_torch, device=self._dev) if min(sh) > 0 else None
+                     for sh in shapes]
+
+    # ---- reference attribute access to the boundary state ------------------
+    def _mem_full(self, name):
+        nx, ny, nz = self.gridsize
+        out = torch.zeros(self.gridsize, dtype=self._dt_torch, device=self._dev)
+        if self._prof is None:
+            return out
+        d, comp = MEM3[name]
+        m = self._mem[d]
+        if m is None:
+            return out
+        lo, hi = self._tables[d]["lo"], self._tables[d]["hi"]
+        n = self.gridsize[d]
+        sl = [slice(None)] * 3
+        src = m[comp]
+        sel = lambda a, b: tuple(slice(a, b) if q == d else slice(None) for q in range(3))
+        if lo:
+            out[sel(0, lo)] = src[sel(0, lo)]
+        if hi:
+            out[sel(n - hi, n)] = src[sel(lo, lo + hi)]
+        return out
+
+    def __getattr__(self, name):
+        if name in MEM3:
+            if self._scheme == N.SW3D_SPML:
+                raise AttributeError(name)
+            return self._mem_full(name)
+        if name in SPLIT3 and self._scheme == N.SW3D_SPML:
+            if self.__dict__.get("_split") is None:
+                return torch.zeros(self.gridsize, dtype=self._dt_torch, device=self._dev)
+            return self._split[SPLIT3.index(name)]
+        raise AttributeError(name)
+
+    # ---- free surface hooks (Elastic3D_SSG_Tensor.py:151-163) ---------------
+    def AEA_init(self):
+        """lam = 0 and rho halved on the first `star` z layers."""
+        o = self.star
+        self.lam[:, :, :o] = 0
+        self.rho[:, :, :o] = 0.5 * self.rho[:, :, :o]
+
+    def AEA(self):
+        """szz = 0 on the z layer `star`."""
+        self.szz[:, :, self.star] = 0
+
+    # ---- plan --------------------------------------------------------------
+    def _source(self):
+        raise NotImplementedError
+
+    def _receivers(self):
+        raise NotImplementedError
+
+    def _build_plan(self):
+        if self._prof is None:
+            raise RuntimeError("call SetADEPML3D(pml_surface, parameter) before stepping")
+        nx, ny, nz = self.gridsize
+        d = N.Desc3D()
+        d.scheme = self._scheme
+        d.dtype = sw_dtype(self._dt_torch)
+        d.nx, d.ny, d.nz = nx, ny, nz
+        d.order = self.star
+        d.nt_max = self.nt
+        d.dx, d.dy, d.dz, d.dt = float(self.dx), float(self.dy), float(self.dz), float(self.dt)
+        cvals = as_numpy(self.c).astype(np.float64)
+        for m in range(self.star):
+            d.coef[m] = float(cvals[m])
+        keep = []
+        for q, f in enumerate(FIELDS3):
+            t = getattr(self, f)
+            keep.append(t)
+            d.field[q] = t.data_ptr()
+        for nm in ("rho", "lam", "mu"):
+            t = getattr(self, nm)
+            keep.append(t)
+            setattr(d, nm, t.data_ptr())
+        for a in range(3):
+            tb = self._tables[a]
+            d.pml[a].lo, d.pml[a].hi = tb["lo"], tb["hi"]
+            d.pml[a].coef = tb["coef"].data_ptr()
+            d.pml[a].damp = tb["damp"].data_ptr()
+            d.pml[a].flag = tb["flag"].data_ptr()
+            keep += [tb["coef"], tb["damp"], tb["flag"]]
+            m = self._mem[a]
+            d.mem[a] = m.data_ptr() if m is not None else None
+            keep.append(m)
+        if self._split is not None:
+            d.split = self._split.data_ptr()
+            keep.append(self._split)
+        kind, (si, sj, sk), wav, mt = self._source()
+        d.src.kind = kind
+        d.src.i, d.src.j, d.src.k = si, sj, sk
+        self._wavelet = torch.as_tensor(wav, device=self._dev).to(self._dt_torch).contiguous()
+        d.src.wavelet = self._wavelet.data_ptr()
+        keep.append(self._wavelet)
+        for q in range(6):
+            d.src.mt[q] = float(mt[q])
+        field, lin = self._receivers()
+        self._rec_index = torch.as_tensor(lin, dtype=torch.int64, device=self._dev)
+        d.rec.nrec = int(lin.size)
+        d.rec.field = field
+        d.rec.index = self._rec_index.data_ptr()
+        d.rec.data = self.data.data_ptr()
+        d.rec.dtype = N.SW_F64 if self.data.dtype == torch.float64 else N.SW_F32
+        keep += [self._rec_index, self.data]
+        self._plan = N.Plan(d, keep, three_d=True)
+        return self._plan
+
+    def _stream(self) -> int:
+        return torch.cuda.current_stream(self._dev).cuda_stream
+
+    def _step(self, nt):
+        if not 0 <= int(nt) < self.nt:
+            raise IndexError(f"time step {nt} outside 0..{self.nt - 1}")
+        plan = self._plan or self._build_plan()
+        plan.step(int(nt), self._stream())
+
+    def run(self, nt=None, it0: int = 0, use_graph: bool = True):
+        """Steps it0 .. it0+nt-1 in one enqueue (CUDA graph), the drivers'
+        `for i in range(nt): test.update_SSG(i)` loop."""
+        nt = self.nt - it0 if nt is None else int(nt)
+        plan = self._plan or self._build_plan()
+        plan.run(int(it0), nt, use_graph, self._stream())
+        return self
+
+    def set_tile(self, x_chunk: int):
+        (self._plan or self._build_plan()).set_tile(int(x_chunk))
+
+    def check_finite(self) -> int:
+        """Number of non-finite wavefield values (0 when the state is finite)."""
+        return (self._plan or self._build_plan()).check_finite(self._stream())
+
+    def set_model(self, vp, vs, rho, non_blocking: bool = True):
+        """Load a new model of the same shape into the solver's own arrays
+        (host->device copy for host inputs) and recompute mu and lam."""
+        for name, src in (("vp", vp), ("vs", vs), ("rho", rho)):
+            t = getattr(self, name)
+            s = src if isinstance(src, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(as_numpy(src)))
+            if tuple(s.shape) != self.gridsize:
+                raise ValueError(f"{name} has shape {tuple(s.shape)}, the solver grid is {self.gridsize}")
+            t.copy_(s, non_blocking=non_blocking)
+        self.mu.copy_(compute_mu(self.vs, self.rho))
+        self.lam.copy_(compute_lam(self.vs, self.vp, self.rho))
+
+    def reset(self):
+        """Zero every wavefield, memory variable and trace (new shot, same model)."""
+        for f in FIELDS3:
+            getattr(self, f).zero_()
+        for m in self._mem:
+            if m is not None:
+                m.zero_()
+        if self._split is not None:
+            self._split.zero_()
+        self.data.zero_()

@@ -1,0 +1,197 @@
+"""ctypes binding of libseiswave.so (include/seiswave.h).
+
+The structures below mirror the C declarations field for field; struct_sizes()
+checks them against the library's own sizeof.  The library is loaded from the
+package's lib/ folder (built in-tree by build_native.py).  There is no CPU
+fallback: if the library is missing, load() raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "lib" / "libseiswave.so"
+
+SW_MAX_ORDER = 8
+SW_OK = 0
+SW_ERR_ARG = -1
+SW_ERR_CUDA = -2
+SW_ERR_NONFINITE = -3
+SW_ERR_UNSUPPORTED = -4
+SW_ERR_TIMEOUT = -5
+
+SW_F32, SW_F64 = 0, 1
+SW2D_SSG_VS, SW2D_SSG_SV, SW2D_RSG = 0, 1, 2
+SW3D_CPML_FORCE, SW3D_CPML_TENSOR, SW3D_SPML = 0, 1, 2
+SW_SRC_NONE, SW_SRC_FORCE, SW_SRC_MOMENT, SW_SRC_RSG4 = 0, 1, 2, 3
+
+# every symbol include/seiswave.h declares
+EXPORTS = (
+    "sw_version", "sw_last_error", "sw2d_plan_create", "sw3d_plan_create",
+    "sw_plan_set_tile", "sw_abi_sizeof", "sw_plan_destroy", "sw_step", "sw_step_amp",
+    "sw_run", "sw_check_finite",
+)
+
+
+class PmlAxis(C.Structure):
+    _fields_ = [
+        ("lo", C.c_int32), ("hi", C.c_int32),
+        ("coef", C.c_void_p), ("damp", C.c_void_p), ("flag", C.c_void_p),
+    ]
+
+
+class Receivers(C.Structure):
+    _fields_ = [
+        ("nrec", C.c_int32), ("field", C.c_int32),
+        ("index", C.c_void_p), ("data", C.c_void_p), ("dtype", C.c_int32),
+    ]
+
+
+class Source(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32), ("i", C.c_int32), ("j", C.c_int32), ("k", C.c_int32),
+        ("wavelet", C.c_void_p), ("mt", C.c_double * 6),
+    ]
+
+
+class Desc2D(C.Structure):
+    _fields_ = [
+        ("scheme", C.c_int32), ("dtype", C.c_int32), ("nx", C.c_int32), ("nz", C.c_int32),
+        ("order", C.c_int32), ("nt_max", C.c_int32),
+        ("dx", C.c_double), ("dz", C.c_double), ("dt", C.c_double),
+        ("coef", C.c_double * SW_MAX_ORDER),
+        ("field", C.c_void_p * 5),
+        ("rho", C.c_void_p), ("lam", C.c_void_p), ("mu", C.c_void_p),
+        ("pml", PmlAxis * 2),
+        ("mem", C.c_void_p * 2),
+        ("src", Source),
+        ("rec", Receivers),
+    ]
+
+
+class Desc3D(C.Structure):
+    _fields_ = [
+        ("scheme", C.c_int32), ("dtype", C.c_int32), ("nx", C.c_int32), ("ny", C.c_int32),
+        ("nz", C.c_int32), ("order", C.c_int32), ("nt_max", C.c_int32),
+        ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double), ("dt", C.c_double),
+        ("coef", C.c_double * SW_MAX_ORDER),
+        ("field", C.c_void_p * 9),
+        ("rho", C.c_void_p), ("lam", C.c_void_p), ("mu", C.c_void_p),
+        ("pml", PmlAxis * 3),
+        ("mem", C.c_void_p * 3),
+        ("split", C.c_void_p),
+        ("src", Source),
+        ("rec", Receivers),
+    ]
+
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Load libseiswave.so once; raise if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise ImportError(
+            f"{LIB_PATH} is missing: build the sm_100a kernels with "
+            "`python -m seiswave_taichi_b200.build_native` (there is no CPU fallback)")
+    lib = C.CDLL(str(LIB_PATH))
+    vp = C.c_void_p
+    sig = {
+        "sw_version": (C.c_int, []),
+        "sw_last_error": (C.c_char_p, []),
+        "sw2d_plan_create": (C.c_int, [C.POINTER(Desc2D), C.POINTER(vp)]),
+        "sw3d_plan_create": (C.c_int, [C.POINTER(Desc3D), C.POINTER(vp)]),
+        "sw_plan_set_tile": (C.c_int, [vp, C.c_int32]),
+        "sw_abi_sizeof": (C.c_int, [C.c_int32]),
+        "sw_plan_destroy": (C.c_int, [vp]),
+        "sw_step": (C.c_int, [vp, C.c_int32, vp]),
+        "sw_step_amp": (C.c_int, [vp, C.c_int32, C.c_double, vp]),
+        "sw_run": (C.c_int, [vp, C.c_int32, C.c_int32, C.c_int32, vp]),
+        "sw_check_finite": (C.c_int, [vp, vp, C.POINTER(C.c_int64)]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def struct_sizes() -> dict:
+    """(python sizeof, library sizeof) of each ABI struct."""
+    lib = load()
+    ours = [PmlAxis, Receivers, Source, Desc2D, Desc3D]
+    return {t.__name__: (C.sizeof(t), lib.sw_abi_sizeof(q)) for q, t in enumerate(ours)}
+
+
+class SeisWaveError(RuntimeError):
+    """A libseiswave call returned an error status."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"libseiswave error {code}: {msg}")
+        self.code = code
+
+
+def check(rc: int) -> None:
+    if rc != SW_OK:
+        msg = load().sw_last_error()
+        raise SeisWaveError(rc, msg.decode() if msg else "")
+
+
+def ptr(t) -> int | None:
+    """Raw device pointer of a torch tensor (None for None)."""
+    if t is None:
+        return None
+    return t.data_ptr()
+
+
+class Plan:
+    """Owns one sw_plan; keeps every tensor it borrows alive."""
+
+    def __init__(self, desc, keep, three_d: bool):
+        lib = load()
+        h = C.c_void_p()
+        if three_d:
+            check(lib.sw3d_plan_create(C.byref(desc), C.byref(h)))
+        else:
+            check(lib.sw2d_plan_create(C.byref(desc), C.byref(h)))
+        self._h = h
+        self._desc = desc
+        self._keep = keep
+
+    @property
+    def handle(self):
+        return self._h
+
+    def step(self, it: int, stream: int = 0) -> None:
+        check(load().sw_step(self._h, int(it), C.c_void_p(stream)))
+
+    def step_amp(self, it: int, amp: float, stream: int = 0) -> None:
+        check(load().sw_step_amp(self._h, int(it), float(amp), C.c_void_p(stream)))
+
+    def run(self, it0: int, nsteps: int, use_graph: bool = True, stream: int = 0) -> None:
+        check(load().sw_run(self._h, int(it0), int(nsteps), 1 if use_graph else 0, C.c_void_p(stream)))
+
+    def set_tile(self, x_chunk: int) -> None:
+        check(load().sw_plan_set_tile(self._h, int(x_chunk)))
+
+    def check_finite(self, stream: int = 0) -> int:
+        n = C.c_int64(0)
+        rc = load().sw_check_finite(self._h, C.c_void_p(stream), C.byref(n))
+        if rc not in (SW_OK, SW_ERR_NONFINITE):
+            check(rc)
+        return int(n.value)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            load().sw_plan_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,468 @@
+// capi.cu -- the extern "C" boundary of libseiswave.so (include/seiswave.h).
+//
+// A plan validates a descriptor once (shapes, orders, slab extents, source and
+// receiver cells) and freezes the kernel parameter blocks; sw_step / sw_run
+// then only enqueue kernels.  sw_run replays a cached CUDA graph of the whole
+// step sequence so the per-step launch cost of the reference's Python loop
+// (test2d_homegenous.py:55-56) disappears.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "sw_device.cuh"
+
+namespace sw {
+template <typename T> cudaError_t sw3_velocity(const P3<T>&, int, int, bool, bool, cudaStream_t);
+template <typename T> cudaError_t sw3_stress(const P3<T>&, int, int, bool, cudaStream_t);
+template <typename T> cudaError_t sw3_moment_inject(const P3<T>&, int, cudaStream_t);
+template <typename T> cudaError_t sw3_force_inject(const P3<T>&, int, cudaStream_t);
+template <typename T> cudaError_t sw3_gather(const P3<T>&, int, cudaStream_t);
+template <typename T> cudaError_t sw3_spml_step(const P3<T>&, int, int, bool, cudaStream_t);
+template <typename T> cudaError_t sw2_step(const P2<T>&, int, int, int, T, bool, cudaStream_t);
+}  // namespace sw
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+int cuda_fail(cudaError_t e, const char* where) {
+  return fail(SW_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+// count of non-finite values over a set of arrays
+template <typename T>
+__global__ void k_count_nonfinite(const T* a, long long n, unsigned long long* out) {
+  unsigned long long local = 0;
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    if (!isfinite(a[q])) ++local;
+  if (local) atomicAdd(out, local);
+}
+
+}  // namespace
+
+struct sw_plan {
+  int dim = 0, scheme = 0, dtype = 0, order = 0, nt_max = 0;
+  sw::P2<float> p2f{};
+  sw::P2<double> p2d{};
+  sw::P3<float> p3f{};
+  sw::P3<double> p3d{};
+  bool gather_in_stress = true;  // receivers record a velocity field
+  bool src_in_kernel = true;     // the source cell is covered by the fused passes
+  int src_kind = SW_SRC_NONE;
+  long long ncell = 0;
+  int nfield = 0;
+  void* fields[9] = {};
+  cudaStream_t cap_stream = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  int g_it0 = -1, g_n = -1;
+  unsigned long long* d_count = nullptr;
+};
+
+namespace {
+
+int dsize(int dtype) { return dtype == SW_F64 ? 8 : 4; }
+
+bool aligned(const void* p, int n) { return ((uintptr_t)p % (uintptr_t)n) == 0; }
+
+int check_axis(const sw_pml_axis& a, int n, const char* name, bool need_damp, int esz) {
+  char buf[256];
+  if (a.lo < 0 || a.hi < 0 || a.lo + a.hi > n) {
+    snprintf(buf, sizeof buf, "pml axis %s: slab widths lo=%d hi=%d do not fit n=%d", name, a.lo, a.hi, n);
+    return fail(SW_ERR_ARG, buf);
+  }
+  if (!a.coef || !aligned(a.coef, esz)) {
+    snprintf(buf, sizeof buf, "pml axis %s: coefficient table missing or misaligned", name);
+    return fail(SW_ERR_ARG, buf);
+  }
+  if (!a.flag) {
+    snprintf(buf, sizeof buf, "pml axis %s: predicate flags missing", name);
+    return fail(SW_ERR_ARG, buf);
+  }
+  if (need_damp && (!a.damp || !aligned(a.damp, esz))) {
+    snprintf(buf, sizeof buf, "pml axis %s: split-PML damping profile missing", name);
+    return fail(SW_ERR_ARG, buf);
+  }
+  return SW_OK;
+}
+
+int check_receivers(const sw_receivers& r, int nfield, long long ncell, int nt_max) {
+  if (r.nrec < 0) return fail(SW_ERR_ARG, "receivers: nrec < 0");
+  if (r.nrec == 0) return SW_OK;
+  if (!r.index || !r.data) return fail(SW_ERR_ARG, "receivers: index or data pointer missing");
+  if (r.field < 0 || r.field >= nfield) return fail(SW_ERR_ARG, "receivers: field index out of range");
+  if (r.dtype != SW_F32 && r.dtype != SW_F64) return fail(SW_ERR_ARG, "receivers: dtype must be SW_F32 or SW_F64");
+  if (nt_max <= 0) return fail(SW_ERR_ARG, "receivers: nt_max must be positive");
+  std::vector<long long> h(r.nrec);
+  cudaError_t e = cudaMemcpy(h.data(), r.index, sizeof(long long) * r.nrec, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(e, "receivers: reading the index table");
+  for (int q = 0; q < r.nrec; ++q)
+    if (h[q] < 0 || h[q] >= ncell) {
+      char buf[160];
+      snprintf(buf, sizeof buf, "receivers: index %d = %lld outside the grid of %lld cells", q, h[q], ncell);
+      return fail(SW_ERR_ARG, buf);
+    }
+  return SW_OK;
+}
+
+template <typename T>
+void fill_axis3(sw::P3<T>& p, int d, const sw_pml_axis& a, int n) {
+  p.cf[d] = (const T*)a.coef;
+  p.dmp[d] = (const T*)a.damp;
+  p.fl[d] = a.flag;
+  p.lo[d] = a.lo;
+  p.hi[d] = a.hi;
+  p.sn[d] = a.lo + a.hi;
+  (void)n;
+}
+
+int choose_x_chunk(int nx, int ny, int nz) {
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long tiles = (long long)((nz + 31) / 32) * ((ny + 7) / 8);
+  const long long target = (long long)sms * 8;  // ~8 resident-sized CTAs per SM
+  long long chunks = (target + tiles - 1) / tiles;
+  if (chunks < 1) chunks = 1;
+  int xc = (int)((nx + chunks - 1) / chunks);
+  if (xc < 4) xc = 4;
+  return xc;
+}
+
+template <typename T>
+int make_p3(sw_plan* pl, const sw3d_desc* d, sw::P3<T>& p) {
+  p.nx = d->nx; p.ny = d->ny; p.nz = d->nz;
+  p.dx = (T)d->dx; p.dy = (T)d->dy; p.dz = (T)d->dz; p.dt = (T)d->dt;
+  for (int m = 0; m < SW_MAX_ORDER; ++m) p.c[m] = (T)d->coef[m];
+  for (int q = 0; q < 9; ++q) p.f[q] = (T*)d->field[q];
+  p.rho = (const T*)d->rho; p.lam = (const T*)d->lam; p.mu = (const T*)d->mu;
+  const int ns[3] = {d->nx, d->ny, d->nz};
+  for (int a = 0; a < 3; ++a) fill_axis3(p, a, d->pml[a], ns[a]);
+  for (int a = 0; a < 3; ++a) p.mem[a] = (T*)d->mem[a];
+  p.mcomp[0] = (long long)p.sn[0] * d->ny * d->nz;
+  p.mcomp[1] = (long long)d->nx * p.sn[1] * d->nz;
+  p.mcomp[2] = (long long)d->nx * d->ny * p.sn[2];
+  p.split = (T*)d->split;
+  p.src_kind = d->src.kind; p.si = d->src.i; p.sj = d->src.j; p.sk = d->src.k;
+  p.wav = (const T*)d->src.wavelet;
+  for (int q = 0; q < 6; ++q) p.mneg[q] = -(T)(float)d->src.mt[q];
+  p.nrec = d->rec.nrec; p.rec_field = d->rec.field;
+  p.rec_idx = (const long long*)d->rec.index; p.rec_data = d->rec.data;
+  p.rec_f64 = d->rec.dtype == SW_F64;
+  p.x_chunk = choose_x_chunk(d->nx, d->ny, d->nz);
+  (void)pl;
+  return SW_OK;
+}
+
+template <typename T>
+int make_p2(const sw2d_desc* d, sw::P2<T>& p) {
+  p.nx = d->nx; p.nz = d->nz;
+  p.dx = (T)d->dx; p.dz = (T)d->dz; p.dt = (T)d->dt;
+  for (int m = 0; m < SW_MAX_ORDER; ++m) p.c[m] = (T)d->coef[m];
+  for (int q = 0; q < 5; ++q) p.f[q] = (T*)d->field[q];
+  p.rho = (const T*)d->rho; p.lam = (const T*)d->lam; p.mu = (const T*)d->mu;
+  for (int a = 0; a < 2; ++a) {
+    p.cf[a] = (const T*)d->pml[a].coef;
+    p.fl[a] = d->pml[a].flag;
+    p.lo[a] = d->pml[a].lo;
+    p.hi[a] = d->pml[a].hi;
+    p.sn[a] = d->pml[a].lo + d->pml[a].hi;
+    p.mem[a] = (T*)d->mem[a];
+  }
+  p.mcomp[0] = (long long)p.sn[0] * d->nz;
+  p.mcomp[1] = (long long)d->nx * p.sn[1];
+  p.src_kind = d->src.kind; p.si = d->src.i; p.sk = d->src.j;
+  p.wav = (const T*)d->src.wavelet;
+  p.nrec = d->rec.nrec; p.rec_field = d->rec.field;
+  p.rec_idx = (const long long*)d->rec.index; p.rec_data = d->rec.data;
+  p.rec_f64 = d->rec.dtype == SW_F64;
+  return SW_OK;
+}
+
+// ---------------------------------------------------------------------------
+// one step, enqueued
+// ---------------------------------------------------------------------------
+template <typename T>
+cudaError_t enqueue3(sw_plan* pl, const sw::P3<T>& p, int it, bool first, bool last, cudaStream_t st) {
+  cudaError_t e = cudaSuccess;
+  sw::P3<T> q = p;
+  if (!pl->gather_in_stress) q.nrec = 0;
+  if (pl->scheme == SW3D_SPML) {
+    e = sw::sw3_spml_step<T>(q, pl->order, it, pl->gather_in_stress, st);
+    if (e == cudaSuccess && !pl->gather_in_stress) e = sw::sw3_gather<T>(p, it, st);
+    return e;
+  }
+  const bool tensor = pl->scheme == SW3D_CPML_TENSOR;
+  const bool moment = pl->src_kind == SW_SRC_MOMENT;
+  // moment tensor: the stress pass of step it-1 already added step it's
+  // source unless this is the first step of the sequence
+  if (moment && (first || !pl->src_in_kernel)) {
+    e = sw::sw3_moment_inject<T>(p, it, st);
+    if (e != cudaSuccess) return e;
+  }
+  const bool force = pl->src_kind == SW_SRC_FORCE;
+  e = sw::sw3_velocity<T>(q, pl->order, it, tensor, force && pl->src_in_kernel, st);
+  if (e != cudaSuccess) return e;
+  if (force && !pl->src_in_kernel) {
+    e = sw::sw3_force_inject<T>(p, it, st);
+    if (e != cudaSuccess) return e;
+  }
+  const bool inject_next = moment && pl->src_in_kernel && !last;
+  e = sw::sw3_stress<T>(q, pl->order, it, inject_next, st);
+  if (e != cudaSuccess) return e;
+  if (!pl->gather_in_stress) e = sw::sw3_gather<T>(p, it, st);
+  return e;
+}
+
+cudaError_t enqueue_step(sw_plan* pl, int it, bool first, bool last, bool has_amp, double amp, cudaStream_t st) {
+  if (pl->dim == 3) {
+    return pl->dtype == SW_F32 ? enqueue3<float>(pl, pl->p3f, it, first, last, st)
+                               : enqueue3<double>(pl, pl->p3d, it, first, last, st);
+  }
+  if (pl->dtype == SW_F32) {
+    float a = has_amp ? (float)amp : 0.f;
+    return sw::sw2_step<float>(pl->p2f, pl->scheme, pl->order, it, a, pl->gather_in_stress, st);
+  }
+  double a = has_amp ? (double)(float)amp : 0.0;
+  return sw::sw2_step<double>(pl->p2d, pl->scheme, pl->order, it, a, pl->gather_in_stress, st);
+}
+
+int check_it(sw_plan* pl, int it0, int n) {
+  if (!pl) return fail(SW_ERR_ARG, "null plan");
+  if (n < 0 || it0 < 0) return fail(SW_ERR_ARG, "negative step index or count");
+  const bool needs_wavelet = pl->src_kind == SW_SRC_FORCE || pl->src_kind == SW_SRC_MOMENT;
+  const bool records = pl->dim == 3 ? pl->p3f.nrec + pl->p3d.nrec > 0 : pl->p2f.nrec + pl->p2d.nrec > 0;
+  if ((needs_wavelet || records) && (long long)it0 + n > pl->nt_max) {
+    char buf[160];
+    snprintf(buf, sizeof buf, "steps %d..%d exceed nt_max=%d of the wavelet/receiver arrays", it0,
+             it0 + n - 1, pl->nt_max);
+    return fail(SW_ERR_ARG, buf);
+  }
+  return SW_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sw_version(void) { return SW_ABI_VERSION; }
+
+int sw_abi_sizeof(int32_t which) {
+  switch (which) {
+    case 0: return (int)sizeof(sw_pml_axis);
+    case 1: return (int)sizeof(sw_receivers);
+    case 2: return (int)sizeof(sw_source);
+    case 3: return (int)sizeof(sw2d_desc);
+    case 4: return (int)sizeof(sw3d_desc);
+    default: return -1;
+  }
+}
+
+const char* sw_last_error(void) { return g_err.c_str(); }
+
+int sw2d_plan_create(const sw2d_desc* d, sw_plan** out) {
+  g_err.clear();
+  if (!d || !out) return fail(SW_ERR_ARG, "null descriptor or output pointer");
+  *out = nullptr;
+  if (d->scheme < SW2D_SSG_VS || d->scheme > SW2D_RSG) return fail(SW_ERR_ARG, "unknown 2D scheme");
+  if (d->dtype != SW_F32 && d->dtype != SW_F64) return fail(SW_ERR_ARG, "dtype must be SW_F32 or SW_F64");
+  if (d->order < 1 || d->order > SW_MAX_ORDER) return fail(SW_ERR_ARG, "order (accuracy) must be in 1..8");
+  const int N = d->order;
+  if (d->nx < 2 * N + 3 || d->nz < 2 * N + 3) return fail(SW_ERR_ARG, "grid too small for the stencil order");
+  if (!(d->dx > 0) || !(d->dz > 0) || !(d->dt > 0)) return fail(SW_ERR_ARG, "dx, dz and dt must be positive");
+  const int esz = dsize(d->dtype);
+  for (int q = 0; q < 5; ++q)
+    if (!d->field[q] || !aligned(d->field[q], esz)) return fail(SW_ERR_ARG, "wavefield pointer missing or misaligned");
+  if (!d->rho || !d->lam || !d->mu) return fail(SW_ERR_ARG, "material pointer missing");
+  int rc;
+  if ((rc = check_axis(d->pml[0], d->nx, "x", false, esz)) != SW_OK) return rc;
+  if ((rc = check_axis(d->pml[1], d->nz, "z", false, esz)) != SW_OK) return rc;
+  if (d->pml[0].lo + d->pml[0].hi > 0 && !d->mem[0]) return fail(SW_ERR_ARG, "x memory variables missing");
+  if (d->pml[1].lo + d->pml[1].hi > 0 && !d->mem[1]) return fail(SW_ERR_ARG, "z memory variables missing");
+  const sw_source& s = d->src;
+  if (s.kind != SW_SRC_NONE) {
+    if (d->scheme == SW2D_RSG) {
+      if (s.kind != SW_SRC_RSG4) return fail(SW_ERR_ARG, "RSG takes the SW_SRC_RSG4 source");
+      if (s.i < 1 || s.i >= d->nx || s.j < 1 || s.j >= d->nz) return fail(SW_ERR_ARG, "RSG source block outside the grid");
+    } else {
+      if (s.kind != SW_SRC_FORCE) return fail(SW_ERR_ARG, "2D SSG schemes take a SW_SRC_FORCE source");
+      if (s.i < 0 || s.i >= d->nx || s.j < 0 || s.j >= d->nz) return fail(SW_ERR_ARG, "source cell outside the grid");
+      if (!s.wavelet) return fail(SW_ERR_ARG, "source wavelet missing");
+    }
+  }
+  const long long ncell = (long long)d->nx * d->nz;
+  if ((rc = check_receivers(d->rec, 5, ncell, d->nt_max)) != SW_OK) return rc;
+  sw_plan* pl = new sw_plan();
+  pl->dim = 2; pl->scheme = d->scheme; pl->dtype = d->dtype; pl->order = N; pl->nt_max = d->nt_max;
+  pl->src_kind = s.kind;
+  pl->gather_in_stress = d->rec.nrec == 0 || d->rec.field <= 1;
+  pl->ncell = ncell;
+  pl->nfield = 5;
+  for (int q = 0; q < 5; ++q) pl->fields[q] = d->field[q];
+  if (d->dtype == SW_F32) make_p2<float>(d, pl->p2f);
+  else make_p2<double>(d, pl->p2d);
+  *out = pl;
+  return SW_OK;
+}
+
+int sw3d_plan_create(const sw3d_desc* d, sw_plan** out) {
+  g_err.clear();
+  if (!d || !out) return fail(SW_ERR_ARG, "null descriptor or output pointer");
+  *out = nullptr;
+  if (d->scheme < SW3D_CPML_FORCE || d->scheme > SW3D_SPML) return fail(SW_ERR_ARG, "unknown 3D scheme");
+  if (d->dtype != SW_F32 && d->dtype != SW_F64) return fail(SW_ERR_ARG, "dtype must be SW_F32 or SW_F64");
+  if (d->order < 1 || d->order > SW_MAX_ORDER) return fail(SW_ERR_ARG, "order (accuracy) must be in 1..8");
+  const int N = d->order;
+  if (d->nx < 2 * N + 3 || d->ny < 2 * N + 3 || d->nz < 2 * N + 3)
+    return fail(SW_ERR_ARG, "grid too small for the stencil order");
+  if (!(d->dx > 0) || !(d->dy > 0) || !(d->dz > 0) || !(d->dt > 0))
+    return fail(SW_ERR_ARG, "dx, dy, dz and dt must be positive");
+  const int esz = dsize(d->dtype);
+  for (int q = 0; q < 9; ++q)
+    if (!d->field[q] || !aligned(d->field[q], esz)) return fail(SW_ERR_ARG, "wavefield pointer missing or misaligned");
+  if (!d->rho || !d->lam || !d->mu) return fail(SW_ERR_ARG, "material pointer missing");
+  const bool spml = d->scheme == SW3D_SPML;
+  int rc;
+  const char* names[3] = {"x", "y", "z"};
+  const int ns[3] = {d->nx, d->ny, d->nz};
+  for (int a = 0; a < 3; ++a) {
+    if ((rc = check_axis(d->pml[a], ns[a], names[a], spml, esz)) != SW_OK) return rc;
+    if (!spml && d->pml[a].lo + d->pml[a].hi > 0 && !d->mem[a])
+      return fail(SW_ERR_ARG, std::string(names[a]) + " memory variables missing");
+  }
+  if (spml && !d->split) return fail(SW_ERR_ARG, "split-PML fields missing");
+  const sw_source& s = d->src;
+  bool in_kernel = true;
+  if (s.kind != SW_SRC_NONE) {
+    if (s.i < 0 || s.i >= d->nx || s.j < 0 || s.j >= d->ny || s.k < 0 || s.k >= d->nz)
+      return fail(SW_ERR_ARG, "source cell outside the grid");
+    if (!s.wavelet) return fail(SW_ERR_ARG, "source wavelet missing");
+    if (d->scheme == SW3D_CPML_TENSOR && s.kind != SW_SRC_MOMENT)
+      return fail(SW_ERR_ARG, "the tensor scheme takes a SW_SRC_MOMENT source");
+    if (d->scheme != SW3D_CPML_TENSOR && s.kind != SW_SRC_FORCE)
+      return fail(SW_ERR_ARG, "the point-force schemes take a SW_SRC_FORCE source");
+    // the fused passes cover cells [N, n-N) on every axis
+    in_kernel = s.i >= N && s.i < d->nx - N && s.j >= N && s.j < d->ny - N && s.k >= N && s.k < d->nz - N;
+    if (spml) in_kernel = true;
+  }
+  const long long ncell = (long long)d->nx * d->ny * d->nz;
+  if ((rc = check_receivers(d->rec, 9, ncell, d->nt_max)) != SW_OK) return rc;
+  sw_plan* pl = new sw_plan();
+  pl->dim = 3; pl->scheme = d->scheme; pl->dtype = d->dtype; pl->order = N; pl->nt_max = d->nt_max;
+  pl->src_kind = s.kind;
+  pl->src_in_kernel = in_kernel;
+  pl->gather_in_stress = d->rec.nrec == 0 || d->rec.field <= 2;
+  pl->ncell = ncell;
+  pl->nfield = 9;
+  for (int q = 0; q < 9; ++q) pl->fields[q] = d->field[q];
+  if (d->dtype == SW_F32) make_p3<float>(pl, d, pl->p3f);
+  else make_p3<double>(pl, d, pl->p3d);
+  *out = pl;
+  return SW_OK;
+}
+
+int sw_plan_set_tile(sw_plan* pl, int32_t x_chunk) {
+  if (!pl) return fail(SW_ERR_ARG, "null plan");
+  if (pl->dim != 3) return fail(SW_ERR_UNSUPPORTED, "tile choice applies to 3D plans");
+  if (x_chunk < 1) return fail(SW_ERR_ARG, "x_chunk must be >= 1");
+  pl->p3f.x_chunk = x_chunk;
+  pl->p3d.x_chunk = x_chunk;
+  if (pl->gexec) { cudaGraphExecDestroy(pl->gexec); pl->gexec = nullptr; pl->g_it0 = pl->g_n = -1; }
+  return SW_OK;
+}
+
+int sw_plan_destroy(sw_plan* pl) {
+  if (!pl) return SW_OK;
+  if (pl->gexec) cudaGraphExecDestroy(pl->gexec);
+  if (pl->cap_stream) cudaStreamDestroy(pl->cap_stream);
+  if (pl->d_count) cudaFree(pl->d_count);
+  delete pl;
+  return SW_OK;
+}
+
+int sw_step(sw_plan* pl, int32_t it, void* stream) {
+  int rc = check_it(pl, it, 1);
+  if (rc != SW_OK) return rc;
+  cudaError_t e = enqueue_step(pl, it, true, true, false, 0.0, (cudaStream_t)stream);
+  if (e != cudaSuccess) return cuda_fail(e, "sw_step");
+  return SW_OK;
+}
+
+int sw_step_amp(sw_plan* pl, int32_t it, double amplitude, void* stream) {
+  if (!pl) return fail(SW_ERR_ARG, "null plan");
+  if (!(pl->dim == 2 && pl->scheme == SW2D_RSG))
+    return fail(SW_ERR_UNSUPPORTED, "a per-call source amplitude applies to the 2D RSG scheme");
+  int rc = check_it(pl, it, 1);
+  if (rc != SW_OK) return rc;
+  cudaError_t e = enqueue_step(pl, it, true, true, true, amplitude, (cudaStream_t)stream);
+  if (e != cudaSuccess) return cuda_fail(e, "sw_step_amp");
+  return SW_OK;
+}
+
+int sw_run(sw_plan* pl, int32_t it0, int32_t nsteps, int32_t use_graph, void* stream) {
+  int rc = check_it(pl, it0, nsteps);
+  if (rc != SW_OK) return rc;
+  if (nsteps == 0) return SW_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e;
+  if (!use_graph) {
+    for (int s = 0; s < nsteps; ++s) {
+      e = enqueue_step(pl, it0 + s, s == 0, s == nsteps - 1, false, 0.0, st);
+      if (e != cudaSuccess) return cuda_fail(e, "sw_run");
+    }
+    return SW_OK;
+  }
+  if (!(pl->gexec && pl->g_it0 == it0 && pl->g_n == nsteps)) {
+    if (pl->gexec) { cudaGraphExecDestroy(pl->gexec); pl->gexec = nullptr; }
+    if (!pl->cap_stream) {
+      e = cudaStreamCreateWithFlags(&pl->cap_stream, cudaStreamNonBlocking);
+      if (e != cudaSuccess) return cuda_fail(e, "sw_run: capture stream");
+    }
+    e = cudaStreamBeginCapture(pl->cap_stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return cuda_fail(e, "sw_run: begin capture");
+    cudaError_t le = cudaSuccess;
+    for (int s = 0; s < nsteps && le == cudaSuccess; ++s)
+      le = enqueue_step(pl, it0 + s, s == 0, s == nsteps - 1, false, 0.0, pl->cap_stream);
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(pl->cap_stream, &g);
+    if (le != cudaSuccess) { if (g) cudaGraphDestroy(g); return cuda_fail(le, "sw_run: capture"); }
+    if (e != cudaSuccess) return cuda_fail(e, "sw_run: end capture");
+    e = cudaGraphInstantiate(&pl->gexec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) { pl->gexec = nullptr; return cuda_fail(e, "sw_run: instantiate"); }
+    pl->g_it0 = it0;
+    pl->g_n = nsteps;
+  }
+  e = cudaGraphLaunch(pl->gexec, st);
+  if (e != cudaSuccess) return cuda_fail(e, "sw_run: graph launch");
+  return SW_OK;
+}
+
+int sw_check_finite(sw_plan* pl, void* stream, int64_t* nonfinite) {
+  if (!pl || !nonfinite) return fail(SW_ERR_ARG, "null plan or output");
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e;
+  if (!pl->d_count) {
+    e = cudaMalloc(&pl->d_count, sizeof(unsigned long long));
+    if (e != cudaSuccess) return cuda_fail(e, "sw_check_finite: counter");
+  }
+  e = cudaMemsetAsync(pl->d_count, 0, sizeof(unsigned long long), st);
+  if (e != cudaSuccess) return cuda_fail(e, "sw_check_finite: reset");
+  for (int q = 0; q < pl->nfield; ++q) {
+    if (pl->dtype == SW_F32) k_count_nonfinite<float><<<1184, 256, 0, st>>>((const float*)pl->fields[q], pl->ncell, pl->d_count);
+    else k_count_nonfinite<double><<<1184, 256, 0, st>>>((const double*)pl->fields[q], pl->ncell, pl->d_count);
+  }
+  unsigned long long h = 0;
+  e = cudaMemcpyAsync(&h, pl->d_count, sizeof h, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(e, "sw_check_finite");
+  *nonfinite = (int64_t)h;
+  if (h) return fail(SW_ERR_NONFINITE, "wavefield holds " + std::to_string(h) + " non-finite values");
+  return SW_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,399 @@
+// elastic2d.cu -- 2D P-SV staggered-grid kernels with ADE-CPML.
+//
+// Restates src/Elastic2D_CPML.py as two passes per step, one thread per cell:
+//   k2_velocity<VS>  vx, vz, point source                 update_SSG_VS :144-170
+//   k2_stress<VS>    sxx szz, sxz (+ receivers of v)       update_SSG_VS :172-200
+//   k2_velocity<SV>  / k2_stress<SV>                       update_SSG_SV :218-274
+//   k2_velocity<RSG> / k2_stress<RSG>                      update_RSG    :292-353
+// Block = 32 (z, contiguous) x 8 (x).  CPML memory variables live only on their
+// slabs (mem[0]: x direction (4, lo+hi, nz); mem[1]: z direction (4, nx, lo+hi)),
+// components x: sxx_dx sxz_dx dvx_dx dvz_dx, z: sxz_dz szz_dz dvz_dz dvx_dz --
+// the same named arrays serve all three schemes, as in the reference.
+#include "sw_device.cuh"
+
+namespace sw {
+
+constexpr int T2Z = 32;
+constexpr int T2X = 8;
+
+template <typename T>
+__device__ __forceinline__ void pml2(T* __restrict__ m, T b, T a, T kk, T& d) {
+  T psi = b * (*m) + a * d;
+  *m = psi;
+  d = d / kk + psi;
+}
+
+// ---- 2D stencils of src/Differential2D.py, read through the read-only path --
+template <typename T, int N>
+__device__ __forceinline__ T dx_fm(const T* f, long long idx, int nz, const T* c) {
+  T v = 0;
+#pragma unroll
+  for (int m = 0; m < N; ++m) v += c[m] * (ldg(f + idx + (long long)(m + 1) * nz) - ldg(f + idx - (long long)m * nz));
+  return v;
+}
+template <typename T, int N>
+__device__ __forceinline__ T dz_fm(const T* f, long long idx, const T* c) {
+  T v = 0;
+#pragma unroll
+  for (int m = 0; m < N; ++m) v += c[m] * (ldg(f + idx + (m + 1)) - ldg(f + idx - m));
+  return v;
+}
+template <typename T, int N>
+__device__ __forceinline__ T dx_bm(const T* f, long long idx, int nz, const T* c) {
+  T v = 0;
+#pragma unroll
+  for (int m = 0; m < N; ++m) v += c[m] * (ldg(f + idx + (long long)m * nz) - ldg(f + idx - (long long)(m + 1) * nz));
+  return v;
+}
+template <typename T, int N>
+__device__ __forceinline__ T dz_bm(const T* f, long long idx, const T* c) {
+  T v = 0;
+#pragma unroll
+  for (int m = 0; m < N; ++m) v += c[m] * (ldg(f + idx + m) - ldg(f + idx - (m + 1)));
+  return v;
+}
+// rotated: Drx2fm f[i+m+1, j+m+1] - f[i-m, j-m]
+template <typename T, int N>
+__device__ __forceinline__ T drx_fm(const T* f, long long idx, int nz, const T* c) {
+  T v = 0;
+#pragma unroll
+  for (int m = 0; m < N; ++m)
+    v += c[m] * (ldg(f + idx + (long long)(m + 1) * nz + (m + 1)) - ldg(f + idx - (long long)m * nz - m));
+  return v;
+}
+// Drz2fm f[i-m, j+m+1] - f[i+m+1, j-m]
+template <typename T, int N>
+__device__ __forceinline__ T drz_fm(const T* f, long long idx, int nz, const T* c) {
+  T v = 0;
+#pragma unroll
+  for (int m = 0; m < N; ++m)
+    v += c[m] * (ldg(f + idx - (long long)m * nz + (m + 1)) - ldg(f + idx + (long long)(m + 1) * nz - m));
+  return v;
+}
+// Drx2bm f[i+m, j+m] - f[i-m-1, j-m-1]
+template <typename T, int N>
+__device__ __forceinline__ T drx_bm(const T* f, long long idx, int nz, const T* c) {
+  T v = 0;
+#pragma unroll
+  for (int m = 0; m < N; ++m)
+    v += c[m] * (ldg(f + idx + (long long)m * nz + m) - ldg(f + idx - (long long)(m + 1) * nz - (m + 1)));
+  return v;
+}
+// Drz2bm f[i-m-1, j+m] - f[i+m, j-m-1]
+template <typename T, int N>
+__device__ __forceinline__ T drz_bm(const T* f, long long idx, int nz, const T* c) {
+  T v = 0;
+#pragma unroll
+  for (int m = 0; m < N; ++m)
+    v += c[m] * (ldg(f + idx - (long long)(m + 1) * nz + m) - ldg(f + idx + (long long)m * nz - (m + 1)));
+  return v;
+}
+
+// memory-variable pointers
+template <typename T>
+__device__ __forceinline__ T* mx(const P2<T>& p, int comp, int xi, int j) {
+  return p.mem[0] + comp * p.mcomp[0] + (long long)xi * p.nz + j;
+}
+template <typename T>
+__device__ __forceinline__ T* mz(const P2<T>& p, int comp, int i, int zj) {
+  return p.mem[1] + comp * p.mcomp[1] + (long long)i * p.sn[1] + zj;
+}
+
+// ---------------------------------------------------------------------------
+template <typename T, int N, int SCHEME>
+__global__ void __launch_bounds__(T2Z * T2X)
+k2_velocity(const __grid_constant__ P2<T> p, int it, T amp, int src_here) {
+  const int j = blockIdx.x * T2Z + threadIdx.x;
+  const int i = blockIdx.y * T2X + threadIdx.y;
+  const int nx = p.nx, nz = p.nz;
+  if (i >= nx || j >= nz) return;
+  const long long idx = (long long)i * nz + j;
+  const T dx = p.dx, dz = p.dz, dt = p.dt;
+  T c[N];
+#pragma unroll
+  for (int m = 0; m < N; ++m) c[m] = p.c[m];
+  const T* sxx = p.f[2];
+  const T* szz = p.f[3];
+  const T* sxz = p.f[4];
+  T* vx = p.f[0];
+  T* vz = p.f[1];
+  const T* rho = p.rho;
+  const T* cfx = p.cf[0];
+  const T* cfz = p.cf[1];
+  const int xi = slab_index(i, nx, p.lo[0], p.hi[0]);
+  const int zj = slab_index(j, nz, p.lo[1], p.hi[1]);
+  const uint8_t fx = p.fl[0][i], fz = p.fl[1][j];
+  const bool any_slab = (xi >= 0 || zj >= 0);
+
+  if (SCHEME == SW2D_SSG_VS) {
+    // vx at (i, j): :144-154
+    if (i >= N + 1 && i < nx - N && j >= N + 1 && j < nz - N) {
+      T dsxxdx = dx_bm<T, N>(sxx, idx, nz, c) / dx;
+      T dsxzdz = dz_bm<T, N>(sxz, idx, c) / dz;
+      if (any_slab && ((fx & 1) || (fz & 1))) {
+        if (xi >= 0) pml2(mx(p, 0, xi, j), cfx[CB * nx + i], cfx[CA * nx + i], cfx[CK * nx + i], dsxxdx);
+        if (zj >= 0) pml2(mz(p, 0, i, zj), cfz[CB * nz + j], cfz[CA * nz + j], cfz[CK * nz + j], dsxzdz);
+      }
+      T t = (dsxxdx + dsxzdz) * dt;
+      t = t / ldg(rho + idx);
+      vx[idx] = vx[idx] + t;
+    }
+    // vz at (i+1/2, j+1/2): :156-167, then the source :170
+    const bool upd = i >= N && i < nx - N - 1 && j >= N && j < nz - N - 1;
+    const bool src = src_here && i == p.si && j == p.sk;
+    if (upd || src) {
+      T v = vz[idx];
+      if (upd) {
+        const T rh = (T)0.25 * (ldg(rho + idx) + ldg(rho + idx + 1) + ldg(rho + idx + nz + 1) + ldg(rho + idx + nz));
+        T dsxzdx = dx_fm<T, N>(sxz, idx, nz, c) / dx;
+        T dszzdz = dz_fm<T, N>(szz, idx, c) / dz;
+        if (any_slab && ((fx & 2) || (fz & 2))) {
+          if (xi >= 0) pml2(mx(p, 1, xi, j), cfx[CBH * nx + i], cfx[CAH * nx + i], cfx[CKH * nx + i], dsxzdx);
+          if (zj >= 0) pml2(mz(p, 1, i, zj), cfz[CBH * nz + j], cfz[CAH * nz + j], cfz[CKH * nz + j], dszzdz);
+        }
+        T t = (dszzdz + dsxzdx) * dt;
+        t = t / rh;
+        v = v + t;
+      }
+      if (src) {
+        T t = dt * p.wav[it];
+        t = t / ldg(rho + idx);
+        v = v + t;
+      }
+      vz[idx] = v;
+    }
+  } else if (SCHEME == SW2D_SSG_SV) {
+    // vx at (i+1/2, j): :218-229, then the source :245
+    const bool upd = i >= N && i < nx - N - 1 && j >= N + 1 && j < nz - N;
+    const bool src = src_here && i == p.si && j == p.sk;
+    if (upd || src) {
+      T v = vx[idx];
+      if (upd) {
+        T dsxxdx = dx_fm<T, N>(sxx, idx, nz, c) / dx;
+        T dsxzdz = dz_bm<T, N>(sxz, idx, c) / dz;
+        const T rhx = (ldg(rho + idx) + ldg(rho + idx + nz)) / (T)2;
+        if (any_slab && ((fx & 2) || (fz & 1))) {
+          if (xi >= 0) pml2(mx(p, 0, xi, j), cfx[CBH * nx + i], cfx[CAH * nx + i], cfx[CKH * nx + i], dsxxdx);
+          if (zj >= 0) pml2(mz(p, 0, i, zj), cfz[CB * nz + j], cfz[CA * nz + j], cfz[CK * nz + j], dsxzdz);
+        }
+        T t = (dsxxdx + dsxzdz) * dt;
+        t = t / rhx;
+        v = v + t;
+      }
+      if (src) {
+        T t = dt * p.wav[it];
+        t = t / ldg(rho + idx);
+        v = v + t;
+      }
+      vx[idx] = v;
+    }
+    // vz at (i, j+1/2): :231-242
+    if (i >= N + 1 && i < nx - N && j >= N && j < nz - N - 1) {
+      const T rhz = (T)0.5 * (ldg(rho + idx) + ldg(rho + idx + 1));
+      T dsxzdx = dx_bm<T, N>(sxz, idx, nz, c) / dx;
+      T dszzdz = dz_fm<T, N>(szz, idx, c) / dz;
+      if (any_slab && ((fx & 1) || (fz & 2))) {
+        if (xi >= 0) pml2(mx(p, 1, xi, j), cfx[CB * nx + i], cfx[CA * nx + i], cfx[CK * nx + i], dsxzdx);
+        if (zj >= 0) pml2(mz(p, 1, i, zj), cfz[CBH * nz + j], cfz[CAH * nz + j], cfz[CKH * nz + j], dszzdz);
+      }
+      T t = (dszzdz + dsxzdx) * dt;
+      t = t / rhz;
+      vz[idx] = vz[idx] + t;
+    }
+  } else {  // SW2D_RSG, :292-323
+    const bool upd = i >= N + 1 && i < nx - N && j >= N + 1 && j < nz - N;
+    const bool src = src_here && (i == p.si || i == p.si - 1) && (j == p.sk || j == p.sk - 1);
+    if (upd) {
+      const T dsxxrx = drx_bm<T, N>(sxx, idx, nz, c), dsxxrz = drz_bm<T, N>(sxx, idx, nz, c);
+      const T dszzrx = drx_bm<T, N>(szz, idx, nz, c), dszzrz = drz_bm<T, N>(szz, idx, nz, c);
+      const T dsxzrx = drx_bm<T, N>(sxz, idx, nz, c), dsxzrz = drz_bm<T, N>(sxz, idx, nz, c);
+      T dsxxdx = (dsxxrz - dsxxrx) / ((T)2 * dx);
+      T dszzdz = (dszzrz + dszzrx) / ((T)2 * dz);
+      T dsxzdx = (dsxzrz - dsxzrx) / ((T)2 * dx);
+      T dsxzdz = (dsxzrz + dsxzrx) / ((T)2 * dz);
+      const T rh = ldg(rho + idx);
+      if (any_slab && ((fx & 1) || (fz & 1))) {
+        if (xi >= 0) {
+          pml2(mx(p, 0, xi, j), cfx[CB * nx + i], cfx[CA * nx + i], cfx[CK * nx + i], dsxxdx);
+          pml2(mx(p, 1, xi, j), cfx[CB * nx + i], cfx[CA * nx + i], cfx[CK * nx + i], dsxzdx);
+        }
+        if (zj >= 0) {
+          pml2(mz(p, 1, i, zj), cfz[CB * nz + j], cfz[CA * nz + j], cfz[CK * nz + j], dszzdz);
+          pml2(mz(p, 0, i, zj), cfz[CB * nz + j], cfz[CA * nz + j], cfz[CK * nz + j], dsxzdz);
+        }
+      }
+      T t = (dsxxdx + dsxzdz) * dt;
+      t = t / rh;
+      vx[idx] = vx[idx] + t;
+      T u = (dszzdz + dsxzdx) * dt;
+      u = u / rh;
+      T v = vz[idx] + u;
+      if (src) {
+        T s = dt * amp;
+        s = s / ((T)8 * rh);
+        v = v + s;
+      }
+      vz[idx] = v;
+    } else if (src) {
+      T s = dt * amp;
+      s = s / ((T)8 * ldg(rho + idx));
+      vz[idx] = vz[idx] + s;
+    }
+  }
+}
+
+template <typename T, int N, int SCHEME>
+__global__ void __launch_bounds__(T2Z * T2X)
+k2_stress(const __grid_constant__ P2<T> p, int it) {
+  // receivers of the velocity fields (final for this step, not written here)
+  {
+    const long long b = blockIdx.x + (long long)gridDim.x * blockIdx.y;
+    const long long r = b * (T2Z * T2X) + threadIdx.y * T2Z + threadIdx.x;
+    if (r < p.nrec) store_rec(p.rec_data, p.rec_f64, (long long)it * p.nrec + r, p.f[p.rec_field][p.rec_idx[r]]);
+  }
+  const int j = blockIdx.x * T2Z + threadIdx.x;
+  const int i = blockIdx.y * T2X + threadIdx.y;
+  const int nx = p.nx, nz = p.nz;
+  if (i >= nx || j >= nz) return;
+  const long long idx = (long long)i * nz + j;
+  const T dx = p.dx, dz = p.dz, dt = p.dt;
+  T c[N];
+#pragma unroll
+  for (int m = 0; m < N; ++m) c[m] = p.c[m];
+  const T* vx = p.f[0];
+  const T* vz = p.f[1];
+  T* sxx = p.f[2];
+  T* szz = p.f[3];
+  T* sxz = p.f[4];
+  const T* lam = p.lam;
+  const T* mu = p.mu;
+  const T* cfx = p.cf[0];
+  const T* cfz = p.cf[1];
+  const int xi = slab_index(i, nx, p.lo[0], p.hi[0]);
+  const int zj = slab_index(j, nz, p.lo[1], p.hi[1]);
+  const uint8_t fx = p.fl[0][i], fz = p.fl[1][j];
+  const bool any_slab = (xi >= 0 || zj >= 0);
+
+  if (SCHEME == SW2D_SSG_VS) {
+    // sxx szz at (i+1/2, j): :172-186
+    if (i >= N && i < nx - N - 1 && j >= N + 1 && j < nz - N) {
+      const T lhx = (T)0.5 * (ldg(lam + idx) + ldg(lam + idx + nz));
+      const T mhx = (T)0.5 * (ldg(mu + idx) + ldg(mu + idx + nz));
+      const T lpm = lhx + (T)2 * mhx;
+      T dvxdx = dx_fm<T, N>(vx, idx, nz, c) / dx;
+      T dvzdz = dz_bm<T, N>(vz, idx, c) / dz;
+      if (any_slab && ((fx & 2) || (fz & 1))) {
+        if (xi >= 0) pml2(mx(p, 2, xi, j), cfx[CBH * nx + i], cfx[CAH * nx + i], cfx[CKH * nx + i], dvxdx);
+        if (zj >= 0) pml2(mz(p, 2, i, zj), cfz[CB * nz + j], cfz[CA * nz + j], cfz[CK * nz + j], dvzdz);
+      }
+      sxx[idx] = sxx[idx] + (lpm * dvxdx + lhx * dvzdz) * dt;
+      szz[idx] = szz[idx] + (lpm * dvzdz + lhx * dvxdx) * dt;
+    }
+    // sxz at (i, j+1/2): :188-199
+    if (i >= N + 1 && i < nx - N && j >= N && j < nz - N - 1) {
+      const T mhz = (T)0.5 * (ldg(mu + idx + 1) + ldg(mu + idx));
+      T dvzdx = dx_bm<T, N>(vz, idx, nz, c) / dx;
+      T dvxdz = dz_fm<T, N>(vx, idx, c) / dz;
+      if (any_slab && ((fx & 1) || (fz & 2))) {
+        if (xi >= 0) pml2(mx(p, 3, xi, j), cfx[CB * nx + i], cfx[CA * nx + i], cfx[CK * nx + i], dvzdx);
+        if (zj >= 0) pml2(mz(p, 3, i, zj), cfz[CBH * nz + j], cfz[CAH * nz + j], cfz[CKH * nz + j], dvxdz);
+      }
+      sxz[idx] = sxz[idx] + mhz * (dvxdz + dvzdx) * dt;
+    }
+  } else if (SCHEME == SW2D_SSG_SV) {
+    // sxx szz at (i, j): :247-260
+    if (i >= N + 1 && i < nx - N && j >= N + 1 && j < nz - N) {
+      const T lm = ldg(lam + idx);
+      const T lpm = ldg(lam + idx) + (T)2 * ldg(mu + idx);
+      T dvxdx = dx_bm<T, N>(vx, idx, nz, c) / dx;
+      T dvzdz = dz_bm<T, N>(vz, idx, c) / dz;
+      if (any_slab && ((fx & 1) || (fz & 1))) {
+        if (xi >= 0) pml2(mx(p, 2, xi, j), cfx[CB * nx + i], cfx[CA * nx + i], cfx[CK * nx + i], dvxdx);
+        if (zj >= 0) pml2(mz(p, 2, i, zj), cfz[CB * nz + j], cfz[CA * nz + j], cfz[CK * nz + j], dvzdz);
+      }
+      sxx[idx] = sxx[idx] + (lpm * dvxdx + lm * dvzdz) * dt;
+      szz[idx] = szz[idx] + (lpm * dvzdz + lm * dvxdx) * dt;
+    }
+    // sxz at (i+1/2, j+1/2): :262-273
+    if (i >= N + 1 && i < nx - N && j >= N + 1 && j < nz - N) {
+      const T m4 = (T)0.25 * (ldg(mu + idx + 1) + ldg(mu + idx) + ldg(mu + idx + nz + 1) + ldg(mu + idx + nz));
+      T dvzdx = dx_fm<T, N>(vz, idx, nz, c) / dx;
+      T dvxdz = dz_fm<T, N>(vx, idx, c) / dz;
+      if (any_slab && ((fx & 2) || (fz & 2))) {
+        if (xi >= 0) pml2(mx(p, 3, xi, j), cfx[CBH * nx + i], cfx[CAH * nx + i], cfx[CKH * nx + i], dvzdx);
+        if (zj >= 0) pml2(mz(p, 3, i, zj), cfz[CBH * nz + j], cfz[CAH * nz + j], cfz[CKH * nz + j], dvxdz);
+      }
+      sxz[idx] = sxz[idx] + m4 * (dvxdz + dvzdx) * dt;
+    }
+  } else {  // RSG :326-353
+    if (i >= N && i < nx - N - 1 && j >= N && j < nz - N - 1) {
+      const T lm = ldg(lam + idx), u = ldg(mu + idx);
+      const T lpm = lm + (T)2 * u;
+      const T dvxrx = drx_fm<T, N>(vx, idx, nz, c), dvxrz = drz_fm<T, N>(vx, idx, nz, c);
+      const T dvzrx = drx_fm<T, N>(vz, idx, nz, c), dvzrz = drz_fm<T, N>(vz, idx, nz, c);
+      T dvxdx = (dvxrz - dvxrx) / ((T)2 * dx);
+      T dvxdz = (dvxrz + dvxrx) / ((T)2 * dz);
+      T dvzdx = (dvzrz - dvzrx) / ((T)2 * dx);
+      T dvzdz = (dvzrz + dvzrx) / ((T)2 * dz);
+      if (any_slab && ((fx & 2) || (fz & 2))) {
+        if (xi >= 0) {
+          pml2(mx(p, 2, xi, j), cfx[CBH * nx + i], cfx[CAH * nx + i], cfx[CKH * nx + i], dvxdx);
+          pml2(mx(p, 3, xi, j), cfx[CBH * nx + i], cfx[CAH * nx + i], cfx[CKH * nx + i], dvzdx);
+        }
+        if (zj >= 0) {
+          pml2(mz(p, 3, i, zj), cfz[CBH * nz + j], cfz[CAH * nz + j], cfz[CKH * nz + j], dvxdz);
+          pml2(mz(p, 2, i, zj), cfz[CBH * nz + j], cfz[CAH * nz + j], cfz[CKH * nz + j], dvzdz);
+        }
+      }
+      sxx[idx] = sxx[idx] + (lpm * dvxdx + lm * dvzdz) * dt;
+      szz[idx] = szz[idx] + (lpm * dvzdz + lm * dvxdx) * dt;
+      sxz[idx] = sxz[idx] + (u * (dvxdz + dvzdx)) * dt;
+    }
+  }
+}
+
+template <typename T>
+__global__ void k2_gather(const __grid_constant__ P2<T> p, int it) {
+  const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r < p.nrec) store_rec(p.rec_data, p.rec_f64, (long long)it * p.nrec + r, p.f[p.rec_field][p.rec_idx[r]]);
+}
+
+template <typename T, int N, int S>
+static cudaError_t launch2(const P2<T>& p, int it, T amp, bool gather_in_stress, cudaStream_t st) {
+  dim3 block(T2Z, T2X);
+  dim3 grid((p.nz + T2Z - 1) / T2Z, (p.nx + T2X - 1) / T2X);
+  k2_velocity<T, N, S><<<grid, block, 0, st>>>(p, it, amp, p.src_kind != SW_SRC_NONE ? 1 : 0);
+  P2<T> q = p;
+  if (!gather_in_stress) q.nrec = 0;
+  k2_stress<T, N, S><<<grid, block, 0, st>>>(q, it);
+  if (!gather_in_stress && p.nrec > 0) k2_gather<T><<<(p.nrec + 255) / 256, 256, 0, st>>>(p, it);
+  return cudaGetLastError();
+}
+
+template <typename T, int S>
+static cudaError_t dispatch2(const P2<T>& p, int order, int it, T amp, bool g, cudaStream_t st) {
+  switch (order) {
+    case 1: return launch2<T, 1, S>(p, it, amp, g, st);
+    case 2: return launch2<T, 2, S>(p, it, amp, g, st);
+    case 3: return launch2<T, 3, S>(p, it, amp, g, st);
+    case 4: return launch2<T, 4, S>(p, it, amp, g, st);
+    case 5: return launch2<T, 5, S>(p, it, amp, g, st);
+    case 6: return launch2<T, 6, S>(p, it, amp, g, st);
+    case 7: return launch2<T, 7, S>(p, it, amp, g, st);
+    case 8: return launch2<T, 8, S>(p, it, amp, g, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <typename T>
+cudaError_t sw2_step(const P2<T>& p, int scheme, int order, int it, T amp, bool gather_in_stress,
+                     cudaStream_t st) {
+  if (scheme == SW2D_SSG_VS) return dispatch2<T, SW2D_SSG_VS>(p, order, it, amp, gather_in_stress, st);
+  if (scheme == SW2D_SSG_SV) return dispatch2<T, SW2D_SSG_SV>(p, order, it, amp, gather_in_stress, st);
+  return dispatch2<T, SW2D_RSG>(p, order, it, amp, gather_in_stress, st);
+}
+
+template cudaError_t sw2_step<float>(const P2<float>&, int, int, int, float, bool, cudaStream_t);
+template cudaError_t sw2_step<double>(const P2<double>&, int, int, int, double, bool, cudaStream_t);
+
+}  // namespace sw

@@ -1,0 +1,278 @@
+// elastic3d_spml.cu -- 3D staggered-grid kernels with the split-field PML of
+// src/Elastic3D_SSG_SPML.py:160-393 (update_SSG_SPML).
+//
+// Inside the PML predicate each component is advanced as split parts
+//   psi_d <- ((1 - dt/2 d) psi_d + dt * term_d) / (1 + dt/2 d)
+// and the field is set to their sum; outside it the plain update is used.
+// The 24 split fields are full-grid arrays (split[24][nx][ny][nz]) that are
+// only touched inside the PML region.  One thread per cell, block 32 (z) x 8
+// (y), one x plane per blockIdx.z.
+#include "sw_device.cuh"
+
+namespace sw {
+
+constexpr int TSZ = 32;
+constexpr int TSY = 8;
+
+// split-field order (reference names)
+enum {
+  PVX_X = 0, PVX_Y, PVX_Z, PVY_X, PVY_Y, PVY_Z, PVZ_X, PVZ_Y, PVZ_Z,
+  PSXX_X, PSXX_Y, PSXX_Z, PSYY_X, PSYY_Y, PSYY_Z,
+  PSXY_X, PSXY_Y, PSXZ_X, PSXZ_Z, PSYZ_Y, PSYZ_Z,
+  PSZZ_X, PSZZ_Y, PSZZ_Z
+};
+
+template <typename T, int N>
+__device__ __forceinline__ T d_fm(const T* f, long long idx, long long s, const T* c) {
+  T v = 0;
+#pragma unroll
+  for (int m = 0; m < N; ++m) v += c[m] * (ldg(f + idx + (m + 1) * s) - ldg(f + idx - m * s));
+  return v;
+}
+template <typename T, int N>
+__device__ __forceinline__ T d_bm(const T* f, long long idx, long long s, const T* c) {
+  T v = 0;
+#pragma unroll
+  for (int m = 0; m < N; ++m) v += c[m] * (ldg(f + idx + m * s) - ldg(f + idx - (m + 1) * s));
+  return v;
+}
+
+template <typename T, int N>
+__global__ void __launch_bounds__(TSZ * TSY)
+ks_velocity(const __grid_constant__ P3<T> p, int it, int src_here) {
+  const int k = blockIdx.x * TSZ + threadIdx.x;
+  const int j = blockIdx.y * TSY + threadIdx.y;
+  const int i = blockIdx.z;
+  const int nx = p.nx, ny = p.ny, nz = p.nz;
+  if (j >= ny || k >= nz) return;
+  const long long sx = (long long)ny * nz, sy = nz;
+  const long long idx = (long long)i * sx + (long long)j * nz + k;
+  const long long G = (long long)nx * sx;
+  const T dx = p.dx, dy = p.dy, dz = p.dz, dt = p.dt;
+  const T hdt = (T)0.5 * dt;
+  T c[N];
+#pragma unroll
+  for (int m = 0; m < N; ++m) c[m] = p.c[m];
+  const T *sxx = p.f[3], *syy = p.f[4], *szz = p.f[5], *sxy = p.f[6], *sxz = p.f[7], *syz = p.f[8];
+  T *vx = p.f[0], *vy = p.f[1], *vz = p.f[2];
+  T* sp = p.split;
+  const T *rho = p.rho, *dpx = p.dmp[0], *dpy = p.dmp[1], *dpz = p.dmp[2];
+  const uint8_t fx = p.fl[0][i], fy = p.fl[1][j], fz = p.fl[2][k];
+
+  // vx :182-205
+  if (i >= N && i < nx - N - 1 && j >= N + 1 && j < ny - N && k >= N + 1 && k < nz - N) {
+    T dsxxdx = d_fm<T, N>(sxx, idx, sx, c) / dx;
+    T dsxydy = d_bm<T, N>(sxy, idx, sy, c) / dy;
+    T dsxzdz = d_bm<T, N>(sxz, idx, 1, c) / dz;
+    const T rh = ldg(rho + idx);
+    const T ro = (T)1 / rh;
+    if ((fx & 2) || (fy & 1) || (fz & 1)) {
+      const T xn = (T)1 - hdt * dpx[nx + i], yn = (T)1 - hdt * dpy[j], zn = (T)1 - hdt * dpz[k];
+      const T xd = (T)1 + hdt * dpx[nx + i], yd = (T)1 + hdt * dpy[j], zd = (T)1 + hdt * dpz[k];
+      T a = (xn * sp[PVX_X * G + idx] + dsxxdx * dt * ro) / xd;
+      T b = (yn * sp[PVX_Y * G + idx] + dsxydy * dt * ro) / yd;
+      T cc = (zn * sp[PVX_Z * G + idx] + dsxzdz * dt * ro) / zd;
+      sp[PVX_X * G + idx] = a;
+      sp[PVX_Y * G + idx] = b;
+      sp[PVX_Z * G + idx] = cc;
+      vx[idx] = a + b + cc;
+    } else {
+      vx[idx] = vx[idx] + (dsxxdx + dsxydy + dsxzdz) * dt * ro;
+    }
+  }
+  // vy :209-233
+  if (i >= N + 1 && i < nx - N && j >= N && j < ny - N - 1 && k >= N + 1 && k < nz - N) {
+    const T rhy = (T)0.5 * (ldg(rho + idx) + ldg(rho + idx + sy));
+    const T ro = (T)1 / rhy;
+    T dsxydx = d_bm<T, N>(sxy, idx, sx, c) / dx;
+    T dsyydy = d_fm<T, N>(syy, idx, sy, c) / dy;
+    T dsyzdz = d_bm<T, N>(syz, idx, 1, c) / dz;
+    if ((fx & 1) || (fy & 2) || (fz & 1)) {
+      const T xn = (T)1 - hdt * dpx[i], yn = (T)1 - hdt * dpy[ny + j], zn = (T)1 - hdt * dpz[k];
+      const T xd = (T)1 + hdt * dpx[i], yd = (T)1 + hdt * dpy[ny + j], zd = (T)1 + hdt * dpz[k];
+      T a = (xn * sp[PVY_X * G + idx] + dt * dsxydx * ro) / xd;
+      T b = (yn * sp[PVY_Y * G + idx] + dt * dsyydy * ro) / yd;
+      T cc = (zn * sp[PVY_Z * G + idx] + dt * dsyzdz * ro) / zd;
+      sp[PVY_X * G + idx] = a;
+      sp[PVY_Y * G + idx] = b;
+      sp[PVY_Z * G + idx] = cc;
+      vy[idx] = a + b + cc;
+    } else {
+      vy[idx] = vy[idx] + (dsxydx + dsyydy + dsyzdz) * dt * ro;
+    }
+  }
+  // vz :235-259, then the source :294
+  const bool upd = i >= N + 1 && i < nx - N && j >= N + 1 && j < ny - N && k >= N && k < nz - N - 1;
+  const bool src = src_here && i == p.si && j == p.sj && k == p.sk;
+  if (upd || src) {
+    T v = vz[idx];
+    if (upd) {
+      const T r4 = (T)0.25 * (ldg(rho + idx) + ldg(rho + idx + sy) + ldg(rho + idx + sx + sy) + ldg(rho + idx + sx));
+      const T ro = (T)1 / r4;
+      T dsxzdx = d_bm<T, N>(sxz, idx, sx, c) / dx;
+      T dsyzdy = d_bm<T, N>(syz, idx, sy, c) / dy;
+      T dszzdz = d_fm<T, N>(szz, idx, 1, c) / dz;
+      if ((fx & 1) || (fy & 1) || (fz & 2)) {
+        const T xn = (T)1 - hdt * dpx[i], yn = (T)1 - hdt * dpy[j], zn = (T)1 - hdt * dpz[nz + k];
+        const T xd = (T)1 + hdt * dpx[i], yd = (T)1 + hdt * dpy[j], zd = (T)1 + hdt * dpz[nz + k];
+        T a = (xn * sp[PVZ_X * G + idx] + dt * dsxzdx * ro) / xd;
+        T b = (yn * sp[PVZ_Y * G + idx] + dt * dsyzdy * ro) / yd;
+        T cc = (zn * sp[PVZ_Z * G + idx] + dt * dszzdz * ro) / zd;
+        sp[PVZ_X * G + idx] = a;
+        sp[PVZ_Y * G + idx] = b;
+        sp[PVZ_Z * G + idx] = cc;
+        v = a + b + cc;
+      } else {
+        v = v + (dsxzdx + dsyzdy + dszzdz) * dt * ro;
+      }
+    }
+    if (src) {
+      T t = dt * p.wav[it];
+      t = t / ldg(rho + idx);
+      v = v + t;
+    }
+    vz[idx] = v;
+  }
+}
+
+template <typename T, int N>
+__global__ void __launch_bounds__(TSZ * TSY)
+ks_stress(const __grid_constant__ P3<T> p, int it) {
+  {
+    const long long b = blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z);
+    const long long r = b * (TSZ * TSY) + threadIdx.y * TSZ + threadIdx.x;
+    if (r < p.nrec) store_rec(p.rec_data, p.rec_f64, (long long)it * p.nrec + r, p.f[p.rec_field][p.rec_idx[r]]);
+  }
+  const int k = blockIdx.x * TSZ + threadIdx.x;
+  const int j = blockIdx.y * TSY + threadIdx.y;
+  const int i = blockIdx.z;
+  const int nx = p.nx, ny = p.ny, nz = p.nz;
+  if (j >= ny || k >= nz) return;
+  const long long sx = (long long)ny * nz, sy = nz;
+  const long long idx = (long long)i * sx + (long long)j * nz + k;
+  const long long G = (long long)nx * sx;
+  const T dx = p.dx, dy = p.dy, dz = p.dz, dt = p.dt;
+  const T hdt = (T)0.5 * dt;
+  T c[N];
+#pragma unroll
+  for (int m = 0; m < N; ++m) c[m] = p.c[m];
+  const T *vx = p.f[0], *vy = p.f[1], *vz = p.f[2];
+  T *sxx = p.f[3], *syy = p.f[4], *szz = p.f[5], *sxy = p.f[6], *sxz = p.f[7], *syz = p.f[8];
+  T* sp = p.split;
+  const T *lam = p.lam, *mu = p.mu, *dpx = p.dmp[0], *dpy = p.dmp[1], *dpz = p.dmp[2];
+  const uint8_t fx = p.fl[0][i], fy = p.fl[1][j], fz = p.fl[2][k];
+
+  // normal stresses :296-333
+  if (i >= N + 1 && i < nx - N && j >= N + 1 && j < ny - N && k >= N + 1 && k < nz - N) {
+    const T lm = ldg(lam + idx), u = ldg(mu + idx);
+    const T l2m = lm + (T)2 * u;
+    T dvxdx = d_bm<T, N>(vx, idx, sx, c) / dx;
+    T dvydy = d_bm<T, N>(vy, idx, sy, c) / dy;
+    T dvzdz = d_bm<T, N>(vz, idx, 1, c) / dz;
+    if ((fx | fy | fz) & 1) {
+      const T xn = (T)1 - hdt * dpx[i], yn = (T)1 - hdt * dpy[j], zn = (T)1 - hdt * dpz[k];
+      const T xd = (T)1 + hdt * dpx[i], yd = (T)1 + hdt * dpy[j], zd = (T)1 + hdt * dpz[k];
+      T xx = (xn * sp[PSXX_X * G + idx] + dt * l2m * dvxdx) / xd;
+      T xy = (yn * sp[PSXX_Y * G + idx] + dt * lm * dvydy) / yd;
+      T xz = (zn * sp[PSXX_Z * G + idx] + dt * lm * dvzdz) / zd;
+      T yx = (xn * sp[PSYY_X * G + idx] + dt * lm * dvxdx) / xd;
+      T yy = (yn * sp[PSYY_Y * G + idx] + dt * l2m * dvydy) / yd;
+      T yz = (zn * sp[PSYY_Z * G + idx] + dt * lm * dvzdz) / zd;
+      T zx = (xn * sp[PSZZ_X * G + idx] + dt * lm * dvxdx) / xd;
+      T zy = (yn * sp[PSZZ_Y * G + idx] + dt * lm * dvydy) / yd;
+      T zz = (zn * sp[PSZZ_Z * G + idx] + dt * l2m * dvzdz) / zd;
+      sp[PSXX_X * G + idx] = xx; sp[PSXX_Y * G + idx] = xy; sp[PSXX_Z * G + idx] = xz;
+      sp[PSYY_X * G + idx] = yx; sp[PSYY_Y * G + idx] = yy; sp[PSYY_Z * G + idx] = yz;
+      sp[PSZZ_X * G + idx] = zx; sp[PSZZ_Y * G + idx] = zy; sp[PSZZ_Z * G + idx] = zz;
+      sxx[idx] = xx + xy + xz;
+      syy[idx] = yx + yy + yz;
+      szz[idx] = zx + zy + zz;
+    } else {
+      sxx[idx] = sxx[idx] + (l2m * dvxdx + lm * (dvzdz + dvydy)) * dt;
+      syy[idx] = syy[idx] + (l2m * dvydy + lm * (dvxdx + dvzdz)) * dt;
+      szz[idx] = szz[idx] + (l2m * dvzdz + lm * (dvxdx + dvydy)) * dt;
+    }
+  }
+  // sxy :334-350
+  if (i >= N + 1 && i < nx - N && j >= N + 1 && j < ny - N && k >= N && k < nz - N) {
+    const T m4 = (T)0.25 * (ldg(mu + idx + sy) + ldg(mu + idx) + ldg(mu + idx) + ldg(mu + idx + sx));
+    T dvydx = d_fm<T, N>(vy, idx, sx, c) / dx;
+    T dvxdy = d_fm<T, N>(vx, idx, sy, c) / dy;
+    if ((fx & 2) || (fy & 2) || (fz & 1)) {
+      const T xn = (T)1 - hdt * dpx[nx + i], yn = (T)1 - hdt * dpy[ny + j];
+      const T xd = (T)1 + hdt * dpx[nx + i], yd = (T)1 + hdt * dpy[ny + j];
+      T a = (xn * sp[PSXY_X * G + idx] + dt * m4 * dvydx) / xd;
+      T b = (yn * sp[PSXY_Y * G + idx] + dt * m4 * dvxdy) / yd;
+      sp[PSXY_X * G + idx] = a;
+      sp[PSXY_Y * G + idx] = b;
+      sxy[idx] = a + b;
+    } else {
+      sxy[idx] = sxy[idx] + m4 * (dvxdy + dvydx) * dt;
+    }
+  }
+  // sxz :352-371
+  if (i >= N && i < nx - N - 1 && j >= N && j < ny - N && k >= N && k < nz - N - 1) {
+    const T m4 = (T)0.25 * (ldg(mu + idx) + ldg(mu + idx + sx) + ldg(mu + idx) + ldg(mu + idx + sy));
+    T dvzdx = d_fm<T, N>(vz, idx, sx, c) / dx;
+    T dvxdz = d_fm<T, N>(vx, idx, 1, c) / dz;
+    if ((fx & 2) || (fy & 1) || (fz & 2)) {
+      const T xn = (T)1 - hdt * dpx[nx + i], zn = (T)1 - hdt * dpz[nz + k];
+      const T xd = (T)1 + hdt * dpx[nx + i], zd = (T)1 + hdt * dpz[nz + k];
+      T a = (xn * sp[PSXZ_X * G + idx] + dt * m4 * dvzdx) / xd;
+      T b = (zn * sp[PSXZ_Z * G + idx] + dt * m4 * dvxdz) / zd;
+      sp[PSXZ_X * G + idx] = a;
+      sp[PSXZ_Z * G + idx] = b;
+      sxz[idx] = a + b;
+    } else {
+      sxz[idx] = sxz[idx] + m4 * (dvxdz + dvzdx) * dt;
+    }
+  }
+  // syz :373-391
+  if (i >= N && i < nx - N && j >= N && j < ny - N - 1 && k >= N && k < nz - N - 1) {
+    const T m4 = (T)0.25 * (ldg(mu + idx + sy) + ldg(mu + idx) + ldg(mu + idx + 1) + ldg(mu + idx));
+    T dvzdy = d_fm<T, N>(vz, idx, sy, c) / dy;
+    T dvydz = d_fm<T, N>(vy, idx, 1, c) / dz;
+    if ((fx & 1) || (fy & 2) || (fz & 2)) {
+      const T yn = (T)1 - hdt * dpy[ny + j], zn = (T)1 - hdt * dpz[nz + k];
+      const T yd = (T)1 + hdt * dpy[ny + j], zd = (T)1 + hdt * dpz[nz + k];
+      T a = (yn * sp[PSYZ_Y * G + idx] + dt * m4 * dvzdy) / yd;
+      T b = (zn * sp[PSYZ_Z * G + idx] + dt * m4 * dvydz) / zd;
+      sp[PSYZ_Y * G + idx] = a;
+      sp[PSYZ_Z * G + idx] = b;
+      syz[idx] = a + b;
+    } else {
+      syz[idx] = syz[idx] + m4 * (dvydz + dvzdy) * dt;
+    }
+  }
+}
+
+template <typename T, int N>
+static cudaError_t launch_spml(const P3<T>& p, int it, bool gather_in_stress, cudaStream_t st) {
+  dim3 block(TSZ, TSY);
+  dim3 grid((p.nz + TSZ - 1) / TSZ, (p.ny + TSY - 1) / TSY, p.nx);
+  ks_velocity<T, N><<<grid, block, 0, st>>>(p, it, p.src_kind != SW_SRC_NONE ? 1 : 0);
+  P3<T> q = p;
+  if (!gather_in_stress) q.nrec = 0;
+  ks_stress<T, N><<<grid, block, 0, st>>>(q, it);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t sw3_spml_step(const P3<T>& p, int order, int it, bool gather_in_stress, cudaStream_t st) {
+  switch (order) {
+    case 1: return launch_spml<T, 1>(p, it, gather_in_stress, st);
+    case 2: return launch_spml<T, 2>(p, it, gather_in_stress, st);
+    case 3: return launch_spml<T, 3>(p, it, gather_in_stress, st);
+    case 4: return launch_spml<T, 4>(p, it, gather_in_stress, st);
+    case 5: return launch_spml<T, 5>(p, it, gather_in_stress, st);
+    case 6: return launch_spml<T, 6>(p, it, gather_in_stress, st);
+    case 7: return launch_spml<T, 7>(p, it, gather_in_stress, st);
+    case 8: return launch_spml<T, 8>(p, it, gather_in_stress, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template cudaError_t sw3_spml_step<float>(const P3<float>&, int, int, bool, cudaStream_t);
+template cudaError_t sw3_spml_step<double>(const P3<double>&, int, int, bool, cudaStream_t);
+
+}  // namespace sw
