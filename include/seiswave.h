@@ -162,6 +162,23 @@ SW_API int sw3d_plan_create(const sw3d_desc* desc, sw_plan** plan);
  * (the autotuner's knob; the plan picks a default from the grid and SM count). */
 SW_API int sw_plan_set_tile(sw_plan* plan, int32_t x_chunk);
 
+/* Block until the stream is idle and report a device-side failure recorded
+ * by the plan's kernels since creation (SW_ERR_TIMEOUT: a bounded wait for
+ * TMA data gave up).  No reference counterpart (the reference has no error
+ * path); it is the status read the drivers' loops can add after run(). */
+SW_API int sw_plan_status(sw_plan* plan, void* stream);
+
+/* Describe the plan's execution path: info[0] fused single-pass kernel
+ * available, [1] constant-divisor fast path verified, [2] fused grid size,
+ * [3] fused x-chunk length, [4] two-pass x-chunk length, [5] fused path
+ * enabled.  info must hold 6 int32. */
+SW_API int sw_plan_info(sw_plan* plan, int32_t* info);
+
+/* Choose the execution path of sw_run: use_fused = 0 keeps every step on the
+ * two-pass kernels; chunk_len > 0 sets the x planes per fused work unit
+ * (the autotuner's knob). */
+SW_API int sw_plan_set_path(sw_plan* plan, int32_t use_fused, int32_t chunk_len);
+
 /* sizeof of the ABI structs as this library was compiled: which = 0
  * sw_pml_axis, 1 sw_receivers, 2 sw_source, 3 sw2d_desc, 4 sw3d_desc; -1 else.
  * Lets a binding check its struct layout without touching a GPU. */

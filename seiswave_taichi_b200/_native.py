@@ -29,7 +29,7 @@ SW_SRC_NONE, SW_SRC_FORCE, SW_SRC_MOMENT, SW_SRC_RSG4 = 0, 1, 2, 3
 EXPORTS = (
     "sw_version", "sw_last_error", "sw2d_plan_create", "sw3d_plan_create",
     "sw_plan_set_tile", "sw_abi_sizeof", "sw_plan_destroy", "sw_step", "sw_step_amp",
-    "sw_run", "sw_check_finite",
+    "sw_run", "sw_check_finite", "sw_plan_status", "sw_plan_info", "sw_plan_set_path",
 )
 
 
@@ -111,6 +111,9 @@ def load() -> C.CDLL:
         "sw_step_amp": (C.c_int, [vp, C.c_int32, C.c_double, vp]),
         "sw_run": (C.c_int, [vp, C.c_int32, C.c_int32, C.c_int32, vp]),
         "sw_check_finite": (C.c_int, [vp, vp, C.POINTER(C.c_int64)]),
+        "sw_plan_status": (C.c_int, [vp, vp]),
+        "sw_plan_info": (C.c_int, [vp, C.POINTER(C.c_int32)]),
+        "sw_plan_set_path": (C.c_int, [vp, C.c_int32, C.c_int32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -184,6 +187,19 @@ class Plan:
         if rc not in (SW_OK, SW_ERR_NONFINITE):
             check(rc)
         return int(n.value)
+
+    def status(self, stream: int = 0) -> None:
+        """Synchronize and raise if a kernel recorded a device-side failure."""
+        check(load().sw_plan_status(self._h, C.c_void_p(stream)))
+
+    def info(self) -> dict:
+        a = (C.c_int32 * 6)()
+        check(load().sw_plan_info(self._h, a))
+        return {"fused": bool(a[0]), "fast_div": bool(a[1]), "fused_grid": a[2], "fused_chunk": a[3],
+                "two_pass_chunk": a[4], "use_fused": bool(a[5])}
+
+    def set_path(self, use_fused: bool = True, chunk_len: int = 0) -> None:
+        check(load().sw_plan_set_path(self._h, 1 if use_fused else 0, int(chunk_len)))
 
     def close(self) -> None:
         if getattr(self, "_h", None) is not None and self._h.value:

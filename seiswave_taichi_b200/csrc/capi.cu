@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "sw_device.cuh"
+#include "sw_fused.cuh"
 
 namespace sw {
 template <typename T> cudaError_t sw3_velocity(const P3<T>&, int, int, bool, bool, cudaStream_t);
@@ -62,6 +63,14 @@ struct sw_plan {
   cudaGraphExec_t gexec = nullptr;
   int g_it0 = -1, g_n = -1;
   unsigned long long* d_count = nullptr;
+  // fused single-pass path (3D float CPML schemes)
+  bool fused = false;
+  int fused_N = 0, fused_grid = 0;
+  sw::FusedMaps fmaps{};
+  sw::FusedExtra fx{};
+  void* fused_buf = nullptr;
+  int* d_err = nullptr;
+  int use_fused = 1;
 };
 
 namespace {
@@ -133,6 +142,39 @@ int choose_x_chunk(int nx, int ny, int nz) {
   return xc;
 }
 
+// ---------------------------------------------------------------------------
+// constant divisors: enable div_c's Markstein path only where it equals IEEE
+// division for every finite float numerator (checked once per divisor value)
+// ---------------------------------------------------------------------------
+bool verified_divisor(float d, float r, cudaStream_t st) {
+  static std::vector<std::pair<uint32_t, bool>> cache;
+  uint32_t bits;
+  memcpy(&bits, &d, 4);
+  for (auto& e : cache)
+    if (e.first == bits) return e.second;
+  unsigned long long* dbad = nullptr;
+  unsigned long long hbad = 1;
+  bool ok = false;
+  if (cudaMalloc(&dbad, sizeof(unsigned long long)) == cudaSuccess) {
+    ok = sw::sw3_check_divisor(d, r, dbad, &hbad, st) == cudaSuccess && hbad == 0;
+    cudaFree(dbad);
+  }
+  cudaGetLastError();
+  cache.push_back({bits, ok});
+  return ok;
+}
+
+template <typename T>
+void set_divisors(T* rd, int* fast, const double* h, int n) {
+  int f = 1;
+  for (int a = 0; a < n; ++a) {
+    rd[a] = (T)1 / (T)h[a];
+    if (sizeof(T) == 4) f = f && verified_divisor((float)(T)h[a], (float)rd[a], 0);
+    else f = 0;
+  }
+  *fast = f;
+}
+
 template <typename T>
 int make_p3(sw_plan* pl, const sw3d_desc* d, sw::P3<T>& p) {
   p.nx = d->nx; p.ny = d->ny; p.nz = d->nz;
@@ -154,6 +196,8 @@ int make_p3(sw_plan* pl, const sw3d_desc* d, sw::P3<T>& p) {
   p.rec_idx = (const long long*)d->rec.index; p.rec_data = d->rec.data;
   p.rec_f64 = d->rec.dtype == SW_F64;
   p.x_chunk = choose_x_chunk(d->nx, d->ny, d->nz);
+  const double hs[3] = {d->dx, d->dy, d->dz};
+  set_divisors<T>(p.rd, &p.fast_div, hs, 3);
   (void)pl;
   return SW_OK;
 }
@@ -180,6 +224,16 @@ int make_p2(const sw2d_desc* d, sw::P2<T>& p) {
   p.nrec = d->rec.nrec; p.rec_field = d->rec.field;
   p.rec_idx = (const long long*)d->rec.index; p.rec_data = d->rec.data;
   p.rec_f64 = d->rec.dtype == SW_F64;
+  const double h1[2] = {d->dx, d->dz}, h2[2] = {2 * d->dx, 2 * d->dz};
+  int f1 = 0, f2 = 0;
+  set_divisors<T>(p.rd, &f1, h1, 2);
+  if (d->scheme == SW2D_RSG) {
+    for (int a = 0; a < 2; ++a) p.rd2[a] = (T)1 / ((T)2 * (T)h1[a]);
+    const double hh[2] = {(double)((T)2 * (T)h1[0]), (double)((T)2 * (T)h1[1])};
+    T tmp[2];
+    set_divisors<T>(tmp, &f2, hh, 2);
+  }
+  p.fast_div = f1 | (f2 << 1);
   return SW_OK;
 }
 
@@ -243,6 +297,110 @@ int check_it(sw_plan* pl, int it0, int n) {
     return fail(SW_ERR_ARG, buf);
   }
   return SW_OK;
+}
+
+
+// ---------------------------------------------------------------------------
+// fused single-pass path: second buffer set, tensor maps, divisor check
+// ---------------------------------------------------------------------------
+int choose_fused_grid(sw_plan* pl, const sw::FusedConfig& fc) {
+  const auto& p = pl->p3f;
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  auto& x = pl->fx;
+  x.tiles_y = (p.ny + fc.TY - 1) / fc.TY;
+  x.tiles_z = (p.nz + fc.tz - 1) / fc.tz;
+  const int tiles = x.tiles_y * x.tiles_z;
+  int chunks = (5 * sms + tiles - 1) / tiles;
+  if (chunks < 1) chunks = 1;
+  int len = (p.nx + chunks - 1) / chunks;
+  if (len < 4 * fc.N) len = 4 * fc.N;
+  x.chunk_len = len;
+  x.chunks = (p.nx + len - 1) / len;
+  const int units = tiles * x.chunks;
+  return units < sms ? units : sms;
+}
+
+void setup_fused(sw_plan* pl) {
+  pl->fused = false;
+  if (pl->dim != 3 || pl->dtype != SW_F32) return;
+  if (pl->scheme != SW3D_CPML_TENSOR && pl->scheme != SW3D_CPML_FORCE) return;
+  if (!pl->src_in_kernel) return;
+  sw::FusedConfig fc;
+  if (!sw::sw3_fused_config(pl->order, &fc)) return;
+  auto& p = pl->p3f;
+  const int N = pl->order;
+  if (p.nz % 4 != 0) return;
+  if (pl->src_kind == SW_SRC_MOMENT && p.si >= p.nx - N) return;
+  for (int q = 0; q < 9; ++q)
+    if (!aligned(p.f[q], 16)) return;
+  if (!aligned(p.rho, 16) || !aligned(p.lam, 16) || !aligned(p.mu, 16)) return;
+  int dev = 0, maxsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if ((size_t)maxsm < fc.smem) return;
+  // second buffer set: nine wavefields + three velocity memory-variable comps per direction
+  const size_t ncell = (size_t)p.nx * p.ny * p.nz;
+  size_t total = 9 * ncell;
+  size_t mv[3];
+  for (int d = 0; d < 3; ++d) {
+    mv[d] = 3 * (size_t)p.mcomp[d];
+    total += (mv[d] + 63) / 64 * 64;
+  }
+  float* buf = nullptr;
+  if (cudaMalloc(&buf, total * sizeof(float)) != cudaSuccess) { cudaGetLastError(); return; }
+  if (cudaMalloc(&pl->d_err, sizeof(int)) != cudaSuccess) { cudaFree(buf); cudaGetLastError(); return; }
+  cudaMemset(pl->d_err, 0, sizeof(int));
+  cudaMemset(buf, 0, total * sizeof(float));
+  auto& x = pl->fx;
+  float* cur = buf;
+  for (int q = 0; q < 9; ++q) { x.fB[q] = cur; cur += ncell; }
+  for (int d = 0; d < 3; ++d) {
+    x.memB[d] = mv[d] ? cur : nullptr;
+    cur += (mv[d] + 63) / 64 * 64;
+  }
+  x.err = pl->d_err;
+  if (!sw::sw3_fused_maps(N, p, x, &pl->fmaps)) {
+    cudaFree(buf); cudaFree(pl->d_err); pl->d_err = nullptr;
+    return;
+  }
+  pl->fused_grid = choose_fused_grid(pl, fc);
+  pl->fused_buf = buf;
+  pl->fused_N = N;
+  pl->fused = true;
+}
+
+// nsteps >= 2 steps through the fused kernel (the last one two-pass when odd)
+cudaError_t enqueue_fused_run(sw_plan* pl, int it0, int nsteps, cudaStream_t st) {
+  const auto& p = pl->p3f;
+  const bool moment = pl->src_kind == SW_SRC_MOMENT;
+  const bool tensor = pl->scheme == SW3D_CPML_TENSOR;
+  cudaError_t e;
+  if (moment) {
+    e = sw::sw3_moment_inject<float>(p, it0, st);
+    if (e != cudaSuccess) return e;
+  }
+  const int nf = nsteps & ~1;
+  for (int s = 0; s < nf; ++s) {
+    const int it = it0 + s;
+    e = sw::sw3_fused_step(pl->fused_N, tensor, p, pl->fmaps, pl->fx, pl->fused_grid, it, s & 1,
+                           moment && s < nsteps - 1, s > 0 ? it - 1 : -1, st);
+    if (e != cudaSuccess) return e;
+  }
+  // the fused steps end in the caller's buffers; record the last one's receivers
+  e = sw::sw3_gather<float>(p, it0 + nf - 1, st);
+  if (e != cudaSuccess) return e;
+  if (nsteps & 1) return enqueue3<float>(pl, p, it0 + nsteps - 1, false, true, st);
+  return cudaSuccess;
+}
+
+cudaError_t enqueue_sequence(sw_plan* pl, int it0, int nsteps, cudaStream_t st) {
+  if (pl->fused && pl->use_fused && nsteps >= 2) return enqueue_fused_run(pl, it0, nsteps, st);
+  for (int s = 0; s < nsteps; ++s) {
+    cudaError_t e = enqueue_step(pl, it0 + s, s == 0, s == nsteps - 1, false, 0.0, st);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 }  // namespace
@@ -361,6 +519,7 @@ int sw3d_plan_create(const sw3d_desc* d, sw_plan** out) {
   for (int q = 0; q < 9; ++q) pl->fields[q] = d->field[q];
   if (d->dtype == SW_F32) make_p3<float>(pl, d, pl->p3f);
   else make_p3<double>(pl, d, pl->p3d);
+  setup_fused(pl);
   *out = pl;
   return SW_OK;
 }
@@ -375,11 +534,56 @@ int sw_plan_set_tile(sw_plan* pl, int32_t x_chunk) {
   return SW_OK;
 }
 
+int sw_plan_status(sw_plan* pl, void* stream) {
+  if (!pl) return fail(SW_ERR_ARG, "null plan");
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(e, "sw_plan_status");
+  if (pl->d_err) {
+    int h = 0;
+    e = cudaMemcpy(&h, pl->d_err, sizeof h, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e, "sw_plan_status");
+    if (h) return fail(SW_ERR_TIMEOUT, "a bounded device wait gave up (TMA data never arrived)");
+  }
+  return SW_OK;
+}
+
+int sw_plan_info(sw_plan* pl, int32_t* info) {
+  if (!pl || !info) return fail(SW_ERR_ARG, "null plan or output");
+  info[0] = pl->fused ? 1 : 0;
+  info[1] = pl->dim == 3 ? (pl->dtype == SW_F32 ? pl->p3f.fast_div : 0) : (pl->dtype == SW_F32 ? pl->p2f.fast_div : 0);
+  info[2] = pl->fused ? pl->fused_grid : 0;
+  info[3] = pl->fused ? pl->fx.chunk_len : 0;
+  info[4] = pl->dim == 3 ? (pl->dtype == SW_F32 ? pl->p3f.x_chunk : pl->p3d.x_chunk) : 0;
+  info[5] = pl->use_fused;
+  return SW_OK;
+}
+
+int sw_plan_set_path(sw_plan* pl, int32_t use_fused, int32_t chunk_len) {
+  if (!pl) return fail(SW_ERR_ARG, "null plan");
+  pl->use_fused = use_fused ? 1 : 0;
+  if (chunk_len > 0 && pl->fused) {
+    sw::FusedConfig fc;
+    sw::sw3_fused_config(pl->fused_N, &fc);
+    int len = chunk_len < 2 * fc.N ? 2 * fc.N : chunk_len;
+    pl->fx.chunk_len = len;
+    pl->fx.chunks = (pl->p3f.nx + len - 1) / len;
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int units = pl->fx.tiles_y * pl->fx.tiles_z * pl->fx.chunks;
+    pl->fused_grid = units < sms ? units : sms;
+  }
+  if (pl->gexec) { cudaGraphExecDestroy(pl->gexec); pl->gexec = nullptr; pl->g_it0 = pl->g_n = -1; }
+  return SW_OK;
+}
+
 int sw_plan_destroy(sw_plan* pl) {
   if (!pl) return SW_OK;
   if (pl->gexec) cudaGraphExecDestroy(pl->gexec);
   if (pl->cap_stream) cudaStreamDestroy(pl->cap_stream);
   if (pl->d_count) cudaFree(pl->d_count);
+  if (pl->fused_buf) cudaFree(pl->fused_buf);
+  if (pl->d_err) cudaFree(pl->d_err);
   delete pl;
   return SW_OK;
 }
@@ -410,10 +614,8 @@ int sw_run(sw_plan* pl, int32_t it0, int32_t nsteps, int32_t use_graph, void* st
   cudaStream_t st = (cudaStream_t)stream;
   cudaError_t e;
   if (!use_graph) {
-    for (int s = 0; s < nsteps; ++s) {
-      e = enqueue_step(pl, it0 + s, s == 0, s == nsteps - 1, false, 0.0, st);
-      if (e != cudaSuccess) return cuda_fail(e, "sw_run");
-    }
+    e = enqueue_sequence(pl, it0, nsteps, st);
+    if (e != cudaSuccess) return cuda_fail(e, "sw_run");
     return SW_OK;
   }
   if (!(pl->gexec && pl->g_it0 == it0 && pl->g_n == nsteps)) {
@@ -424,9 +626,7 @@ int sw_run(sw_plan* pl, int32_t it0, int32_t nsteps, int32_t use_graph, void* st
     }
     e = cudaStreamBeginCapture(pl->cap_stream, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return cuda_fail(e, "sw_run: begin capture");
-    cudaError_t le = cudaSuccess;
-    for (int s = 0; s < nsteps && le == cudaSuccess; ++s)
-      le = enqueue_step(pl, it0 + s, s == 0, s == nsteps - 1, false, 0.0, pl->cap_stream);
+    cudaError_t le = enqueue_sequence(pl, it0, nsteps, pl->cap_stream);
     cudaGraph_t g = nullptr;
     e = cudaStreamEndCapture(pl->cap_stream, &g);
     if (le != cudaSuccess) { if (g) cudaGraphDestroy(g); return cuda_fail(le, "sw_run: capture"); }

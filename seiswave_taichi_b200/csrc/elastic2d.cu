@@ -20,7 +20,7 @@ template <typename T>
 __device__ __forceinline__ void pml2(T* __restrict__ m, T b, T a, T kk, T& d) {
   T psi = b * (*m) + a * d;
   *m = psi;
-  d = d / kk + psi;
+  d = div_v(d, kk) + psi;
 }
 
 // ---- 2D stencils of src/Differential2D.py, read through the read-only path --
@@ -128,14 +128,14 @@ k2_velocity(const __grid_constant__ P2<T> p, int it, T amp, int src_here) {
   if (SCHEME == SW2D_SSG_VS) {
     // vx at (i, j): :144-154
     if (i >= N + 1 && i < nx - N && j >= N + 1 && j < nz - N) {
-      T dsxxdx = dx_bm<T, N>(sxx, idx, nz, c) / dx;
-      T dsxzdz = dz_bm<T, N>(sxz, idx, c) / dz;
+      T dsxxdx = div_c(dx_bm<T, N>(sxx, idx, nz, c), dx, p.rd[0], p.fast_div & 1);
+      T dsxzdz = div_c(dz_bm<T, N>(sxz, idx, c), dz, p.rd[1], p.fast_div & 1);
       if (any_slab && ((fx & 1) || (fz & 1))) {
         if (xi >= 0) pml2(mx(p, 0, xi, j), cfx[CB * nx + i], cfx[CA * nx + i], cfx[CK * nx + i], dsxxdx);
         if (zj >= 0) pml2(mz(p, 0, i, zj), cfz[CB * nz + j], cfz[CA * nz + j], cfz[CK * nz + j], dsxzdz);
       }
       T t = (dsxxdx + dsxzdz) * dt;
-      t = t / ldg(rho + idx);
+      t = div_v(t, ldg(rho + idx));
       vx[idx] = vx[idx] + t;
     }
     // vz at (i+1/2, j+1/2): :156-167, then the source :170
@@ -145,19 +145,19 @@ k2_velocity(const __grid_constant__ P2<T> p, int it, T amp, int src_here) {
       T v = vz[idx];
       if (upd) {
         const T rh = (T)0.25 * (ldg(rho + idx) + ldg(rho + idx + 1) + ldg(rho + idx + nz + 1) + ldg(rho + idx + nz));
-        T dsxzdx = dx_fm<T, N>(sxz, idx, nz, c) / dx;
-        T dszzdz = dz_fm<T, N>(szz, idx, c) / dz;
+        T dsxzdx = div_c(dx_fm<T, N>(sxz, idx, nz, c), dx, p.rd[0], p.fast_div & 1);
+        T dszzdz = div_c(dz_fm<T, N>(szz, idx, c), dz, p.rd[1], p.fast_div & 1);
         if (any_slab && ((fx & 2) || (fz & 2))) {
           if (xi >= 0) pml2(mx(p, 1, xi, j), cfx[CBH * nx + i], cfx[CAH * nx + i], cfx[CKH * nx + i], dsxzdx);
           if (zj >= 0) pml2(mz(p, 1, i, zj), cfz[CBH * nz + j], cfz[CAH * nz + j], cfz[CKH * nz + j], dszzdz);
         }
         T t = (dszzdz + dsxzdx) * dt;
-        t = t / rh;
+        t = div_v(t, rh);
         v = v + t;
       }
       if (src) {
         T t = dt * p.wav[it];
-        t = t / ldg(rho + idx);
+        t = div_v(t, ldg(rho + idx));
         v = v + t;
       }
       vz[idx] = v;
@@ -169,20 +169,20 @@ k2_velocity(const __grid_constant__ P2<T> p, int it, T amp, int src_here) {
     if (upd || src) {
       T v = vx[idx];
       if (upd) {
-        T dsxxdx = dx_fm<T, N>(sxx, idx, nz, c) / dx;
-        T dsxzdz = dz_bm<T, N>(sxz, idx, c) / dz;
+        T dsxxdx = div_c(dx_fm<T, N>(sxx, idx, nz, c), dx, p.rd[0], p.fast_div & 1);
+        T dsxzdz = div_c(dz_bm<T, N>(sxz, idx, c), dz, p.rd[1], p.fast_div & 1);
         const T rhx = (ldg(rho + idx) + ldg(rho + idx + nz)) / (T)2;
         if (any_slab && ((fx & 2) || (fz & 1))) {
           if (xi >= 0) pml2(mx(p, 0, xi, j), cfx[CBH * nx + i], cfx[CAH * nx + i], cfx[CKH * nx + i], dsxxdx);
           if (zj >= 0) pml2(mz(p, 0, i, zj), cfz[CB * nz + j], cfz[CA * nz + j], cfz[CK * nz + j], dsxzdz);
         }
         T t = (dsxxdx + dsxzdz) * dt;
-        t = t / rhx;
+        t = div_v(t, rhx);
         v = v + t;
       }
       if (src) {
         T t = dt * p.wav[it];
-        t = t / ldg(rho + idx);
+        t = div_v(t, ldg(rho + idx));
         v = v + t;
       }
       vx[idx] = v;
@@ -190,14 +190,14 @@ k2_velocity(const __grid_constant__ P2<T> p, int it, T amp, int src_here) {
     // vz at (i, j+1/2): :231-242
     if (i >= N + 1 && i < nx - N && j >= N && j < nz - N - 1) {
       const T rhz = (T)0.5 * (ldg(rho + idx) + ldg(rho + idx + 1));
-      T dsxzdx = dx_bm<T, N>(sxz, idx, nz, c) / dx;
-      T dszzdz = dz_fm<T, N>(szz, idx, c) / dz;
+      T dsxzdx = div_c(dx_bm<T, N>(sxz, idx, nz, c), dx, p.rd[0], p.fast_div & 1);
+      T dszzdz = div_c(dz_fm<T, N>(szz, idx, c), dz, p.rd[1], p.fast_div & 1);
       if (any_slab && ((fx & 1) || (fz & 2))) {
         if (xi >= 0) pml2(mx(p, 1, xi, j), cfx[CB * nx + i], cfx[CA * nx + i], cfx[CK * nx + i], dsxzdx);
         if (zj >= 0) pml2(mz(p, 1, i, zj), cfz[CBH * nz + j], cfz[CAH * nz + j], cfz[CKH * nz + j], dszzdz);
       }
       T t = (dszzdz + dsxzdx) * dt;
-      t = t / rhz;
+      t = div_v(t, rhz);
       vz[idx] = vz[idx] + t;
     }
   } else {  // SW2D_RSG, :292-323
@@ -207,10 +207,10 @@ k2_velocity(const __grid_constant__ P2<T> p, int it, T amp, int src_here) {
       const T dsxxrx = drx_bm<T, N>(sxx, idx, nz, c), dsxxrz = drz_bm<T, N>(sxx, idx, nz, c);
       const T dszzrx = drx_bm<T, N>(szz, idx, nz, c), dszzrz = drz_bm<T, N>(szz, idx, nz, c);
       const T dsxzrx = drx_bm<T, N>(sxz, idx, nz, c), dsxzrz = drz_bm<T, N>(sxz, idx, nz, c);
-      T dsxxdx = (dsxxrz - dsxxrx) / ((T)2 * dx);
-      T dszzdz = (dszzrz + dszzrx) / ((T)2 * dz);
-      T dsxzdx = (dsxzrz - dsxzrx) / ((T)2 * dx);
-      T dsxzdz = (dsxzrz + dsxzrx) / ((T)2 * dz);
+      T dsxxdx = div_c(dsxxrz - dsxxrx, (T)2 * dx, p.rd2[0], (p.fast_div >> 1) & 1);
+      T dszzdz = div_c(dszzrz + dszzrx, (T)2 * dz, p.rd2[1], (p.fast_div >> 1) & 1);
+      T dsxzdx = div_c(dsxzrz - dsxzrx, (T)2 * dx, p.rd2[0], (p.fast_div >> 1) & 1);
+      T dsxzdz = div_c(dsxzrz + dsxzrx, (T)2 * dz, p.rd2[1], (p.fast_div >> 1) & 1);
       const T rh = ldg(rho + idx);
       if (any_slab && ((fx & 1) || (fz & 1))) {
         if (xi >= 0) {
@@ -223,20 +223,20 @@ k2_velocity(const __grid_constant__ P2<T> p, int it, T amp, int src_here) {
         }
       }
       T t = (dsxxdx + dsxzdz) * dt;
-      t = t / rh;
+      t = div_v(t, rh);
       vx[idx] = vx[idx] + t;
       T u = (dszzdz + dsxzdx) * dt;
-      u = u / rh;
+      u = div_v(u, rh);
       T v = vz[idx] + u;
       if (src) {
         T s = dt * amp;
-        s = s / ((T)8 * rh);
+        s = div_v(s, (T)8 * rh);
         v = v + s;
       }
       vz[idx] = v;
     } else if (src) {
       T s = dt * amp;
-      s = s / ((T)8 * ldg(rho + idx));
+      s = div_v(s, (T)8 * ldg(rho + idx));
       vz[idx] = vz[idx] + s;
     }
   }
@@ -280,8 +280,8 @@ k2_stress(const __grid_constant__ P2<T> p, int it) {
       const T lhx = (T)0.5 * (ldg(lam + idx) + ldg(lam + idx + nz));
       const T mhx = (T)0.5 * (ldg(mu + idx) + ldg(mu + idx + nz));
       const T lpm = lhx + (T)2 * mhx;
-      T dvxdx = dx_fm<T, N>(vx, idx, nz, c) / dx;
-      T dvzdz = dz_bm<T, N>(vz, idx, c) / dz;
+      T dvxdx = div_c(dx_fm<T, N>(vx, idx, nz, c), dx, p.rd[0], p.fast_div & 1);
+      T dvzdz = div_c(dz_bm<T, N>(vz, idx, c), dz, p.rd[1], p.fast_div & 1);
       if (any_slab && ((fx & 2) || (fz & 1))) {
         if (xi >= 0) pml2(mx(p, 2, xi, j), cfx[CBH * nx + i], cfx[CAH * nx + i], cfx[CKH * nx + i], dvxdx);
         if (zj >= 0) pml2(mz(p, 2, i, zj), cfz[CB * nz + j], cfz[CA * nz + j], cfz[CK * nz + j], dvzdz);
@@ -292,8 +292,8 @@ k2_stress(const __grid_constant__ P2<T> p, int it) {
     // sxz at (i, j+1/2): :188-199
     if (i >= N + 1 && i < nx - N && j >= N && j < nz - N - 1) {
       const T mhz = (T)0.5 * (ldg(mu + idx + 1) + ldg(mu + idx));
-      T dvzdx = dx_bm<T, N>(vz, idx, nz, c) / dx;
-      T dvxdz = dz_fm<T, N>(vx, idx, c) / dz;
+      T dvzdx = div_c(dx_bm<T, N>(vz, idx, nz, c), dx, p.rd[0], p.fast_div & 1);
+      T dvxdz = div_c(dz_fm<T, N>(vx, idx, c), dz, p.rd[1], p.fast_div & 1);
       if (any_slab && ((fx & 1) || (fz & 2))) {
         if (xi >= 0) pml2(mx(p, 3, xi, j), cfx[CB * nx + i], cfx[CA * nx + i], cfx[CK * nx + i], dvzdx);
         if (zj >= 0) pml2(mz(p, 3, i, zj), cfz[CBH * nz + j], cfz[CAH * nz + j], cfz[CKH * nz + j], dvxdz);
@@ -305,8 +305,8 @@ k2_stress(const __grid_constant__ P2<T> p, int it) {
     if (i >= N + 1 && i < nx - N && j >= N + 1 && j < nz - N) {
       const T lm = ldg(lam + idx);
       const T lpm = ldg(lam + idx) + (T)2 * ldg(mu + idx);
-      T dvxdx = dx_bm<T, N>(vx, idx, nz, c) / dx;
-      T dvzdz = dz_bm<T, N>(vz, idx, c) / dz;
+      T dvxdx = div_c(dx_bm<T, N>(vx, idx, nz, c), dx, p.rd[0], p.fast_div & 1);
+      T dvzdz = div_c(dz_bm<T, N>(vz, idx, c), dz, p.rd[1], p.fast_div & 1);
       if (any_slab && ((fx & 1) || (fz & 1))) {
         if (xi >= 0) pml2(mx(p, 2, xi, j), cfx[CB * nx + i], cfx[CA * nx + i], cfx[CK * nx + i], dvxdx);
         if (zj >= 0) pml2(mz(p, 2, i, zj), cfz[CB * nz + j], cfz[CA * nz + j], cfz[CK * nz + j], dvzdz);
@@ -317,8 +317,8 @@ k2_stress(const __grid_constant__ P2<T> p, int it) {
     // sxz at (i+1/2, j+1/2): :262-273
     if (i >= N + 1 && i < nx - N && j >= N + 1 && j < nz - N) {
       const T m4 = (T)0.25 * (ldg(mu + idx + 1) + ldg(mu + idx) + ldg(mu + idx + nz + 1) + ldg(mu + idx + nz));
-      T dvzdx = dx_fm<T, N>(vz, idx, nz, c) / dx;
-      T dvxdz = dz_fm<T, N>(vx, idx, c) / dz;
+      T dvzdx = div_c(dx_fm<T, N>(vz, idx, nz, c), dx, p.rd[0], p.fast_div & 1);
+      T dvxdz = div_c(dz_fm<T, N>(vx, idx, c), dz, p.rd[1], p.fast_div & 1);
       if (any_slab && ((fx & 2) || (fz & 2))) {
         if (xi >= 0) pml2(mx(p, 3, xi, j), cfx[CBH * nx + i], cfx[CAH * nx + i], cfx[CKH * nx + i], dvzdx);
         if (zj >= 0) pml2(mz(p, 3, i, zj), cfz[CBH * nz + j], cfz[CAH * nz + j], cfz[CKH * nz + j], dvxdz);
@@ -331,10 +331,10 @@ k2_stress(const __grid_constant__ P2<T> p, int it) {
       const T lpm = lm + (T)2 * u;
       const T dvxrx = drx_fm<T, N>(vx, idx, nz, c), dvxrz = drz_fm<T, N>(vx, idx, nz, c);
       const T dvzrx = drx_fm<T, N>(vz, idx, nz, c), dvzrz = drz_fm<T, N>(vz, idx, nz, c);
-      T dvxdx = (dvxrz - dvxrx) / ((T)2 * dx);
-      T dvxdz = (dvxrz + dvxrx) / ((T)2 * dz);
-      T dvzdx = (dvzrz - dvzrx) / ((T)2 * dx);
-      T dvzdz = (dvzrz + dvzrx) / ((T)2 * dz);
+      T dvxdx = div_c(dvxrz - dvxrx, (T)2 * dx, p.rd2[0], (p.fast_div >> 1) & 1);
+      T dvxdz = div_c(dvxrz + dvxrx, (T)2 * dz, p.rd2[1], (p.fast_div >> 1) & 1);
+      T dvzdx = div_c(dvzrz - dvzrx, (T)2 * dx, p.rd2[0], (p.fast_div >> 1) & 1);
+      T dvzdz = div_c(dvzrz + dvzrx, (T)2 * dz, p.rd2[1], (p.fast_div >> 1) & 1);
       if (any_slab && ((fx & 2) || (fz & 2))) {
         if (xi >= 0) {
           pml2(mx(p, 2, xi, j), cfx[CBH * nx + i], cfx[CAH * nx + i], cfx[CKH * nx + i], dvxdx);

@@ -23,7 +23,7 @@ template <typename T>
 __device__ __forceinline__ void pml_apply(T* __restrict__ m, T b, T a, T kk, T& d) {
   T psi = b * (*m) + a * d;
   *m = psi;
-  d = d / kk + psi;
+  d = div_v(d, kk) + psi;
 }
 
 // ---------------------------------------------------------------------------
@@ -112,9 +112,9 @@ k3_velocity(const __grid_constant__ P3<T> p, int it, int force_here) {
         const T hi = (m == 0) ? qxz[N] : ldg(sxz + idx + m);
         dsxzdz += c[m] * (hi - ldg(sxz + idx - (m + 1)));
       }
-      dsxxdx = dsxxdx / dx;
-      dsxydy = dsxydy / dy;
-      dsxzdz = dsxzdz / dz;
+      dsxxdx = div_c(dsxxdx, dx, p.rd[0], p.fast_div);
+      dsxydy = div_c(dsxydy, dy, p.rd[1], p.fast_div);
+      dsxzdz = div_c(dsxzdz, dz, p.rd[2], p.fast_div);
       if ((xi >= 0 || yj >= 0 || zk >= 0) && ((fx & 2) || (fy & 1) || (fz & 1))) {
         if (xi >= 0)
           pml_apply(p.mem[0] + ((long long)xi * ny + j) * nz + k,
@@ -127,7 +127,7 @@ k3_velocity(const __grid_constant__ P3<T> p, int it, int force_here) {
                     cfz[CB * nz + k], cfz[CA * nz + k], cfz[CK * nz + k], dsxzdz);
       }
       T t = (dsxxdx + dsxzdz + dsxydy) * dt;
-      t = t / rc0;
+      t = div_v(t, rc0);
       vx[idx] = vx[idx] + t;
     }
 
@@ -143,9 +143,9 @@ k3_velocity(const __grid_constant__ P3<T> p, int it, int force_here) {
 #pragma unroll
       for (int m = 0; m < N; ++m)
         dsyzdz += c[m] * (ldg(syz + idx + m) - ldg(syz + idx - (m + 1)));
-      dsxydx = dsxydx / dx;
-      dsyydy = dsyydy / dy;
-      dsyzdz = dsyzdz / dz;
+      dsxydx = div_c(dsxydx, dx, p.rd[0], p.fast_div);
+      dsyydy = div_c(dsyydy, dy, p.rd[1], p.fast_div);
+      dsyzdz = div_c(dsyzdz, dz, p.rd[2], p.fast_div);
       if ((xi >= 0 || yj >= 0 || zk >= 0) && ((fx & 1) || (fy & 2) || (fz & 1))) {
         if (xi >= 0)
           pml_apply(p.mem[0] + p.mcomp[0] + ((long long)xi * ny + j) * nz + k,
@@ -158,7 +158,7 @@ k3_velocity(const __grid_constant__ P3<T> p, int it, int force_here) {
                     cfz[CB * nz + k], cfz[CA * nz + k], cfz[CK * nz + k], dsyzdz);
       }
       T t = (dsxydx + dsyydy + dsyzdz) * dt;
-      t = t / rhy;
+      t = div_v(t, rhy);
       vy[idx] = vy[idx] + t;
     }
 
@@ -178,9 +178,9 @@ k3_velocity(const __grid_constant__ P3<T> p, int it, int force_here) {
 #pragma unroll
         for (int m = 0; m < N; ++m)
           dszzdz += c[m] * (ldg(szz + idx + (m + 1)) - ldg(szz + idx - m));
-        dsxzdx = dsxzdx / dx;
-        dsyzdy = dsyzdy / dy;
-        dszzdz = dszzdz / dz;
+        dsxzdx = div_c(dsxzdx, dx, p.rd[0], p.fast_div);
+        dsyzdy = div_c(dsyzdy, dy, p.rd[1], p.fast_div);
+        dszzdz = div_c(dszzdz, dz, p.rd[2], p.fast_div);
         if ((xi >= 0 || yj >= 0 || zk >= 0) && ((fx & 1) || (fy & 1) || (fz & 2))) {
           if (xi >= 0)
             pml_apply(p.mem[0] + 2 * p.mcomp[0] + ((long long)xi * ny + j) * nz + k,
@@ -194,13 +194,13 @@ k3_velocity(const __grid_constant__ P3<T> p, int it, int force_here) {
         }
         T s = TENSOR ? (dsxzdx + dsyzdy + dszzdz) : (dszzdz + dsxzdx + dsyzdy);
         T t = s * dt;
-        t = t / r4;
+        t = div_v(t, r4);
         v = v + t;
       }
       if (vz_src) {
         // Elastic3D_SSG_CPML.py:245 / Elastic3D_SSG_SPML.py:294
         T t = dt * p.wav[it];
-        t = t / rc0;
+        t = div_v(t, rc0);
         v = v + t;
       }
       vz[idx] = v;
@@ -319,9 +319,9 @@ k3_stress(const __grid_constant__ P3<T> p, int it, int inject_next) {
           const T hi = (m == 0) ? qvz[N - 1] : ldg(vz + idx + m);
           dvzdz += c[m] * (hi - ldg(vz + idx - (m + 1)));
         }
-        dvxdx = dvxdx / dx;
-        dvydy = dvydy / dy;
-        dvzdz = dvzdz / dz;
+        dvxdx = div_c(dvxdx, dx, p.rd[0], p.fast_div);
+        dvydy = div_c(dvydy, dy, p.rd[1], p.fast_div);
+        dvzdz = div_c(dvzdz, dz, p.rd[2], p.fast_div);
         if (any_slab && ((fx | fy | fz) & 1)) {
           if (xi >= 0)
             pml_apply(p.mem[0] + 3 * p.mcomp[0] + ((long long)xi * ny + j) * nz + k,
@@ -362,8 +362,8 @@ k3_stress(const __grid_constant__ P3<T> p, int it, int inject_next) {
           const T lo = (m == 0) ? qvx[N] : ldg(vx + idx - (long long)m * nz);
           dvxdy += c[m] * (ldg(vx + idx + (long long)(m + 1) * nz) - lo);
         }
-        dvydx = dvydx / dx;
-        dvxdy = dvxdy / dy;
+        dvydx = div_c(dvydx, dx, p.rd[0], p.fast_div);
+        dvxdy = div_c(dvxdy, dy, p.rd[1], p.fast_div);
         if (any_slab && ((fx & 2) || (fy & 2) || (fz & 1))) {
           if (xi >= 0)
             pml_apply(p.mem[0] + 4 * p.mcomp[0] + ((long long)xi * ny + j) * nz + k,
@@ -393,8 +393,8 @@ k3_stress(const __grid_constant__ P3<T> p, int it, int inject_next) {
           const T lo = (m == 0) ? qvx[N] : ldg(vx + idx - m);
           dvxdz += c[m] * (ldg(vx + idx + (m + 1)) - lo);
         }
-        dvzdx = dvzdx / dx;
-        dvxdz = dvxdz / dz;
+        dvzdx = div_c(dvzdx, dx, p.rd[0], p.fast_div);
+        dvxdz = div_c(dvxdz, dz, p.rd[2], p.fast_div);
         if (any_slab && ((fx & 2) || (fy & 1) || (fz & 2))) {
           if (xi >= 0)
             pml_apply(p.mem[0] + 5 * p.mcomp[0] + ((long long)xi * ny + j) * nz + k,
@@ -427,8 +427,8 @@ k3_stress(const __grid_constant__ P3<T> p, int it, int inject_next) {
           const T lo = (m == 0) ? qvy[N - 1] : ldg(vy + idx - m);
           dvydz += c[m] * (ldg(vy + idx + (m + 1)) - lo);
         }
-        dvzdy = dvzdy / dy;
-        dvydz = dvydz / dz;
+        dvzdy = div_c(dvzdy, dy, p.rd[1], p.fast_div);
+        dvydz = div_c(dvydz, dz, p.rd[2], p.fast_div);
         if (any_slab && ((fx & 1) || (fy & 2) || (fz & 2))) {
           if (yj >= 0)
             pml_apply(p.mem[1] + 5 * p.mcomp[1] + ((long long)i * p.sn[1] + yj) * nz + k,
@@ -471,7 +471,7 @@ template <typename T>
 __global__ void k3_force_inject(const __grid_constant__ P3<T> p, int it) {
   const long long s = ((long long)p.si * p.ny + p.sj) * p.nz + p.sk;
   T t = p.dt * p.wav[it];
-  t = t / p.rho[s];
+  t = div_v(t, p.rho[s]);
   p.f[2][s] = p.f[2][s] + t;
 }
 

@@ -61,17 +61,17 @@ ks_velocity(const __grid_constant__ P3<T> p, int it, int src_here) {
 
   // vx :182-205
   if (i >= N && i < nx - N - 1 && j >= N + 1 && j < ny - N && k >= N + 1 && k < nz - N) {
-    T dsxxdx = d_fm<T, N>(sxx, idx, sx, c) / dx;
-    T dsxydy = d_bm<T, N>(sxy, idx, sy, c) / dy;
-    T dsxzdz = d_bm<T, N>(sxz, idx, 1, c) / dz;
+    T dsxxdx = div_c(d_fm<T, N>(sxx, idx, sx, c), dx, p.rd[0], p.fast_div);
+    T dsxydy = div_c(d_bm<T, N>(sxy, idx, sy, c), dy, p.rd[1], p.fast_div);
+    T dsxzdz = div_c(d_bm<T, N>(sxz, idx, 1, c), dz, p.rd[2], p.fast_div);
     const T rh = ldg(rho + idx);
     const T ro = (T)1 / rh;
     if ((fx & 2) || (fy & 1) || (fz & 1)) {
       const T xn = (T)1 - hdt * dpx[nx + i], yn = (T)1 - hdt * dpy[j], zn = (T)1 - hdt * dpz[k];
       const T xd = (T)1 + hdt * dpx[nx + i], yd = (T)1 + hdt * dpy[j], zd = (T)1 + hdt * dpz[k];
-      T a = (xn * sp[PVX_X * G + idx] + dsxxdx * dt * ro) / xd;
-      T b = (yn * sp[PVX_Y * G + idx] + dsxydy * dt * ro) / yd;
-      T cc = (zn * sp[PVX_Z * G + idx] + dsxzdz * dt * ro) / zd;
+      T a = div_v((xn * sp[PVX_X * G + idx] + dsxxdx * dt * ro), xd);
+      T b = div_v((yn * sp[PVX_Y * G + idx] + dsxydy * dt * ro), yd);
+      T cc = div_v((zn * sp[PVX_Z * G + idx] + dsxzdz * dt * ro), zd);
       sp[PVX_X * G + idx] = a;
       sp[PVX_Y * G + idx] = b;
       sp[PVX_Z * G + idx] = cc;
@@ -84,15 +84,15 @@ ks_velocity(const __grid_constant__ P3<T> p, int it, int src_here) {
   if (i >= N + 1 && i < nx - N && j >= N && j < ny - N - 1 && k >= N + 1 && k < nz - N) {
     const T rhy = (T)0.5 * (ldg(rho + idx) + ldg(rho + idx + sy));
     const T ro = (T)1 / rhy;
-    T dsxydx = d_bm<T, N>(sxy, idx, sx, c) / dx;
-    T dsyydy = d_fm<T, N>(syy, idx, sy, c) / dy;
-    T dsyzdz = d_bm<T, N>(syz, idx, 1, c) / dz;
+    T dsxydx = div_c(d_bm<T, N>(sxy, idx, sx, c), dx, p.rd[0], p.fast_div);
+    T dsyydy = div_c(d_fm<T, N>(syy, idx, sy, c), dy, p.rd[1], p.fast_div);
+    T dsyzdz = div_c(d_bm<T, N>(syz, idx, 1, c), dz, p.rd[2], p.fast_div);
     if ((fx & 1) || (fy & 2) || (fz & 1)) {
       const T xn = (T)1 - hdt * dpx[i], yn = (T)1 - hdt * dpy[ny + j], zn = (T)1 - hdt * dpz[k];
       const T xd = (T)1 + hdt * dpx[i], yd = (T)1 + hdt * dpy[ny + j], zd = (T)1 + hdt * dpz[k];
-      T a = (xn * sp[PVY_X * G + idx] + dt * dsxydx * ro) / xd;
-      T b = (yn * sp[PVY_Y * G + idx] + dt * dsyydy * ro) / yd;
-      T cc = (zn * sp[PVY_Z * G + idx] + dt * dsyzdz * ro) / zd;
+      T a = div_v((xn * sp[PVY_X * G + idx] + dt * dsxydx * ro), xd);
+      T b = div_v((yn * sp[PVY_Y * G + idx] + dt * dsyydy * ro), yd);
+      T cc = div_v((zn * sp[PVY_Z * G + idx] + dt * dsyzdz * ro), zd);
       sp[PVY_X * G + idx] = a;
       sp[PVY_Y * G + idx] = b;
       sp[PVY_Z * G + idx] = cc;
@@ -109,15 +109,15 @@ ks_velocity(const __grid_constant__ P3<T> p, int it, int src_here) {
     if (upd) {
       const T r4 = (T)0.25 * (ldg(rho + idx) + ldg(rho + idx + sy) + ldg(rho + idx + sx + sy) + ldg(rho + idx + sx));
       const T ro = (T)1 / r4;
-      T dsxzdx = d_bm<T, N>(sxz, idx, sx, c) / dx;
-      T dsyzdy = d_bm<T, N>(syz, idx, sy, c) / dy;
-      T dszzdz = d_fm<T, N>(szz, idx, 1, c) / dz;
+      T dsxzdx = div_c(d_bm<T, N>(sxz, idx, sx, c), dx, p.rd[0], p.fast_div);
+      T dsyzdy = div_c(d_bm<T, N>(syz, idx, sy, c), dy, p.rd[1], p.fast_div);
+      T dszzdz = div_c(d_fm<T, N>(szz, idx, 1, c), dz, p.rd[2], p.fast_div);
       if ((fx & 1) || (fy & 1) || (fz & 2)) {
         const T xn = (T)1 - hdt * dpx[i], yn = (T)1 - hdt * dpy[j], zn = (T)1 - hdt * dpz[nz + k];
         const T xd = (T)1 + hdt * dpx[i], yd = (T)1 + hdt * dpy[j], zd = (T)1 + hdt * dpz[nz + k];
-        T a = (xn * sp[PVZ_X * G + idx] + dt * dsxzdx * ro) / xd;
-        T b = (yn * sp[PVZ_Y * G + idx] + dt * dsyzdy * ro) / yd;
-        T cc = (zn * sp[PVZ_Z * G + idx] + dt * dszzdz * ro) / zd;
+        T a = div_v((xn * sp[PVZ_X * G + idx] + dt * dsxzdx * ro), xd);
+        T b = div_v((yn * sp[PVZ_Y * G + idx] + dt * dsyzdy * ro), yd);
+        T cc = div_v((zn * sp[PVZ_Z * G + idx] + dt * dszzdz * ro), zd);
         sp[PVZ_X * G + idx] = a;
         sp[PVZ_Y * G + idx] = b;
         sp[PVZ_Z * G + idx] = cc;
@@ -128,7 +128,7 @@ ks_velocity(const __grid_constant__ P3<T> p, int it, int src_here) {
     }
     if (src) {
       T t = dt * p.wav[it];
-      t = t / ldg(rho + idx);
+      t = div_v(t, ldg(rho + idx));
       v = v + t;
     }
     vz[idx] = v;
@@ -166,21 +166,21 @@ ks_stress(const __grid_constant__ P3<T> p, int it) {
   if (i >= N + 1 && i < nx - N && j >= N + 1 && j < ny - N && k >= N + 1 && k < nz - N) {
     const T lm = ldg(lam + idx), u = ldg(mu + idx);
     const T l2m = lm + (T)2 * u;
-    T dvxdx = d_bm<T, N>(vx, idx, sx, c) / dx;
-    T dvydy = d_bm<T, N>(vy, idx, sy, c) / dy;
-    T dvzdz = d_bm<T, N>(vz, idx, 1, c) / dz;
+    T dvxdx = div_c(d_bm<T, N>(vx, idx, sx, c), dx, p.rd[0], p.fast_div);
+    T dvydy = div_c(d_bm<T, N>(vy, idx, sy, c), dy, p.rd[1], p.fast_div);
+    T dvzdz = div_c(d_bm<T, N>(vz, idx, 1, c), dz, p.rd[2], p.fast_div);
     if ((fx | fy | fz) & 1) {
       const T xn = (T)1 - hdt * dpx[i], yn = (T)1 - hdt * dpy[j], zn = (T)1 - hdt * dpz[k];
       const T xd = (T)1 + hdt * dpx[i], yd = (T)1 + hdt * dpy[j], zd = (T)1 + hdt * dpz[k];
-      T xx = (xn * sp[PSXX_X * G + idx] + dt * l2m * dvxdx) / xd;
-      T xy = (yn * sp[PSXX_Y * G + idx] + dt * lm * dvydy) / yd;
-      T xz = (zn * sp[PSXX_Z * G + idx] + dt * lm * dvzdz) / zd;
-      T yx = (xn * sp[PSYY_X * G + idx] + dt * lm * dvxdx) / xd;
-      T yy = (yn * sp[PSYY_Y * G + idx] + dt * l2m * dvydy) / yd;
-      T yz = (zn * sp[PSYY_Z * G + idx] + dt * lm * dvzdz) / zd;
-      T zx = (xn * sp[PSZZ_X * G + idx] + dt * lm * dvxdx) / xd;
-      T zy = (yn * sp[PSZZ_Y * G + idx] + dt * lm * dvydy) / yd;
-      T zz = (zn * sp[PSZZ_Z * G + idx] + dt * l2m * dvzdz) / zd;
+      T xx = div_v((xn * sp[PSXX_X * G + idx] + dt * l2m * dvxdx), xd);
+      T xy = div_v((yn * sp[PSXX_Y * G + idx] + dt * lm * dvydy), yd);
+      T xz = div_v((zn * sp[PSXX_Z * G + idx] + dt * lm * dvzdz), zd);
+      T yx = div_v((xn * sp[PSYY_X * G + idx] + dt * lm * dvxdx), xd);
+      T yy = div_v((yn * sp[PSYY_Y * G + idx] + dt * l2m * dvydy), yd);
+      T yz = div_v((zn * sp[PSYY_Z * G + idx] + dt * lm * dvzdz), zd);
+      T zx = div_v((xn * sp[PSZZ_X * G + idx] + dt * lm * dvxdx), xd);
+      T zy = div_v((yn * sp[PSZZ_Y * G + idx] + dt * lm * dvydy), yd);
+      T zz = div_v((zn * sp[PSZZ_Z * G + idx] + dt * l2m * dvzdz), zd);
       sp[PSXX_X * G + idx] = xx; sp[PSXX_Y * G + idx] = xy; sp[PSXX_Z * G + idx] = xz;
       sp[PSYY_X * G + idx] = yx; sp[PSYY_Y * G + idx] = yy; sp[PSYY_Z * G + idx] = yz;
       sp[PSZZ_X * G + idx] = zx; sp[PSZZ_Y * G + idx] = zy; sp[PSZZ_Z * G + idx] = zz;
@@ -196,13 +196,13 @@ ks_stress(const __grid_constant__ P3<T> p, int it) {
   // sxy :334-350
   if (i >= N + 1 && i < nx - N && j >= N + 1 && j < ny - N && k >= N && k < nz - N) {
     const T m4 = (T)0.25 * (ldg(mu + idx + sy) + ldg(mu + idx) + ldg(mu + idx) + ldg(mu + idx + sx));
-    T dvydx = d_fm<T, N>(vy, idx, sx, c) / dx;
-    T dvxdy = d_fm<T, N>(vx, idx, sy, c) / dy;
+    T dvydx = div_c(d_fm<T, N>(vy, idx, sx, c), dx, p.rd[0], p.fast_div);
+    T dvxdy = div_c(d_fm<T, N>(vx, idx, sy, c), dy, p.rd[1], p.fast_div);
     if ((fx & 2) || (fy & 2) || (fz & 1)) {
       const T xn = (T)1 - hdt * dpx[nx + i], yn = (T)1 - hdt * dpy[ny + j];
       const T xd = (T)1 + hdt * dpx[nx + i], yd = (T)1 + hdt * dpy[ny + j];
-      T a = (xn * sp[PSXY_X * G + idx] + dt * m4 * dvydx) / xd;
-      T b = (yn * sp[PSXY_Y * G + idx] + dt * m4 * dvxdy) / yd;
+      T a = div_v((xn * sp[PSXY_X * G + idx] + dt * m4 * dvydx), xd);
+      T b = div_v((yn * sp[PSXY_Y * G + idx] + dt * m4 * dvxdy), yd);
       sp[PSXY_X * G + idx] = a;
       sp[PSXY_Y * G + idx] = b;
       sxy[idx] = a + b;
@@ -213,13 +213,13 @@ ks_stress(const __grid_constant__ P3<T> p, int it) {
   // sxz :352-371
   if (i >= N && i < nx - N - 1 && j >= N && j < ny - N && k >= N && k < nz - N - 1) {
     const T m4 = (T)0.25 * (ldg(mu + idx) + ldg(mu + idx + sx) + ldg(mu + idx) + ldg(mu + idx + sy));
-    T dvzdx = d_fm<T, N>(vz, idx, sx, c) / dx;
-    T dvxdz = d_fm<T, N>(vx, idx, 1, c) / dz;
+    T dvzdx = div_c(d_fm<T, N>(vz, idx, sx, c), dx, p.rd[0], p.fast_div);
+    T dvxdz = div_c(d_fm<T, N>(vx, idx, 1, c), dz, p.rd[2], p.fast_div);
     if ((fx & 2) || (fy & 1) || (fz & 2)) {
       const T xn = (T)1 - hdt * dpx[nx + i], zn = (T)1 - hdt * dpz[nz + k];
       const T xd = (T)1 + hdt * dpx[nx + i], zd = (T)1 + hdt * dpz[nz + k];
-      T a = (xn * sp[PSXZ_X * G + idx] + dt * m4 * dvzdx) / xd;
-      T b = (zn * sp[PSXZ_Z * G + idx] + dt * m4 * dvxdz) / zd;
+      T a = div_v((xn * sp[PSXZ_X * G + idx] + dt * m4 * dvzdx), xd);
+      T b = div_v((zn * sp[PSXZ_Z * G + idx] + dt * m4 * dvxdz), zd);
       sp[PSXZ_X * G + idx] = a;
       sp[PSXZ_Z * G + idx] = b;
       sxz[idx] = a + b;
@@ -230,13 +230,13 @@ ks_stress(const __grid_constant__ P3<T> p, int it) {
   // syz :373-391
   if (i >= N && i < nx - N && j >= N && j < ny - N - 1 && k >= N && k < nz - N - 1) {
     const T m4 = (T)0.25 * (ldg(mu + idx + sy) + ldg(mu + idx) + ldg(mu + idx + 1) + ldg(mu + idx));
-    T dvzdy = d_fm<T, N>(vz, idx, sy, c) / dy;
-    T dvydz = d_fm<T, N>(vy, idx, 1, c) / dz;
+    T dvzdy = div_c(d_fm<T, N>(vz, idx, sy, c), dy, p.rd[1], p.fast_div);
+    T dvydz = div_c(d_fm<T, N>(vy, idx, 1, c), dz, p.rd[2], p.fast_div);
     if ((fx & 1) || (fy & 2) || (fz & 2)) {
       const T yn = (T)1 - hdt * dpy[ny + j], zn = (T)1 - hdt * dpz[nz + k];
       const T yd = (T)1 + hdt * dpy[ny + j], zd = (T)1 + hdt * dpz[nz + k];
-      T a = (yn * sp[PSYZ_Y * G + idx] + dt * m4 * dvzdy) / yd;
-      T b = (zn * sp[PSYZ_Z * G + idx] + dt * m4 * dvydz) / zd;
+      T a = div_v((yn * sp[PSYZ_Y * G + idx] + dt * m4 * dvzdy), yd);
+      T b = div_v((zn * sp[PSYZ_Z * G + idx] + dt * m4 * dvydz), zd);
       sp[PSYZ_Y * G + idx] = a;
       sp[PSYZ_Z * G + idx] = b;
       syz[idx] = a + b;

@@ -52,6 +52,8 @@ struct P3 {
   const long long* rec_idx;
   void* rec_data;
   int x_chunk;              // x planes streamed by one CTA
+  T rd[3];                  // RN(1/dx), RN(1/dy), RN(1/dz)
+  int fast_div;             // div_c may use the verified constant-divisor path
 };
 
 // 2D memory-variable components, 4 per direction, shared by all schemes:
@@ -75,10 +77,56 @@ struct P2 {
   int nrec, rec_field, rec_f64;
   const long long* rec_idx;
   void* rec_data;
+  T rd[2];                  // RN(1/dx), RN(1/dz)
+  T rd2[2];                 // RN(1/(2dx)), RN(1/(2dz)) (rotated-grid derivatives)
+  int fast_div;             // bit0: dx, dz verified; bit1: 2dx, 2dz verified
 };
 
 template <typename T>
 __device__ __forceinline__ T ldg(const T* p) { return __ldg(p); }
+
+// x / d for a positive divisor that varies per cell (density, kappa, split-PML
+// denominators).  A zero numerator -- most of the grid ahead of the wavefront
+// -- returns x itself, which is exactly +-0/d for d > 0, without entering the
+// division routine.
+template <typename T>
+__device__ __forceinline__ T div_v(T x, T d) {
+  return x == (T)0 ? x : x / d;
+}
+
+// Division of floats whose numerator may be tiny (the numerical precursor
+// ahead of a wavefront holds values down to the denormal range, for which the
+// float division routine leaves its fast path).  Such numerators are divided
+// in double precision and rounded once to float: with 53 >= 2*24+2 bits the
+// double rounding is innocuous (S. Figueroa, "When is double rounding
+// innocuous?", SIGNUM Newsletter 30(3), 1995), so the result equals the
+// correctly rounded float quotient.  Float inputs are normal doubles, so the
+// double division never leaves its own fast path.
+template <>
+__device__ __forceinline__ float div_v<float>(float x, float d) {
+  const unsigned ex = (__float_as_uint(x) >> 23) & 0xffu;  // biased exponent
+  if (ex - 27u < 200u) return __fdiv_rn(x, d);                // |x| in [2^-100, 2^100)
+  if (x == 0.f) return x;                                   // +-0/d = +-0 for d > 0
+  return __double2float_rn(__ddiv_rn((double)x, (double)d));
+}
+
+// x / d for a divisor fixed for the run (dx, dy, dz), r = RN(1/d).  With
+// fast != 0 (float only) numerators of magnitude in [2^-100, 2^100) use
+// Markstein's correction
+//   q = RN(x*r), e = fma(-q, d, x), result = fma(e, r, q)
+// (P. Markstein, IBM J. Res. Dev. 34(1), 1990); zeros, denormals and huge
+// values take div_v.  The plan enables the fast path only after checking
+// that the whole function equals IEEE division x/d for every finite float x.
+__device__ __forceinline__ float div_c(float x, float d, float r, int fast) {
+  const unsigned ex = (__float_as_uint(x) >> 23) & 0xffu;  // biased exponent
+  if (fast && ex - 27u < 200u) {
+    const float q = __fmul_rn(x, r);
+    const float e = __fmaf_rn(-q, d, x);
+    return __fmaf_rn(e, r, q);
+  }
+  return div_v(x, d);
+}
+__device__ __forceinline__ double div_c(double x, double d, double, int) { return div_v(x, d); }
 
 // receiver sample in the trace's element type
 template <typename T>
