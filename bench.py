@@ -320,7 +320,7 @@ def main(argv=None):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": cfg["name"], "grid": list(cfg["shape"]), "time_steps": nt,
                        "accuracy": cfg["accuracy"], "parallelism": f"replicas{world}",
-                       "path": (w._plan.info() if three_d else {"two_pass": True}),
+                       "path": (w._plan.info() if three_d else {"path": "two_pass"}),
                        "l2": "state larger than L2 (no flush needed)" if three_d else
                              "state fits in L2 (2D 400^2); %HBM not meaningful"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

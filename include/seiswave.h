@@ -168,16 +168,28 @@ SW_API int sw_plan_set_tile(sw_plan* plan, int32_t x_chunk);
  * path); it is the status read the drivers' loops can add after run(). */
 SW_API int sw_plan_status(sw_plan* plan, void* stream);
 
-/* Describe the plan's execution path: info[0] fused single-pass kernel
- * available, [1] constant-divisor fast path verified, [2] fused grid size,
- * [3] fused x-chunk length, [4] two-pass x-chunk length, [5] fused path
- * enabled.  info must hold 6 int32. */
+/* Describe the plan's execution path: info[0] current path of sw_step/sw_run
+ * (0 register-queue two-pass kernels, 1 TMA-staged two-pass kernels, 2 fused
+ * single-pass kernel), [1] constant-divisor fast path verified, [2] staged
+ * path available, [3] its grid, [4] its x-chunk length, [5] fused path set
+ * up, [6] its grid, [7] its x-chunk length, [8] exact numerics (see
+ * sw_plan_set_exact).  info must hold 9 int32. */
 SW_API int sw_plan_info(sw_plan* plan, int32_t* info);
 
-/* Choose the execution path of sw_run: use_fused = 0 keeps every step on the
- * two-pass kernels; chunk_len > 0 sets the x planes per fused work unit
- * (the autotuner's knob). */
-SW_API int sw_plan_set_path(sw_plan* plan, int32_t use_fused, int32_t chunk_len);
+/* Choose the execution path (values of info[0]); the fused path allocates a
+ * second buffer set of the wavefields on first use.  chunk_len > 0 sets the
+ * x planes per work unit of the staged or fused path (the autotuner's knob).
+ * Every path gives the same result bit for bit. */
+SW_API int sw_plan_set_path(sw_plan* plan, int32_t path, int32_t chunk_len);
+
+/* Numeric mode of the staged path.  exact != 0: every operation rounds in
+ * the reference's order with IEEE division (default; results bit-identical
+ * to a CPU evaluation of the reference's expressions).  exact == 0: spacings
+ * folded into the stencil coefficients, fused multiply-adds and approximate
+ * division by the material (receiver traces within relative L2 1e-5 of the
+ * exact mode, final wavefields within 1e-4).  The other paths are always
+ * exact. */
+SW_API int sw_plan_set_exact(sw_plan* plan, int32_t exact);
 
 /* sizeof of the ABI structs as this library was compiled: which = 0
  * sw_pml_axis, 1 sw_receivers, 2 sw_source, 3 sw2d_desc, 4 sw3d_desc; -1 else.

@@ -21,9 +21,9 @@ class ElasticWAVE(Elastic3DBase):
     _scheme = N.SW3D_CPML_FORCE
 
     def __init__(self, vs, vp, rho, dx, dy, dz, dt, isx, isy, isz, rsx, rsy, rsz, nt, accuracy,
-                 freq=100, fieldtype=torch.float32, *, coef64=False):
+                 freq=100, fieldtype=torch.float32, *, coef64=False, exact=True):
         self._init_common(vs, vp, rho, dx, dy, dz, dt, isx, isy, isz, nt, accuracy, freq, fieldtype,
-                          coef64)
+                          coef64, exact)
         self.rsx, self.rsy, self.rsz = rsx, rsy, rsz
         self._rec_lin, _ = receiver_table(self.gridsize, rsx, rsy, rsz)
         self.data = torch.zeros(self.nt, dtype=torch.float32, device=self._dev)

@@ -27,10 +27,10 @@ class ElasticWAVE(Elastic3DBase):
     _scheme = N.SW3D_CPML_TENSOR
 
     def __init__(self, vs, vp, rho, dx, dy, dz, dt, isx, isy, isz, rsx, rsy, rsz, MT, src_scale,
-                 nt, accuracy, freq=100., fieldtype=torch.float32, *, t0=0.03, coef64=False,
+                 nt, accuracy, freq=100., fieldtype=torch.float32, *, t0=0.03, coef64=False, exact=True,
                  rec_component="vx"):
         self._init_common(vs, vp, rho, dx, dy, dz, dt, isx, isy, isz, nt, accuracy, freq, fieldtype,
-                          coef64)
+                          coef64, exact)
         self.rsx, self.rsy, self.rsz = rsx, rsy, rsz
         self.MT = np.asarray(as_numpy(MT), dtype=np.float32).reshape(3, 3)
         self.src_scale = src_scale

@@ -30,6 +30,7 @@ EXPORTS = (
     "sw_version", "sw_last_error", "sw2d_plan_create", "sw3d_plan_create",
     "sw_plan_set_tile", "sw_abi_sizeof", "sw_plan_destroy", "sw_step", "sw_step_amp",
     "sw_run", "sw_check_finite", "sw_plan_status", "sw_plan_info", "sw_plan_set_path",
+    "sw_plan_set_exact",
 )
 
 
@@ -114,6 +115,7 @@ def load() -> C.CDLL:
         "sw_plan_status": (C.c_int, [vp, vp]),
         "sw_plan_info": (C.c_int, [vp, C.POINTER(C.c_int32)]),
         "sw_plan_set_path": (C.c_int, [vp, C.c_int32, C.c_int32]),
+        "sw_plan_set_exact": (C.c_int, [vp, C.c_int32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -192,14 +194,23 @@ class Plan:
         """Synchronize and raise if a kernel recorded a device-side failure."""
         check(load().sw_plan_status(self._h, C.c_void_p(stream)))
 
-    def info(self) -> dict:
-        a = (C.c_int32 * 6)()
-        check(load().sw_plan_info(self._h, a))
-        return {"fused": bool(a[0]), "fast_div": bool(a[1]), "fused_grid": a[2], "fused_chunk": a[3],
-                "two_pass_chunk": a[4], "use_fused": bool(a[5])}
+    PATHS = {"two_pass": 0, "staged": 1, "fused": 2}
 
-    def set_path(self, use_fused: bool = True, chunk_len: int = 0) -> None:
-        check(load().sw_plan_set_path(self._h, 1 if use_fused else 0, int(chunk_len)))
+    def info(self) -> dict:
+        a = (C.c_int32 * 9)()
+        check(load().sw_plan_info(self._h, a))
+        names = {v: k for k, v in self.PATHS.items()}
+        return {"path": names[a[0]], "fast_div": bool(a[1]), "staged": bool(a[2]), "staged_grid": a[3],
+                "staged_chunk": a[4], "fused": bool(a[5]), "fused_grid": a[6], "fused_chunk": a[7],
+                "exact": bool(a[8])}
+
+    def set_exact(self, exact: bool) -> None:
+        """Numeric mode of the staged path (the other paths are always exact)."""
+        check(load().sw_plan_set_exact(self._h, 1 if exact else 0))
+
+    def set_path(self, path: str = "staged", chunk_len: int = 0) -> None:
+        """Execution path of step/run: "two_pass", "staged" or "fused"."""
+        check(load().sw_plan_set_path(self._h, self.PATHS[path], int(chunk_len)))
 
     def close(self) -> None:
         if getattr(self, "_h", None) is not None and self._h.value:

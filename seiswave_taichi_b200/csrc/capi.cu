@@ -12,7 +12,10 @@
 #include <vector>
 
 #include "sw_device.cuh"
+#include <type_traits>
+
 #include "sw_fused.cuh"
+#include "sw_staged.cuh"
 
 namespace sw {
 template <typename T> cudaError_t sw3_velocity(const P3<T>&, int, int, bool, bool, cudaStream_t);
@@ -70,7 +73,13 @@ struct sw_plan {
   sw::FusedExtra fx{};
   void* fused_buf = nullptr;
   int* d_err = nullptr;
-  int use_fused = 1;
+  // TMA-staged two-pass path (3D float CPML schemes)
+  bool staged = false;
+  sw::StagedMaps svm{}, ssm{};
+  sw::StagedArgs sa{};
+  int staged_grid = 0, staged_N = 0;
+  // 0: register-queue two-pass kernels, 1: staged two-pass, 2: fused single pass
+  int path = 0;
 };
 
 namespace {
@@ -198,6 +207,8 @@ int make_p3(sw_plan* pl, const sw3d_desc* d, sw::P3<T>& p) {
   p.x_chunk = choose_x_chunk(d->nx, d->ny, d->nz);
   const double hs[3] = {d->dx, d->dy, d->dz};
   set_divisors<T>(p.rd, &p.fast_div, hs, 3);
+  for (int a = 0; a < 3; ++a)
+    for (int m = 0; m < SW_MAX_ORDER; ++m) p.cs[a][m] = (T)(d->coef[m] / hs[a]);
   (void)pl;
   return SW_OK;
 }
@@ -259,6 +270,16 @@ cudaError_t enqueue3(sw_plan* pl, const sw::P3<T>& p, int it, bool first, bool l
     if (e != cudaSuccess) return e;
   }
   const bool force = pl->src_kind == SW_SRC_FORCE;
+  if constexpr (std::is_same<T, float>::value) {
+    if (pl->path >= 1 && pl->staged) {
+      const bool inject_next = moment && !last;
+      e = sw::sw3_staged_step(pl->staged_N, tensor, p, pl->svm, pl->ssm, pl->sa, pl->staged_grid, it, force,
+                              inject_next, pl->gather_in_stress, st);
+      if (e != cudaSuccess) return e;
+      if (!pl->gather_in_stress) e = sw::sw3_gather<T>(p, it, st);
+      return e;
+    }
+  }
   e = sw::sw3_velocity<T>(q, pl->order, it, tensor, force && pl->src_in_kernel, st);
   if (e != cudaSuccess) return e;
   if (force && !pl->src_in_kernel) {
@@ -349,8 +370,10 @@ void setup_fused(sw_plan* pl) {
   }
   float* buf = nullptr;
   if (cudaMalloc(&buf, total * sizeof(float)) != cudaSuccess) { cudaGetLastError(); return; }
-  if (cudaMalloc(&pl->d_err, sizeof(int)) != cudaSuccess) { cudaFree(buf); cudaGetLastError(); return; }
-  cudaMemset(pl->d_err, 0, sizeof(int));
+  if (!pl->d_err) {
+    if (cudaMalloc(&pl->d_err, sizeof(int)) != cudaSuccess) { cudaFree(buf); cudaGetLastError(); return; }
+    cudaMemset(pl->d_err, 0, sizeof(int));
+  }
   cudaMemset(buf, 0, total * sizeof(float));
   auto& x = pl->fx;
   float* cur = buf;
@@ -361,13 +384,76 @@ void setup_fused(sw_plan* pl) {
   }
   x.err = pl->d_err;
   if (!sw::sw3_fused_maps(N, p, x, &pl->fmaps)) {
-    cudaFree(buf); cudaFree(pl->d_err); pl->d_err = nullptr;
+    cudaFree(buf);
     return;
   }
   pl->fused_grid = choose_fused_grid(pl, fc);
   pl->fused_buf = buf;
   pl->fused_N = N;
   pl->fused = true;
+}
+
+int units_grid(int units, int per_sm) {
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int cap = sms * per_sm;
+  return units < cap ? units : cap;
+}
+
+void staged_chunks(sw_plan* pl, int len) {
+  const auto& p = pl->p3f;
+  sw::StagedConfig sc;
+  sw::sw3_staged_config(pl->staged_N, &sc);
+  auto& a = pl->sa;
+  a.tiles_y = (p.ny + sc.TY - 1) / sc.TY;
+  a.tiles_z = (p.nz + 31) / 32;
+  if (len <= 0) {
+    // about five work units per resident CTA
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int tiles = a.tiles_y * a.tiles_z;
+    int chunks = (10 * sms + tiles - 1) / tiles;
+    len = (p.nx + chunks - 1) / chunks;
+  }
+  if (len < 2 * pl->staged_N + 2) len = 2 * pl->staged_N + 2;
+  a.chunk_len = len;
+  a.chunks = (p.nx + len - 1) / len;
+  int dev = 0, maxsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+  const size_t big = sc.vel_smem > sc.str_smem ? sc.vel_smem : sc.str_smem;
+  int per_sm = (int)((size_t)maxsm / (big + 1024));
+  if (per_sm < 1) per_sm = 1;
+  pl->staged_grid = units_grid(a.tiles_y * a.tiles_z * a.chunks, per_sm);
+}
+
+void setup_staged(sw_plan* pl) {
+  pl->staged = false;
+  if (pl->dim != 3 || pl->dtype != SW_F32) return;
+  if (pl->scheme != SW3D_CPML_TENSOR && pl->scheme != SW3D_CPML_FORCE) return;
+  if (!pl->src_in_kernel) return;
+  sw::StagedConfig sc;
+  if (!sw::sw3_staged_config(pl->order, &sc)) return;
+  auto& p = pl->p3f;
+  if (p.nz % 4 != 0) return;
+  for (int q = 0; q < 9; ++q)
+    if (!aligned(p.f[q], 16)) return;
+  if (!aligned(p.rho, 16) || !aligned(p.lam, 16) || !aligned(p.mu, 16)) return;
+  int dev = 0, maxsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if ((size_t)maxsm < sc.vel_smem || (size_t)maxsm < sc.str_smem) return;
+  if (!pl->d_err) {
+    if (cudaMalloc(&pl->d_err, sizeof(int)) != cudaSuccess) { cudaGetLastError(); return; }
+    cudaMemset(pl->d_err, 0, sizeof(int));
+  }
+  if (!sw::sw3_staged_maps(pl->order, p, &pl->svm, &pl->ssm)) return;
+  pl->staged_N = pl->order;
+  pl->sa.err = pl->d_err;
+  pl->sa.exact = 1;
+  staged_chunks(pl, 0);
+  pl->staged = true;
+  pl->path = 1;
 }
 
 // nsteps >= 2 steps through the fused kernel (the last one two-pass when odd)
@@ -395,7 +481,7 @@ cudaError_t enqueue_fused_run(sw_plan* pl, int it0, int nsteps, cudaStream_t st)
 }
 
 cudaError_t enqueue_sequence(sw_plan* pl, int it0, int nsteps, cudaStream_t st) {
-  if (pl->fused && pl->use_fused && nsteps >= 2) return enqueue_fused_run(pl, it0, nsteps, st);
+  if (pl->fused && pl->path == 2 && nsteps >= 2) return enqueue_fused_run(pl, it0, nsteps, st);
   for (int s = 0; s < nsteps; ++s) {
     cudaError_t e = enqueue_step(pl, it0 + s, s == 0, s == nsteps - 1, false, 0.0, st);
     if (e != cudaSuccess) return e;
@@ -519,7 +605,7 @@ int sw3d_plan_create(const sw3d_desc* d, sw_plan** out) {
   for (int q = 0; q < 9; ++q) pl->fields[q] = d->field[q];
   if (d->dtype == SW_F32) make_p3<float>(pl, d, pl->p3f);
   else make_p3<double>(pl, d, pl->p3d);
-  setup_fused(pl);
+  setup_staged(pl);
   *out = pl;
   return SW_OK;
 }
@@ -550,29 +636,41 @@ int sw_plan_status(sw_plan* pl, void* stream) {
 
 int sw_plan_info(sw_plan* pl, int32_t* info) {
   if (!pl || !info) return fail(SW_ERR_ARG, "null plan or output");
-  info[0] = pl->fused ? 1 : 0;
+  info[0] = pl->path;
   info[1] = pl->dim == 3 ? (pl->dtype == SW_F32 ? pl->p3f.fast_div : 0) : (pl->dtype == SW_F32 ? pl->p2f.fast_div : 0);
-  info[2] = pl->fused ? pl->fused_grid : 0;
-  info[3] = pl->fused ? pl->fx.chunk_len : 0;
-  info[4] = pl->dim == 3 ? (pl->dtype == SW_F32 ? pl->p3f.x_chunk : pl->p3d.x_chunk) : 0;
-  info[5] = pl->use_fused;
+  info[2] = pl->staged ? 1 : 0;
+  info[3] = pl->staged ? pl->staged_grid : 0;
+  info[4] = pl->staged ? pl->sa.chunk_len : 0;
+  info[5] = pl->fused ? 1 : 0;
+  info[6] = pl->fused ? pl->fused_grid : 0;
+  info[7] = pl->fused ? pl->fx.chunk_len : 0;
+  info[8] = pl->staged ? pl->sa.exact : 1;
   return SW_OK;
 }
 
-int sw_plan_set_path(sw_plan* pl, int32_t use_fused, int32_t chunk_len) {
+int sw_plan_set_path(sw_plan* pl, int32_t path, int32_t chunk_len) {
   if (!pl) return fail(SW_ERR_ARG, "null plan");
-  pl->use_fused = use_fused ? 1 : 0;
-  if (chunk_len > 0 && pl->fused) {
+  if (path < 0 || path > 2) return fail(SW_ERR_ARG, "path must be 0, 1 or 2");
+  if (path == 1 && !pl->staged) return fail(SW_ERR_UNSUPPORTED, "this plan has no staged path");
+  if (path == 2 && !pl->fused) setup_fused(pl);  // allocates the second buffer set on first use
+  if (path == 2 && !pl->fused) return fail(SW_ERR_UNSUPPORTED, "this plan has no fused path");
+  pl->path = path;
+  if (chunk_len > 0 && path == 1) staged_chunks(pl, chunk_len);
+  if (chunk_len > 0 && path == 2) {
     sw::FusedConfig fc;
     sw::sw3_fused_config(pl->fused_N, &fc);
     int len = chunk_len < 2 * fc.N ? 2 * fc.N : chunk_len;
     pl->fx.chunk_len = len;
     pl->fx.chunks = (pl->p3f.nx + len - 1) / len;
-    int dev = 0, sms = 148;
-    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int units = pl->fx.tiles_y * pl->fx.tiles_z * pl->fx.chunks;
-    pl->fused_grid = units < sms ? units : sms;
+    pl->fused_grid = units_grid(pl->fx.tiles_y * pl->fx.tiles_z * pl->fx.chunks, 1);
   }
+  if (pl->gexec) { cudaGraphExecDestroy(pl->gexec); pl->gexec = nullptr; pl->g_it0 = pl->g_n = -1; }
+  return SW_OK;
+}
+
+int sw_plan_set_exact(sw_plan* pl, int32_t exact) {
+  if (!pl) return fail(SW_ERR_ARG, "null plan");
+  pl->sa.exact = exact ? 1 : 0;
   if (pl->gexec) { cudaGraphExecDestroy(pl->gexec); pl->gexec = nullptr; pl->g_it0 = pl->g_n = -1; }
   return SW_OK;
 }

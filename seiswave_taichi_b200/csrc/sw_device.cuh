@@ -54,6 +54,7 @@ struct P3 {
   int x_chunk;              // x planes streamed by one CTA
   T rd[3];                  // RN(1/dx), RN(1/dy), RN(1/dz)
   int fast_div;             // div_c may use the verified constant-divisor path
+  T cs[3][SW_MAX_ORDER];    // c_m / dx, c_m / dy, c_m / dz (fast numeric mode)
 };
 
 // 2D memory-variable components, 4 per direction, shared by all schemes:
@@ -102,12 +103,17 @@ __device__ __forceinline__ T div_v(T x, T d) {
 // innocuous?", SIGNUM Newsletter 30(3), 1995), so the result equals the
 // correctly rounded float quotient.  Float inputs are normal doubles, so the
 // double division never leaves its own fast path.
+// Out of line so the rare path does not bloat every call site.
+static __device__ __noinline__ float div_rare(float x, float d) {
+  if (x == 0.f) return x;  // +-0/d = +-0 for d > 0
+  return __double2float_rn(__ddiv_rn((double)x, (double)d));
+}
+
 template <>
 __device__ __forceinline__ float div_v<float>(float x, float d) {
   const unsigned ex = (__float_as_uint(x) >> 23) & 0xffu;  // biased exponent
   if (ex - 27u < 200u) return __fdiv_rn(x, d);                // |x| in [2^-100, 2^100)
-  if (x == 0.f) return x;                                   // +-0/d = +-0 for d > 0
-  return __double2float_rn(__ddiv_rn((double)x, (double)d));
+  return div_rare(x, d);
 }
 
 // x / d for a divisor fixed for the run (dx, dy, dz), r = RN(1/d).  With
@@ -119,12 +125,15 @@ __device__ __forceinline__ float div_v<float>(float x, float d) {
 // that the whole function equals IEEE division x/d for every finite float x.
 __device__ __forceinline__ float div_c(float x, float d, float r, int fast) {
   const unsigned ex = (__float_as_uint(x) >> 23) & 0xffu;  // biased exponent
-  if (fast && ex - 27u < 200u) {
-    const float q = __fmul_rn(x, r);
-    const float e = __fmaf_rn(-q, d, x);
-    return __fmaf_rn(e, r, q);
+  if (ex - 27u < 200u) {
+    if (fast) {
+      const float q = __fmul_rn(x, r);
+      const float e = __fmaf_rn(-q, d, x);
+      return __fmaf_rn(e, r, q);
+    }
+    return __fdiv_rn(x, d);
   }
-  return div_v(x, d);
+  return div_rare(x, d);
 }
 __device__ __forceinline__ double div_c(double x, double d, double, int) { return div_v(x, d); }
 

@@ -9,7 +9,13 @@
 
 namespace sw {
 
-constexpr uint32_t SW_WAIT_LIMIT = 1u << 26;  // polls of try_wait (each may suspend ~us)
+constexpr uint64_t SW_WAIT_NS = 1000000000ull;  // give up a wait after one second
+
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -28,11 +34,12 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
                : "memory");
 }
 
-// true when the phase with the given parity has completed; false after the
-// poll limit (the caller reports a timeout)
+// true when the phase with the given parity has completed; false once
+// SW_WAIT_NS of wall time have passed (the caller reports a timeout)
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   const uint32_t a = smem_u32(bar);
-  for (uint32_t n = 0; n < SW_WAIT_LIMIT; ++n) {
+  uint64_t t0 = 0;
+  for (uint32_t n = 0;; ++n) {
     uint32_t done;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
@@ -40,8 +47,12 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
         : "r"(a), "r"(parity)
         : "memory");
     if (done) return true;
+    if ((n & 63) == 0) {
+      const uint64_t t = global_ns();
+      if (n == 0) t0 = t;
+      else if (t - t0 > SW_WAIT_NS) return false;
+    }
   }
-  return false;
 }
 
 // 3D tiled TMA load of box {c0 (innermost), c1, c2} into shared memory,

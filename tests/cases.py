@@ -66,7 +66,9 @@ def case3d(shape=(40, 36, 44), N=2, scheme="TENSOR", hetero=True, npml=8, nt=120
 
 
 def product3d(c, **kw):
+    """The drop-in solver for case c; exact numerics unless exact=False is passed."""
     import torch
+    kw.setdefault("exact", True)
     if c["scheme"] == "TENSOR":
         from seiswave_taichi_b200.Elastic3D_SSG_Tensor import ElasticWAVE
         w = ElasticWAVE(c["vs"], c["vp"], c["rho"], c["dx"], c["dy"], c["dz"], c["dt"], c["isx"], c["isy"],

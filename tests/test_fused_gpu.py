@@ -43,10 +43,9 @@ def test_fused_bitwise(cuda, kw, steps, chunk):
     c = case3d(nt=80, **kw)
     w = product3d(c)
     plan = w._build_plan()
+    plan.set_path("fused", chunk)
     info = plan.info()
-    assert info["fused"], info
-    if chunk:
-        plan.set_path(True, chunk)
+    assert info["fused"] and info["path"] == "fused", info
     wav = to_np(w._wavelet).astype(np.float32)
     o = oracle3d(c, wavelet=wav)
     w.run(steps)
@@ -58,7 +57,9 @@ def test_fused_bitwise(cuda, kw, steps, chunk):
 def test_fused_constant_divisor_verified(cuda):
     c = case3d(nt=10, dx=10.0, dy=12.5, dz=7.5)
     w = product3d(c)
-    info = w._build_plan().info()
+    plan = w._build_plan()
+    plan.set_path("fused")
+    info = plan.info()
     assert info["fused"] and info["fast_div"], info
 
 
@@ -66,8 +67,10 @@ def test_fused_in_two_runs_equals_one(cuda):
     """Splitting the loop (run(30) then run(33, it0=30)) gives the same state."""
     c = case3d(nt=80, shape=(38, 34, 40))
     a = product3d(c)
+    a._build_plan().set_path("fused")
     a.run(63)
     b = product3d(c)
+    b._build_plan().set_path("fused")
     b.run(30)
     b.run(33, it0=30)
     for f in F3:
@@ -78,10 +81,39 @@ def test_fused_in_two_runs_equals_one(cuda):
 def test_fused_matches_two_pass(cuda):
     c = case3d(nt=80, shape=(44, 40, 48), N=2)
     a = product3d(c)
+    a._build_plan().set_path("fused")
     a.run(80)
     b = product3d(c)
-    b._build_plan().set_path(False)
+    b._build_plan().set_path("two_pass")
     b.run(80)
     for f in F3:
         assert np.array_equal(to_np(getattr(a, f)), to_np(getattr(b, f))), f
     assert np.array_equal(to_np(a.data), to_np(b.data))
+
+
+@pytest.mark.parametrize("kw", CASES, ids=lambda k: "-".join(str(v) for v in k.values()))
+@pytest.mark.parametrize("steps,chunk", [(70, 0), (71, 7), (33, 13)])
+def test_staged_bitwise(cuda, kw, steps, chunk):
+    c = case3d(nt=80, **kw)
+    w = product3d(c)
+    plan = w._build_plan()
+    plan.set_path("staged", chunk)
+    assert plan.info()["path"] == "staged"
+    wav = to_np(w._wavelet).astype(np.float32)
+    o = oracle3d(c, wavelet=wav)
+    w.run(steps)
+    plan.status()
+    o.run(0, steps)
+    _check(w, o)
+
+
+def test_staged_is_default_and_per_step(cuda):
+    c = case3d(nt=40, shape=(40, 36, 44))
+    w = product3d(c)
+    assert w._build_plan().info()["path"] == "staged"
+    wav = to_np(w._wavelet).astype(np.float32)
+    o = oracle3d(c, wavelet=wav)
+    for it in range(40):
+        w.update_SSG(it)
+    o.run(0, 40)
+    _check(w, o)
