@@ -219,6 +219,26 @@ SW_API int sw_run(sw_plan* plan, int32_t it0, int32_t nsteps, int32_t use_graph,
  * returns SW_ERR_NONFINITE when it is non-zero. */
 SW_API int sw_check_finite(sw_plan* plan, void* stream, int64_t* nonfinite);
 
+/* No reference counterpart.  The scan of sw_check_finite over caller-named
+ * device arrays (arrays[a] holds lengths[a] elements of dtype SW_F32 or
+ * SW_F64), allocating no device memory: its counters live in a static device
+ * array of SW_NOALLOC_MAX_ARRAYS 64-bit words inside this library, and
+ * narrays above that limit is rejected with SW_ERR_ARG.  For hosts that may
+ * not allocate at this point: device memory owned by another allocator (a
+ * framework's memory pool), or a loop where cudaFree's device-wide
+ * synchronisation would stall other streams; sw_check_finite allocates its
+ * counter on first use and needs a plan.
+ * counts[a] receives array a's NaN/Inf count; returns SW_ERR_NONFINITE when
+ * any is non-zero.  Blocks on the stream.  Each call zeroes the counters it
+ * uses before its scan, so nothing must be zero on entry.  The first call on
+ * each device (that device current) resolves the counters' address with
+ * cudaGetSymbolAddress; make it before any stream capture.  The counters are
+ * shared by every caller on a device: calls that overlap in time on one device
+ * (several host threads) race and return mixed counts, so serialise them. */
+#define SW_NOALLOC_MAX_ARRAYS 64
+SW_API int sw_count_nonfinite_noalloc(const void* const* arrays, const int64_t* lengths, int32_t narrays,
+                                      int32_t dtype, void* stream, int64_t* counts);
+
 #ifdef __cplusplus
 }
 #endif

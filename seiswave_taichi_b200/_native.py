@@ -30,7 +30,7 @@ EXPORTS = (
     "sw_version", "sw_last_error", "sw2d_plan_create", "sw3d_plan_create",
     "sw_plan_set_tile", "sw_abi_sizeof", "sw_plan_destroy", "sw_step", "sw_step_amp",
     "sw_run", "sw_check_finite", "sw_plan_status", "sw_plan_info", "sw_plan_set_path",
-    "sw_plan_set_exact",
+    "sw_plan_set_exact", "sw_count_nonfinite_noalloc",
 )
 
 
@@ -116,6 +116,8 @@ def load() -> C.CDLL:
         "sw_plan_info": (C.c_int, [vp, C.POINTER(C.c_int32)]),
         "sw_plan_set_path": (C.c_int, [vp, C.c_int32, C.c_int32]),
         "sw_plan_set_exact": (C.c_int, [vp, C.c_int32]),
+        "sw_count_nonfinite_noalloc": (C.c_int, [C.POINTER(vp), C.POINTER(C.c_int64), C.c_int32, C.c_int32, vp,
+                                                 C.POINTER(C.c_int64)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -130,6 +132,29 @@ def struct_sizes() -> dict:
     lib = load()
     ours = [PmlAxis, Receivers, Source, Desc2D, Desc3D]
     return {t.__name__: (C.sizeof(t), lib.sw_abi_sizeof(q)) for q, t in enumerate(ours)}
+
+
+NOALLOC_MAX_ARRAYS = 64
+
+
+def count_nonfinite_noalloc(tensors, stream: int = 0) -> list[int]:
+    """Per-tensor NaN/Inf counts through sw_count_nonfinite_noalloc, which
+    allocates no device memory (at most NOALLOC_MAX_ARRAYS contiguous tensors
+    of one dtype, float32 or float64)."""
+    import torch
+    n = len(tensors)
+    if n and any(t.dtype != tensors[0].dtype for t in tensors):
+        raise ValueError("tensors must share one dtype")
+    if any(not t.is_contiguous() for t in tensors):
+        raise ValueError("tensors must be contiguous")
+    dt = SW_F64 if n and tensors[0].dtype == torch.float64 else SW_F32
+    arr = (C.c_void_p * max(n, 1))(*[ptr(t) for t in tensors])
+    lens = (C.c_int64 * max(n, 1))(*[t.numel() for t in tensors])
+    out = (C.c_int64 * max(n, 1))()
+    rc = load().sw_count_nonfinite_noalloc(arr, lens, n, dt, C.c_void_p(stream), out)
+    if rc not in (SW_OK, SW_ERR_NONFINITE):
+        check(rc)
+    return [int(out[a]) for a in range(n)]
 
 
 class SeisWaveError(RuntimeError):

@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -760,6 +761,89 @@ int sw_check_finite(sw_plan* pl, void* stream, int64_t* nonfinite) {
   if (e != cudaSuccess) return cuda_fail(e, "sw_check_finite");
   *nonfinite = (int64_t)h;
   if (h) return fail(SW_ERR_NONFINITE, "wavefield holds " + std::to_string(h) + " non-finite values");
+  return SW_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// sw_count_nonfinite_noalloc: the NaN/Inf scan of sw_check_finite over arrays
+// the caller names, with its counters in a static device array instead of
+// plan memory, so that the call allocates nothing.
+// ---------------------------------------------------------------------------
+namespace {
+
+// One 64-bit counter per scanned array (SW_NOALLOC_MAX_ARRAYS * 8 = 512
+// bytes).  Every call zeroes the counters it uses on its stream before the
+// scan, so nothing has to be zero on entry.
+static __device__ __align__(256) unsigned long long g_noalloc_count[SW_NOALLOC_MAX_ARRAYS];
+
+constexpr int kNoallocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+unsigned long long* g_noalloc_ptr[kNoallocMaxDevices] = {};
+
+// Address of the counters on the current device, resolved once per device.
+int noalloc_scratch(unsigned long long** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e, "sw_count_nonfinite_noalloc: current device");
+  if (dev < 0 || dev >= kNoallocMaxDevices)
+    return fail(SW_ERR_UNSUPPORTED, "sw_count_nonfinite_noalloc: device ordinal " + std::to_string(dev) +
+                                        " is beyond the " + std::to_string(kNoallocMaxDevices) + " this build tracks");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    unsigned long long* p = nullptr;
+    e = cudaGetSymbolAddress((void**)&p, g_noalloc_count);
+    if (e != cudaSuccess) return cuda_fail(e, "sw_count_nonfinite_noalloc: scratch address");
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return SW_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sw_count_nonfinite_noalloc(const void* const* arrays, const int64_t* lengths, int32_t narrays, int32_t dtype,
+                               void* stream, int64_t* counts) {
+  if (narrays < 0 || narrays > SW_NOALLOC_MAX_ARRAYS)
+    return fail(SW_ERR_ARG, "sw_count_nonfinite_noalloc: " + std::to_string(narrays) +
+                                " arrays requested; the static scratch holds counters for at most " +
+                                std::to_string(SW_NOALLOC_MAX_ARRAYS));
+  if (narrays > 0 && (!arrays || !lengths || !counts))
+    return fail(SW_ERR_ARG, "sw_count_nonfinite_noalloc: null arrays, lengths or counts");
+  if (dtype != SW_F32 && dtype != SW_F64) return fail(SW_ERR_ARG, "sw_count_nonfinite_noalloc: dtype");
+  for (int a = 0; a < narrays; ++a) {
+    if (lengths[a] < 0) return fail(SW_ERR_ARG, "sw_count_nonfinite_noalloc: negative length");
+    if (lengths[a] > 0 && !arrays[a]) return fail(SW_ERR_ARG, "sw_count_nonfinite_noalloc: null array");
+  }
+  if (narrays == 0) return SW_OK;
+  unsigned long long* cnt = nullptr;
+  int rc = noalloc_scratch(&cnt);
+  if (rc != SW_OK) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e = cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * narrays, st);
+  if (e != cudaSuccess) return cuda_fail(e, "sw_count_nonfinite_noalloc: reset");
+  for (int a = 0; a < narrays; ++a) {
+    if (lengths[a] == 0) continue;
+    if (dtype == SW_F32)
+      k_count_nonfinite<float><<<1184, 256, 0, st>>>((const float*)arrays[a], lengths[a], cnt + a);
+    else
+      k_count_nonfinite<double><<<1184, 256, 0, st>>>((const double*)arrays[a], lengths[a], cnt + a);
+  }
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "sw_count_nonfinite_noalloc: launch");
+  unsigned long long h[SW_NOALLOC_MAX_ARRAYS];
+  e = cudaMemcpyAsync(h, cnt, sizeof(unsigned long long) * narrays, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(e, "sw_count_nonfinite_noalloc");
+  unsigned long long total = 0;
+  for (int a = 0; a < narrays; ++a) {
+    counts[a] = (int64_t)h[a];
+    total += h[a];
+  }
+  if (total) return fail(SW_ERR_NONFINITE, "arrays hold " + std::to_string(total) + " non-finite values");
   return SW_OK;
 }
 
