@@ -41,9 +41,9 @@ sys.path.insert(0, str(ROOT))
 
 FALLBACK_HBM_GBS = 6650.0
 
-# DRAM bytes per time step (velocity + stress pass) from ncu, scaled to the
-# full workload; summaries under profiles/.  None until captured.
-NCU_TRAFFIC_PER_STEP = {}
+# DRAM bytes per time step (velocity + stress launch pair, default path and
+# numerics) from one ncu capture of the full workload (profiles/).
+NCU_TRAFFIC_PER_STEP = {"3d-ssg-cpml-tensor-200^3-nt1000": (450.352128 + 126.629888 + 531.473920 + 210.652416) * 1e6}
 
 
 def peaks():

@@ -113,6 +113,7 @@ template <>
 __device__ __forceinline__ float div_v<float>(float x, float d) {
   const unsigned ex = (__float_as_uint(x) >> 23) & 0xffu;  // biased exponent
   if (ex - 27u < 200u) return __fdiv_rn(x, d);                // |x| in [2^-100, 2^100)
+  if ((__float_as_uint(x) << 1) == 0u) return x;              // +-0/d = +-0 for d > 0
   return div_rare(x, d);
 }
 
@@ -133,6 +134,7 @@ __device__ __forceinline__ float div_c(float x, float d, float r, int fast) {
     }
     return __fdiv_rn(x, d);
   }
+  if ((__float_as_uint(x) << 1) == 0u) return x;  // +-0/d = +-0 for d > 0
   return div_rare(x, d);
 }
 __device__ __forceinline__ double div_c(double x, double d, double, int) { return div_v(x, d); }
