@@ -123,7 +123,7 @@ def build_solver2d(cfg, torch):
     from seiswave_taichi_b200.Elastic2D_CPML import ElasticWAVE
     w = ElasticWAVE(cfg["vs"], cfg["vp"], cfg["rho"], cfg["dx"], cfg["dz"], cfg["dt"], cfg["isx"],
                     cfg["isz"], cfg["rsx"], cfg["rsz"], cfg["nt"], cfg["accuracy"], cfg["freq"],
-                    torch.float32)
+                    torch.float32, MT=cfg.get("MT"), src_scale=cfg.get("src_scale", 1.0))
     w.SetADEPML2D(cfg["surface"], cfg["pml"])
     return w
 
@@ -157,9 +157,15 @@ def cpu_baseline(cfg, min_seconds=10.0, max_steps=60):
                        src_scale=cfg["src_scale"])
         step = lambda it, n: o.run(it, n)
     else:
+        from seiswave_taichi_b200 import BaseFun
+        from seiswave_taichi_b200.Elastic2D_CPML import moment_2d
+        wav = BaseFun.series("ricker2", cfg["nt"], cfg["dt"], cfg["freq"], cfg.get("src_scale", 1.0),
+                             t0=np.float32(1.5) / np.float32(cfg["freq"]))
+        table = cfg["rsx"].reshape(-1) * cfg["shape"][1] + cfg["rsz"].reshape(-1)
         o = O.Oracle2D(cfg["vs"], cfg["vp"], cfg["rho"], cfg["dx"], cfg["dz"], cfg["dt"], cfg["isx"], cfg["isz"],
                        int(cfg["rsx"].reshape(-1)[0]), int(cfg["rsz"].reshape(-1)[0]), cfg["nt"],
-                       cfg["accuracy"], cfg["freq"], cfg["surface"], cfg["pml"])
+                       cfg["accuracy"], cfg["freq"], cfg["surface"], cfg["pml"], wavelet=wav,
+                       MT=moment_2d(cfg["MT"]) if cfg.get("MT") is not None else None, rec_index=table)
         step = lambda it, n: o.run("VS", it, n)
     step(0, 1)  # first touch of the state pages
     ncell = int(np.prod(cfg["shape"]))

@@ -20,7 +20,8 @@
  *
  * Threading: work is enqueued on the caller's stream (a cudaStream_t passed as
  * void*, NULL = legacy default stream).  A plan is not thread-safe; use one plan
- * per stream.  No call blocks the host except sw_check_finite.
+ * per stream.  No call blocks the host except sw_check_finite,
+ * sw_count_nonfinite_noalloc and sw_plan_status.
  */
 #ifndef SEISWAVE_H
 #define SEISWAVE_H
@@ -213,6 +214,35 @@ SW_API int sw_step_amp(sw_plan* plan, int32_t it, double amplitude, void* stream
  * `for i in range(nt): obj.update_*(i)` (e.g. test2d_homegenous.py:55-56),
  * replayed from a cached CUDA graph when use_graph != 0. */
 SW_API int sw_run(sw_plan* plan, int32_t it0, int32_t nsteps, int32_t use_graph, void* stream);
+
+/* ---- 2D adjoint (no reference counterpart) --------------------------------
+ * Hand-written discrete adjoint of the SW2D_SSG_VS time loop with a
+ * SW_SRC_MOMENT (or no) source and vz receivers, for gradients of a seismogram
+ * misfit with respect to the material.  sw2d_record runs forward steps
+ * it0..it0+nsteps-1 from the plan's current state and stores nsteps+1
+ * snapshots of sw2d_snapshot_elems() elements each; sw2d_adjoint_run then
+ * steps the adjoint state from it0+nsteps-1 down to it0 using them.  Together
+ * they replace one checkpoint segment of the reference loop
+ * (Elastic2D_CPML.py:128-200) run backwards. */
+typedef struct sw2d_adjoint_desc {
+  void* field[5];            /* adjoint of vx vz sxx szz sxz, (nx, nz) each    */
+  void* mem[2];              /* adjoint memory variables, layout of sw2d_desc.mem */
+  void* tmp[4];              /* scratch, (nx, nz) each                          */
+  void* grad[5];             /* per-cell sums, added to: G_vx (coefficient
+                                dt/rho of vx), G_vz (dt/rho4 of vz), G_lpm
+                                (lambda+2mu at sxx), G_lhx (lambda at sxx),
+                                G_mhz (mu at sxz); see the Python wrapper for
+                                the chain to rho, lambda, mu                    */
+  const void* residual;      /* (nt_max, nrec): d misfit / d data              */
+} sw2d_adjoint_desc;
+
+/* Elements (of the plan's dtype) in one snapshot slot. */
+SW_API int sw2d_snapshot_elems(sw_plan* plan, int64_t* elems);
+/* Forward steps with snapshots: snap holds (nsteps+1) slots. */
+SW_API int sw2d_record(sw_plan* plan, int32_t it0, int32_t nsteps, void* snap, void* stream);
+/* Adjoint steps it0+nsteps-1 .. it0 over the snapshots of sw2d_record(it0, nsteps). */
+SW_API int sw2d_adjoint_run(sw_plan* plan, const sw2d_adjoint_desc* adj, int32_t it0, int32_t nsteps,
+                            const void* snap, void* stream);
 
 /* Scan every wavefield for NaN/Inf; blocks on the stream.  *nonfinite is set
  * to the number of non-finite values found (0 when the state is finite);

@@ -33,7 +33,9 @@ class O2Desc(C.Structure):
                [(n, C.c_void_p) for n in ("vx", "vz", "sxx", "szz", "sxz", "rho", "lam", "mu")] + \
                [("mem", C.c_void_p * 10), ("ax", OAxis * 2),
                 ("isx", C.c_int32), ("isz", C.c_int32), ("rsx", C.c_int32), ("rsz", C.c_int32),
-                ("f0", C.c_double), ("wavelet", C.c_void_p), ("data", C.c_void_p)]
+                ("f0", C.c_double), ("wavelet", C.c_void_p), ("data", C.c_void_p),
+                ("src_kind", C.c_int32), ("nrec", C.c_int32), ("mt", C.c_double * 3),
+                ("rec_idx", C.c_void_p)]
 
 
 class O3Desc(C.Structure):
@@ -129,7 +131,11 @@ class Oracle2D:
     """CPU run of Elastic2D_CPML (schemes 'VS', 'SV', 'RSG')."""
 
     def __init__(self, vs, vp, rho, dx, dz, dt, isx, isz, rsx, rsz, nt, accuracy, freq,
-                 pml_surface, pml_parameter, dtype=np.float32, wavelet=None, coef=None):
+                 pml_surface, pml_parameter, dtype=np.float32, wavelet=None, coef=None, MT=None,
+                 rec_index=None):
+        """MT (xx, zz, xz) selects the moment-tensor source (wavelet required);
+        rec_index (linear cell indices) records (nt, nrec) traces instead of
+        the single receiver (rsx, rsz)."""
         T = dtype
         self.T = T
         self.vs = np.ascontiguousarray(vs, dtype=T)
@@ -143,7 +149,8 @@ class Oracle2D:
         z = lambda: np.zeros((nx, nz), T)
         self.vx, self.vz, self.sxx, self.szz, self.sxz = z(), z(), z(), z(), z()
         self.mem = [z() for _ in range(10)]
-        self.data = np.zeros(nt, T)
+        self.rec_index = None if rec_index is None else np.ascontiguousarray(rec_index, np.int64).reshape(-1)
+        self.data = np.zeros(nt, T) if self.rec_index is None else np.zeros((nt, self.rec_index.size), T)
         p = pml_parameter
         self.axes = []
         for a, (n, h, th) in enumerate(((nx, dx, p["pml_x_thick"]), (nz, dz, p["pml_z_thick"]))):
@@ -168,6 +175,15 @@ class Oracle2D:
         d.f0 = freq
         d.wavelet = _p(self.wavelet)
         d.data = self.data.ctypes.data
+        if MT is not None:
+            if self.wavelet is None:
+                raise ValueError("the moment-tensor source needs its wavelet")
+            d.src_kind = 1
+            for q in range(3):
+                d.mt[q] = float(MT[q])
+        if self.rec_index is not None:
+            d.nrec = int(self.rec_index.size)
+            d.rec_idx = self.rec_index.ctypes.data
         self.desc = d
 
     def run(self, scheme: str, it0: int, n: int, rsg_sources=None):

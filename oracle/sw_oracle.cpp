@@ -58,6 +58,12 @@ struct O2Desc {
   double f0;
   const float* wavelet;           // per-step source value (float), or null
   void* data;                     // receiver trace, length >= it (dtype)
+  // moment-tensor source and receiver arrays (no reference counterpart; they
+  // follow Elastic3D_SSG_Tensor.py's conventions in two dimensions)
+  int32_t src_kind;               // 0: the scheme's point force, 1: moment tensor
+  int32_t nrec;                   // 0: one receiver (rsx, rsz); else rec_idx[nrec]
+  double mt[3];                   // xx zz xz
+  const int64_t* rec_idx;         // linear cell indices; data is (nt, nrec)
 };
 
 struct O3Desc {
@@ -186,12 +192,34 @@ struct S2 {
   }
 };
 
+// 2D moment-tensor source at the start of the step, in the convention of
+// Elastic3D_SSG_Tensor.py:186-193: sigma_ab[src] += w * (-M_ab)
+template <typename T>
+void inject2d_moment(const O2Desc& d, S2<T>& s, int it) {
+  const T w = (T)d.wavelet[it];
+  s.sxx(d.isx, d.isz) += w * (-(T)(float)d.mt[0]);
+  s.szz(d.isx, d.isz) += w * (-(T)(float)d.mt[1]);
+  s.sxz(d.isx, d.isz) += w * (-(T)(float)d.mt[2]);
+}
+
+// receivers after the stress phase: one cell (rsx, rsz) or a table
+template <typename T>
+void record2d(const O2Desc& d, const G2<T>& f, int it) {
+  if (!d.data) return;
+  if (d.nrec <= 0) {
+    ((T*)d.data)[it] = f(d.rsx, d.rsz);
+    return;
+  }
+  for (int r = 0; r < d.nrec; ++r) ((T*)d.data)[(long long)it * d.nrec + r] = f.p[d.rec_idx[r]];
+}
+
 // Elastic2D_CPML.py:128-200
 template <typename T>
 void step2d_vs(const O2Desc& d, int it) {
   S2<T> s(d);
   const int N = s.N, nx = s.nx, nz = s.nz;
   const T dx = s.dx, dz = s.dz, dt = s.dt;
+  if (d.src_kind == 1) inject2d_moment(d, s, it);
   // update vx  :144-154
 #pragma omp parallel for
   for (int i = N + 1; i < nx - N; ++i)
@@ -224,7 +252,7 @@ void step2d_vs(const O2Desc& d, int it) {
       s.vz(i, j) += (dszzdz + dsxzdx) * dt / rh;
     }
   // source :170
-  {
+  if (d.src_kind == 0) {
     float f0 = (float)d.f0;
     float w = d.wavelet ? d.wavelet[it] : ricker2(it, (float)d.dt, 1.5f / f0, f0, 1.0f);
     s.vz(d.isx, d.isz) += dt * (T)w / s.rho(d.isx, d.isz);
@@ -265,7 +293,7 @@ void step2d_vs(const O2Desc& d, int it) {
       s.sxz(i, j) += mhz * (dvxdz + dvzdx) * dt;
     }
   // receiver :200
-  if (d.data) ((T*)d.data)[it] = s.vz(d.rsx, d.rsz);
+  record2d(d, s.vz, it);
 }
 
 // Elastic2D_CPML.py:203-274
@@ -274,6 +302,7 @@ void step2d_sv(const O2Desc& d, int it) {
   S2<T> s(d);
   const int N = s.N, nx = s.nx, nz = s.nz;
   const T dx = s.dx, dz = s.dz, dt = s.dt;
+  if (d.src_kind == 1) inject2d_moment(d, s, it);
   // vx :218-229
 #pragma omp parallel for
   for (int i = N; i < nx - N - 1; ++i)
@@ -307,7 +336,7 @@ void step2d_sv(const O2Desc& d, int it) {
       s.vz(i, j) += (dszzdz + dsxzdx) * dt / rhz;
     }
   // source :245
-  {
+  if (d.src_kind == 0) {
     float w = d.wavelet ? d.wavelet[it] : ricker(it, (float)d.dt, (float)d.f0, 1.0f);
     s.vx(d.isx, d.isz) += dt * (T)w / s.rho(d.isx, d.isz);
   }
@@ -345,7 +374,7 @@ void step2d_sv(const O2Desc& d, int it) {
       }
       s.sxz(i, j) += m4 * (dvxdz + dvzdx) * dt;
     }
-  if (d.data) ((T*)d.data)[it] = s.vx(d.rsx, d.rsz);
+  record2d(d, s.vx, it);
 }
 
 // Elastic2D_CPML.py:277-353 (source value passed by the caller)

@@ -13,6 +13,12 @@ Schemes (Elastic2D_CPML.py):
 Receivers may be single ints (data is (nt,)) or (1, nrec) / (nrec,) integer
 arrays (data is (nt, nrec)).
 
+Keyword MT (no reference counterpart) replaces the point force of the VS and
+SV schemes by a moment-tensor source in the convention of
+Elastic3D_SSG_Tensor.py:186-193, sigma_ab[isx, isz] += w(t) * (-M_ab) at the
+start of the step, with the scheme's own wavelet times src_scale: a 2x2
+[[xx, xz], [xz, zz]] or 3x3 tensor (its x-z block), or "explosive" (M = I).
+
 State on the device: vx vz sxx szz sxz (nx, nz); memory variables
 slab-compact, _mem[0] (4, Lx+Rx, nz) = sxx_dx sxz_dx dvx_dx dvz_dx and
 _mem[1] (4, nx, Lz+Rz) = sxz_dz szz_dz dvz_dz dvx_dz, shared by the three
@@ -39,9 +45,24 @@ MEM2 = {
 }
 
 
+def moment_2d(MT) -> np.ndarray:
+    """(xx, zz, xz) of a 2D moment tensor given as "explosive", a 2x2
+    [[xx, xz], [xz, zz]] array or a 3x3 tensor (its x-z block)."""
+    if isinstance(MT, str):
+        if MT != "explosive":
+            raise ValueError("MT must be an array or 'explosive'")
+        return np.array([1.0, 1.0, 0.0], np.float32)
+    M = np.asarray(MT, np.float32)
+    if M.shape == (2, 2):
+        return np.array([M[0, 0], M[1, 1], M[0, 1]], np.float32)
+    if M.shape == (3, 3):
+        return np.array([M[0, 0], M[2, 2], M[0, 2]], np.float32)
+    raise ValueError("MT must be 2x2, 3x3 or 'explosive'")
+
+
 class ElasticWAVE:
     def __init__(self, vs, vp, rho, dx, dz, dt, isx, isz, rsx, rsz, nt, accuracy=3, freq=100.,
-                 fieldtype=torch.float32, *, coef64=False):
+                 fieldtype=torch.float32, *, coef64=False, MT=None, src_scale=1.0):
         self._dt_torch = torch_dtype(fieldtype)
         self._np_dtype = np.float64 if self._dt_torch == torch.float64 else np.float32
         self._dev = device()
@@ -87,6 +108,8 @@ class ElasticWAVE:
         self._plans = {}
         self._wavelets = {}
         self._mem = [None, None]
+        self.MT = None if MT is None else moment_2d(MT)
+        self.src_scale = float(src_scale)
 
     # ---- reference helpers ------------------------------------------------
     def Compute_mu(self, fieldtype=None):
@@ -222,11 +245,11 @@ class ElasticWAVE:
             keep.append(m)
         if scheme == N.SW2D_SSG_VS:
             t0 = np.float32(1.5) / np.float32(self.f0)
-            wav = BaseFun.series("ricker2", self.nt, self.dt, self.f0, 1.0, t0=t0)
+            wav = BaseFun.series("ricker2", self.nt, self.dt, self.f0, self.src_scale, t0=t0)
             d.src.kind = N.SW_SRC_FORCE
             rec_field = 1  # vz (Elastic2D_CPML.py:200)
         elif scheme == N.SW2D_SSG_SV:
-            wav = BaseFun.series("ricker", self.nt, self.dt, self.f0, 1.0)
+            wav = BaseFun.series("ricker", self.nt, self.dt, self.f0, self.src_scale)
             d.src.kind = N.SW_SRC_FORCE
             rec_field = 0  # vx (Elastic2D_CPML.py:274)
         else:
@@ -238,6 +261,9 @@ class ElasticWAVE:
         self._wavelets[scheme] = wt
         d.src.i, d.src.j = self.isx, self.isz
         d.src.wavelet = wt.data_ptr()
+        if self.MT is not None and scheme != N.SW2D_RSG:
+            d.src.kind = N.SW_SRC_MOMENT
+            d.src.mt[0], d.src.mt[2], d.src.mt[4] = (float(v) for v in self.MT)
         if rec_field >= 0:
             ri = torch.as_tensor(self._rec_lin, dtype=torch.int64, device=self._dev)
             keep += [ri, self.data]
@@ -278,6 +304,13 @@ class ElasticWAVE:
         s = {"VS": N.SW2D_SSG_VS, "SV": N.SW2D_SSG_SV}[scheme]
         self._plan(s).run(int(it0), nt, use_graph, self._stream())
         return self
+
+    def forward_op(self, vp, vs, rho, checkpoint_every: int = 100):
+        """Differentiable seismogram: the VS scheme's (nt, nrec) traces as a
+        function of the vp, vs, rho tensors (device, the solver's dtype),
+        with the hand-written adjoint as backward (no reference counterpart)."""
+        from .adjoint import ForwardOp2D
+        return ForwardOp2D.apply(vp, vs, rho, self, int(checkpoint_every))
 
     def check_finite(self) -> int:
         return self._plan(N.SW2D_SSG_VS).check_finite(self._stream())

@@ -30,8 +30,14 @@ EXPORTS = (
     "sw_version", "sw_last_error", "sw2d_plan_create", "sw3d_plan_create",
     "sw_plan_set_tile", "sw_abi_sizeof", "sw_plan_destroy", "sw_step", "sw_step_amp",
     "sw_run", "sw_check_finite", "sw_plan_status", "sw_plan_info", "sw_plan_set_path",
-    "sw_plan_set_exact", "sw_count_nonfinite_noalloc",
+    "sw_plan_set_exact", "sw_count_nonfinite_noalloc", "sw2d_snapshot_elems", "sw2d_record",
+    "sw2d_adjoint_run",
 )
+
+
+class Adjoint2D(C.Structure):
+    _fields_ = [("field", C.c_void_p * 5), ("mem", C.c_void_p * 2), ("tmp", C.c_void_p * 4),
+                ("grad", C.c_void_p * 5), ("residual", C.c_void_p)]
 
 
 class PmlAxis(C.Structure):
@@ -118,6 +124,9 @@ def load() -> C.CDLL:
         "sw_plan_set_exact": (C.c_int, [vp, C.c_int32]),
         "sw_count_nonfinite_noalloc": (C.c_int, [C.POINTER(vp), C.POINTER(C.c_int64), C.c_int32, C.c_int32, vp,
                                                  C.POINTER(C.c_int64)]),
+        "sw2d_snapshot_elems": (C.c_int, [vp, C.POINTER(C.c_int64)]),
+        "sw2d_record": (C.c_int, [vp, C.c_int32, C.c_int32, vp, vp]),
+        "sw2d_adjoint_run": (C.c_int, [vp, C.POINTER(Adjoint2D), C.c_int32, C.c_int32, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

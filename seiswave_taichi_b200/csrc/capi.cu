@@ -25,7 +25,19 @@ template <typename T> cudaError_t sw3_moment_inject(const P3<T>&, int, cudaStrea
 template <typename T> cudaError_t sw3_force_inject(const P3<T>&, int, cudaStream_t);
 template <typename T> cudaError_t sw3_gather(const P3<T>&, int, cudaStream_t);
 template <typename T> cudaError_t sw3_spml_step(const P3<T>&, int, int, bool, cudaStream_t);
-template <typename T> cudaError_t sw2_step(const P2<T>&, int, int, int, T, bool, cudaStream_t);
+template <typename T> cudaError_t sw2_step(const P2<T>&, int, int, int, T, bool, bool, bool, cudaStream_t);
+template <typename T> cudaError_t sw2_moment_inject(const P2<T>&, int, cudaStream_t);
+template <typename T>
+struct A2 {
+  T* f[5];
+  T* mem[2];
+  T* tmp[4];
+  T* grad[5];
+  const T* res;
+  const T* snap0;
+  const T* snap1;
+};
+template <typename T> cudaError_t sw2_adjoint_step(const P2<T>&, const A2<T>&, int, int, cudaStream_t);
 }  // namespace sw
 
 namespace {
@@ -233,6 +245,11 @@ int make_p2(const sw2d_desc* d, sw::P2<T>& p) {
   p.mcomp[1] = (long long)d->nx * p.sn[1];
   p.src_kind = d->src.kind; p.si = d->src.i; p.sk = d->src.j;
   p.wav = (const T*)d->src.wavelet;
+  // 2D moment tensor: xx zz xz in mt[0], mt[2], mt[4], rounded through float
+  // like the 3D tensor source
+  p.mneg[0] = -(T)(float)d->src.mt[0];
+  p.mneg[1] = -(T)(float)d->src.mt[2];
+  p.mneg[2] = -(T)(float)d->src.mt[4];
   p.nrec = d->rec.nrec; p.rec_field = d->rec.field;
   p.rec_idx = (const long long*)d->rec.index; p.rec_data = d->rec.data;
   p.rec_f64 = d->rec.dtype == SW_F64;
@@ -299,12 +316,17 @@ cudaError_t enqueue_step(sw_plan* pl, int it, bool first, bool last, bool has_am
     return pl->dtype == SW_F32 ? enqueue3<float>(pl, pl->p3f, it, first, last, st)
                                : enqueue3<double>(pl, pl->p3d, it, first, last, st);
   }
+  // moment tensor: the stress pass of step it-1 adds step it's source, unless
+  // this is the first step of the sequence or a receiver records a stress
+  const bool moment = pl->src_kind == SW_SRC_MOMENT;
+  const bool fold = moment && pl->gather_in_stress;
+  const bool pre = moment && (first || !fold), nxt = fold && !last;
   if (pl->dtype == SW_F32) {
     float a = has_amp ? (float)amp : 0.f;
-    return sw::sw2_step<float>(pl->p2f, pl->scheme, pl->order, it, a, pl->gather_in_stress, st);
+    return sw::sw2_step<float>(pl->p2f, pl->scheme, pl->order, it, a, pl->gather_in_stress, pre, nxt, st);
   }
   double a = has_amp ? (double)(float)amp : 0.0;
-  return sw::sw2_step<double>(pl->p2d, pl->scheme, pl->order, it, a, pl->gather_in_stress, st);
+  return sw::sw2_step<double>(pl->p2d, pl->scheme, pl->order, it, a, pl->gather_in_stress, pre, nxt, st);
 }
 
 int check_it(sw_plan* pl, int it0, int n) {
@@ -534,7 +556,8 @@ int sw2d_plan_create(const sw2d_desc* d, sw_plan** out) {
       if (s.kind != SW_SRC_RSG4) return fail(SW_ERR_ARG, "RSG takes the SW_SRC_RSG4 source");
       if (s.i < 1 || s.i >= d->nx || s.j < 1 || s.j >= d->nz) return fail(SW_ERR_ARG, "RSG source block outside the grid");
     } else {
-      if (s.kind != SW_SRC_FORCE) return fail(SW_ERR_ARG, "2D SSG schemes take a SW_SRC_FORCE source");
+      if (s.kind != SW_SRC_FORCE && s.kind != SW_SRC_MOMENT)
+        return fail(SW_ERR_ARG, "2D SSG schemes take a SW_SRC_FORCE or SW_SRC_MOMENT source");
       if (s.i < 0 || s.i >= d->nx || s.j < 0 || s.j >= d->nz) return fail(SW_ERR_ARG, "source cell outside the grid");
       if (!s.wavelet) return fail(SW_ERR_ARG, "source wavelet missing");
     }
@@ -761,6 +784,123 @@ int sw_check_finite(sw_plan* pl, void* stream, int64_t* nonfinite) {
   if (e != cudaSuccess) return cuda_fail(e, "sw_check_finite");
   *nonfinite = (int64_t)h;
   if (h) return fail(SW_ERR_NONFINITE, "wavefield holds " + std::to_string(h) + " non-finite values");
+  return SW_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// 2D adjoint: forward recording and the reverse sweep
+// ---------------------------------------------------------------------------
+namespace {
+
+int adjoint_plan_ok(sw_plan* pl, const char* who) {
+  if (!pl) return fail(SW_ERR_ARG, std::string(who) + ": null plan");
+  if (pl->dim != 2 || pl->scheme != SW2D_SSG_VS)
+    return fail(SW_ERR_UNSUPPORTED, std::string(who) + ": the adjoint covers the 2D SSG_VS scheme");
+  if (pl->src_kind != SW_SRC_MOMENT && pl->src_kind != SW_SRC_NONE)
+    return fail(SW_ERR_UNSUPPORTED, std::string(who) + ": the adjoint covers moment-tensor sources");
+  return SW_OK;
+}
+
+template <typename T>
+long long snap_elems(const sw::P2<T>& p) {
+  return 5LL * p.nx * p.nz + 4 * p.mcomp[0] + 4 * p.mcomp[1];
+}
+
+template <typename T>
+cudaError_t snap_store(const sw::P2<T>& p, T* slot, cudaStream_t st) {
+  const long long nc = (long long)p.nx * p.nz;
+  cudaError_t e = cudaSuccess;
+  for (int q = 0; q < 5 && e == cudaSuccess; ++q)
+    e = cudaMemcpyAsync(slot + q * nc, p.f[q], nc * sizeof(T), cudaMemcpyDeviceToDevice, st);
+  if (e == cudaSuccess && p.mcomp[0] > 0)
+    e = cudaMemcpyAsync(slot + 5 * nc, p.mem[0], 4 * p.mcomp[0] * sizeof(T), cudaMemcpyDeviceToDevice, st);
+  if (e == cudaSuccess && p.mcomp[1] > 0)
+    e = cudaMemcpyAsync(slot + 5 * nc + 4 * p.mcomp[0], p.mem[1], 4 * p.mcomp[1] * sizeof(T),
+                        cudaMemcpyDeviceToDevice, st);
+  return e;
+}
+
+template <typename T>
+cudaError_t record2(sw_plan* pl, const sw::P2<T>& p, int it0, int n, T* snap, cudaStream_t st) {
+  const long long se = snap_elems(p);
+  for (int k = 0; k < n; ++k) {
+    const int it = it0 + k;
+    cudaError_t e = cudaSuccess;
+    if (pl->src_kind == SW_SRC_MOMENT) e = sw::sw2_moment_inject<T>(p, it, st);
+    if (e == cudaSuccess) e = snap_store(p, snap + k * se, st);
+    if (e == cudaSuccess) e = sw::sw2_step<T>(p, pl->scheme, pl->order, it, (T)0, pl->gather_in_stress, false, false, st);
+    if (e != cudaSuccess) return e;
+  }
+  return snap_store(p, snap + (long long)n * se, st);
+}
+
+template <typename T>
+cudaError_t adjoint2(sw_plan* pl, const sw::P2<T>& p, const sw2d_adjoint_desc* d, int it0, int n, const T* snap,
+                     cudaStream_t st) {
+  sw::A2<T> a{};
+  for (int q = 0; q < 5; ++q) a.f[q] = (T*)d->field[q];
+  for (int q = 0; q < 2; ++q) a.mem[q] = (T*)d->mem[q];
+  for (int q = 0; q < 4; ++q) a.tmp[q] = (T*)d->tmp[q];
+  for (int q = 0; q < 5; ++q) a.grad[q] = (T*)d->grad[q];
+  a.res = (const T*)d->residual;
+  const long long se = snap_elems(p);
+  for (int k = n - 1; k >= 0; --k) {
+    a.snap0 = snap + k * se;
+    a.snap1 = snap + (k + 1) * se;
+    cudaError_t e = sw::sw2_adjoint_step<T>(p, a, pl->order, it0 + k, st);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sw2d_snapshot_elems(sw_plan* pl, int64_t* elems) {
+  int rc = adjoint_plan_ok(pl, "sw2d_snapshot_elems");
+  if (rc != SW_OK) return rc;
+  if (!elems) return fail(SW_ERR_ARG, "sw2d_snapshot_elems: null output");
+  *elems = pl->dtype == SW_F32 ? snap_elems(pl->p2f) : snap_elems(pl->p2d);
+  return SW_OK;
+}
+
+int sw2d_record(sw_plan* pl, int32_t it0, int32_t nsteps, void* snap, void* stream) {
+  int rc = adjoint_plan_ok(pl, "sw2d_record");
+  if (rc != SW_OK) return rc;
+  if ((rc = check_it(pl, it0, nsteps)) != SW_OK) return rc;
+  if (!snap || !aligned(snap, dsize(pl->dtype))) return fail(SW_ERR_ARG, "sw2d_record: snapshot buffer");
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e = pl->dtype == SW_F32 ? record2<float>(pl, pl->p2f, it0, nsteps, (float*)snap, st)
+                                      : record2<double>(pl, pl->p2d, it0, nsteps, (double*)snap, st);
+  if (e != cudaSuccess) return cuda_fail(e, "sw2d_record");
+  return SW_OK;
+}
+
+int sw2d_adjoint_run(sw_plan* pl, const sw2d_adjoint_desc* d, int32_t it0, int32_t nsteps, const void* snap,
+                     void* stream) {
+  int rc = adjoint_plan_ok(pl, "sw2d_adjoint_run");
+  if (rc != SW_OK) return rc;
+  if ((rc = check_it(pl, it0, nsteps)) != SW_OK) return rc;
+  const int esz = dsize(pl->dtype);
+  if (!d || !snap || !aligned(snap, esz)) return fail(SW_ERR_ARG, "sw2d_adjoint_run: descriptor or snapshots");
+  for (int q = 0; q < 5; ++q)
+    if (!d->field[q] || !aligned(d->field[q], esz) || !d->grad[q] || !aligned(d->grad[q], esz))
+      return fail(SW_ERR_ARG, "sw2d_adjoint_run: adjoint field or gradient pointer");
+  for (int q = 0; q < 4; ++q)
+    if (!d->tmp[q] || !aligned(d->tmp[q], esz)) return fail(SW_ERR_ARG, "sw2d_adjoint_run: scratch pointer");
+  const long long mc0 = pl->dtype == SW_F32 ? pl->p2f.mcomp[0] : pl->p2d.mcomp[0];
+  const long long mc1 = pl->dtype == SW_F32 ? pl->p2f.mcomp[1] : pl->p2d.mcomp[1];
+  if ((mc0 > 0 && !d->mem[0]) || (mc1 > 0 && !d->mem[1]))
+    return fail(SW_ERR_ARG, "sw2d_adjoint_run: adjoint memory variables missing");
+  const int nrec = pl->dtype == SW_F32 ? pl->p2f.nrec : pl->p2d.nrec;
+  if (nrec > 0 && !d->residual) return fail(SW_ERR_ARG, "sw2d_adjoint_run: residual missing");
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e = pl->dtype == SW_F32 ? adjoint2<float>(pl, pl->p2f, d, it0, nsteps, (const float*)snap, st)
+                                      : adjoint2<double>(pl, pl->p2d, d, it0, nsteps, (const double*)snap, st);
+  if (e != cudaSuccess) return cuda_fail(e, "sw2d_adjoint_run");
   return SW_OK;
 }
 

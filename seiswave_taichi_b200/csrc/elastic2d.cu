@@ -10,94 +10,12 @@
 // components x: sxx_dx sxz_dx dvx_dx dvz_dx, z: sxz_dz szz_dz dvz_dz dvx_dz --
 // the same named arrays serve all three schemes, as in the reference.
 #include "sw_device.cuh"
+#include "sw_stencil2d.cuh"
 
 namespace sw {
 
 constexpr int T2Z = 32;
 constexpr int T2X = 8;
-
-template <typename T>
-__device__ __forceinline__ void pml2(T* __restrict__ m, T b, T a, T kk, T& d) {
-  T psi = b * (*m) + a * d;
-  *m = psi;
-  d = div_v(d, kk) + psi;
-}
-
-// ---- 2D stencils of src/Differential2D.py, read through the read-only path --
-template <typename T, int N>
-__device__ __forceinline__ T dx_fm(const T* f, long long idx, int nz, const T* c) {
-  T v = 0;
-#pragma unroll
-  for (int m = 0; m < N; ++m) v += c[m] * (ldg(f + idx + (long long)(m + 1) * nz) - ldg(f + idx - (long long)m * nz));
-  return v;
-}
-template <typename T, int N>
-__device__ __forceinline__ T dz_fm(const T* f, long long idx, const T* c) {
-  T v = 0;
-#pragma unroll
-  for (int m = 0; m < N; ++m) v += c[m] * (ldg(f + idx + (m + 1)) - ldg(f + idx - m));
-  return v;
-}
-template <typename T, int N>
-__device__ __forceinline__ T dx_bm(const T* f, long long idx, int nz, const T* c) {
-  T v = 0;
-#pragma unroll
-  for (int m = 0; m < N; ++m) v += c[m] * (ldg(f + idx + (long long)m * nz) - ldg(f + idx - (long long)(m + 1) * nz));
-  return v;
-}
-template <typename T, int N>
-__device__ __forceinline__ T dz_bm(const T* f, long long idx, const T* c) {
-  T v = 0;
-#pragma unroll
-  for (int m = 0; m < N; ++m) v += c[m] * (ldg(f + idx + m) - ldg(f + idx - (m + 1)));
-  return v;
-}
-// rotated: Drx2fm f[i+m+1, j+m+1] - f[i-m, j-m]
-template <typename T, int N>
-__device__ __forceinline__ T drx_fm(const T* f, long long idx, int nz, const T* c) {
-  T v = 0;
-#pragma unroll
-  for (int m = 0; m < N; ++m)
-    v += c[m] * (ldg(f + idx + (long long)(m + 1) * nz + (m + 1)) - ldg(f + idx - (long long)m * nz - m));
-  return v;
-}
-// Drz2fm f[i-m, j+m+1] - f[i+m+1, j-m]
-template <typename T, int N>
-__device__ __forceinline__ T drz_fm(const T* f, long long idx, int nz, const T* c) {
-  T v = 0;
-#pragma unroll
-  for (int m = 0; m < N; ++m)
-    v += c[m] * (ldg(f + idx - (long long)m * nz + (m + 1)) - ldg(f + idx + (long long)(m + 1) * nz - m));
-  return v;
-}
-// Drx2bm f[i+m, j+m] - f[i-m-1, j-m-1]
-template <typename T, int N>
-__device__ __forceinline__ T drx_bm(const T* f, long long idx, int nz, const T* c) {
-  T v = 0;
-#pragma unroll
-  for (int m = 0; m < N; ++m)
-    v += c[m] * (ldg(f + idx + (long long)m * nz + m) - ldg(f + idx - (long long)(m + 1) * nz - (m + 1)));
-  return v;
-}
-// Drz2bm f[i-m-1, j+m] - f[i+m, j-m-1]
-template <typename T, int N>
-__device__ __forceinline__ T drz_bm(const T* f, long long idx, int nz, const T* c) {
-  T v = 0;
-#pragma unroll
-  for (int m = 0; m < N; ++m)
-    v += c[m] * (ldg(f + idx - (long long)(m + 1) * nz + m) - ldg(f + idx + (long long)m * nz - (m + 1)));
-  return v;
-}
-
-// memory-variable pointers
-template <typename T>
-__device__ __forceinline__ T* mx(const P2<T>& p, int comp, int xi, int j) {
-  return p.mem[0] + comp * p.mcomp[0] + (long long)xi * p.nz + j;
-}
-template <typename T>
-__device__ __forceinline__ T* mz(const P2<T>& p, int comp, int i, int zj) {
-  return p.mem[1] + comp * p.mcomp[1] + (long long)i * p.sn[1] + zj;
-}
 
 // ---------------------------------------------------------------------------
 template <typename T, int N, int SCHEME>
@@ -244,7 +162,7 @@ k2_velocity(const __grid_constant__ P2<T> p, int it, T amp, int src_here) {
 
 template <typename T, int N, int SCHEME>
 __global__ void __launch_bounds__(T2Z * T2X)
-k2_stress(const __grid_constant__ P2<T> p, int it) {
+k2_stress(const __grid_constant__ P2<T> p, int it, int inject_next) {
   // receivers of the velocity fields (final for this step, not written here)
   {
     const long long b = blockIdx.x + (long long)gridDim.x * blockIdx.y;
@@ -350,6 +268,25 @@ k2_stress(const __grid_constant__ P2<T> p, int it) {
       sxz[idx] = sxz[idx] + (u * (dvxdz + dvzdx)) * dt;
     }
   }
+  // moment-tensor source of step it+1, added after this cell's own update
+  // (nothing reads the stresses between here and the next velocity pass)
+  if (inject_next && i == p.si && j == p.sk) {
+    const T w = p.wav[it + 1];
+    sxx[idx] = sxx[idx] + w * p.mneg[0];
+    szz[idx] = szz[idx] + w * p.mneg[1];
+    sxz[idx] = sxz[idx] + w * p.mneg[2];
+  }
+}
+
+// moment-tensor source of step it before the velocity pass
+// (2D form of Elastic3D_SSG_Tensor.py:186-193)
+template <typename T>
+__global__ void k2_moment_inject(const __grid_constant__ P2<T> p, int it) {
+  const long long s = (long long)p.si * p.nz + p.sk;
+  const T w = p.wav[it];
+  p.f[2][s] = p.f[2][s] + w * p.mneg[0];
+  p.f[3][s] = p.f[3][s] + w * p.mneg[1];
+  p.f[4][s] = p.f[4][s] + w * p.mneg[2];
 }
 
 template <typename T>
@@ -359,41 +296,55 @@ __global__ void k2_gather(const __grid_constant__ P2<T> p, int it) {
 }
 
 template <typename T, int N, int S>
-static cudaError_t launch2(const P2<T>& p, int it, T amp, bool gather_in_stress, cudaStream_t st) {
+static cudaError_t launch2(const P2<T>& p, int it, T amp, bool gather_in_stress, bool pre_inject,
+                           bool inject_next, cudaStream_t st) {
   dim3 block(T2Z, T2X);
   dim3 grid((p.nz + T2Z - 1) / T2Z, (p.nx + T2X - 1) / T2X);
-  k2_velocity<T, N, S><<<grid, block, 0, st>>>(p, it, amp, p.src_kind != SW_SRC_NONE ? 1 : 0);
+  const bool moment = p.src_kind == SW_SRC_MOMENT;
+  if (moment && pre_inject) k2_moment_inject<T><<<1, 1, 0, st>>>(p, it);
+  k2_velocity<T, N, S><<<grid, block, 0, st>>>(p, it, amp, (p.src_kind != SW_SRC_NONE && !moment) ? 1 : 0);
   P2<T> q = p;
   if (!gather_in_stress) q.nrec = 0;
-  k2_stress<T, N, S><<<grid, block, 0, st>>>(q, it);
+  k2_stress<T, N, S><<<grid, block, 0, st>>>(q, it, (moment && inject_next) ? 1 : 0);
   if (!gather_in_stress && p.nrec > 0) k2_gather<T><<<(p.nrec + 255) / 256, 256, 0, st>>>(p, it);
   return cudaGetLastError();
 }
 
 template <typename T, int S>
-static cudaError_t dispatch2(const P2<T>& p, int order, int it, T amp, bool g, cudaStream_t st) {
+static cudaError_t dispatch2(const P2<T>& p, int order, int it, T amp, bool g, bool pre, bool nxt,
+                             cudaStream_t st) {
   switch (order) {
-    case 1: return launch2<T, 1, S>(p, it, amp, g, st);
-    case 2: return launch2<T, 2, S>(p, it, amp, g, st);
-    case 3: return launch2<T, 3, S>(p, it, amp, g, st);
-    case 4: return launch2<T, 4, S>(p, it, amp, g, st);
-    case 5: return launch2<T, 5, S>(p, it, amp, g, st);
-    case 6: return launch2<T, 6, S>(p, it, amp, g, st);
-    case 7: return launch2<T, 7, S>(p, it, amp, g, st);
-    case 8: return launch2<T, 8, S>(p, it, amp, g, st);
+    case 1: return launch2<T, 1, S>(p, it, amp, g, pre, nxt, st);
+    case 2: return launch2<T, 2, S>(p, it, amp, g, pre, nxt, st);
+    case 3: return launch2<T, 3, S>(p, it, amp, g, pre, nxt, st);
+    case 4: return launch2<T, 4, S>(p, it, amp, g, pre, nxt, st);
+    case 5: return launch2<T, 5, S>(p, it, amp, g, pre, nxt, st);
+    case 6: return launch2<T, 6, S>(p, it, amp, g, pre, nxt, st);
+    case 7: return launch2<T, 7, S>(p, it, amp, g, pre, nxt, st);
+    case 8: return launch2<T, 8, S>(p, it, amp, g, pre, nxt, st);
     default: return cudaErrorInvalidValue;
   }
 }
 
 template <typename T>
-cudaError_t sw2_step(const P2<T>& p, int scheme, int order, int it, T amp, bool gather_in_stress,
-                     cudaStream_t st) {
-  if (scheme == SW2D_SSG_VS) return dispatch2<T, SW2D_SSG_VS>(p, order, it, amp, gather_in_stress, st);
-  if (scheme == SW2D_SSG_SV) return dispatch2<T, SW2D_SSG_SV>(p, order, it, amp, gather_in_stress, st);
-  return dispatch2<T, SW2D_RSG>(p, order, it, amp, gather_in_stress, st);
+cudaError_t sw2_step(const P2<T>& p, int scheme, int order, int it, T amp, bool gather_in_stress, bool pre_inject,
+                     bool inject_next, cudaStream_t st) {
+  if (scheme == SW2D_SSG_VS)
+    return dispatch2<T, SW2D_SSG_VS>(p, order, it, amp, gather_in_stress, pre_inject, inject_next, st);
+  if (scheme == SW2D_SSG_SV)
+    return dispatch2<T, SW2D_SSG_SV>(p, order, it, amp, gather_in_stress, pre_inject, inject_next, st);
+  return dispatch2<T, SW2D_RSG>(p, order, it, amp, gather_in_stress, pre_inject, inject_next, st);
 }
 
-template cudaError_t sw2_step<float>(const P2<float>&, int, int, int, float, bool, cudaStream_t);
-template cudaError_t sw2_step<double>(const P2<double>&, int, int, int, double, bool, cudaStream_t);
+template <typename T>
+cudaError_t sw2_moment_inject(const P2<T>& p, int it, cudaStream_t st) {
+  k2_moment_inject<T><<<1, 1, 0, st>>>(p, it);
+  return cudaGetLastError();
+}
+template cudaError_t sw2_moment_inject<float>(const P2<float>&, int, cudaStream_t);
+template cudaError_t sw2_moment_inject<double>(const P2<double>&, int, cudaStream_t);
+
+template cudaError_t sw2_step<float>(const P2<float>&, int, int, int, float, bool, bool, bool, cudaStream_t);
+template cudaError_t sw2_step<double>(const P2<double>&, int, int, int, double, bool, bool, bool, cudaStream_t);
 
 }  // namespace sw

@@ -81,6 +81,7 @@ struct P2 {
   T rd[2];                  // RN(1/dx), RN(1/dz)
   T rd2[2];                 // RN(1/(2dx)), RN(1/(2dz)) (rotated-grid derivatives)
   int fast_div;             // bit0: dx, dz verified; bit1: 2dx, 2dz verified
+  T mneg[3];                // moment-tensor source: -M_xx, -M_zz, -M_xz
 };
 
 template <typename T>

@@ -135,7 +135,8 @@ def config3(shape=(400, 400, 200), nt=2000, accuracy=2, seed=0):
 
 def config1(n=400, nt=1000, accuracy=2):
     """2D homogeneous P-SV, n^2, dx=dz=10, vp=3000, vs=1732, rho=2000, dt=1 ms,
-    20-cell CPML, 25 Hz source at the centre, 200 receivers at z = N+5."""
+    20-cell CPML, explosive source (M = I) with the 25 Hz Ricker2 (t0 = 1.5/f)
+    at the centre, 200 receivers at z = N+5."""
     shape = (n, n)
     vp, vs, rho = homogeneous(shape)
     nr = 200
@@ -143,5 +144,5 @@ def config1(n=400, nt=1000, accuracy=2):
         name=f"2d-ssg-vs-{n}^2-nt{nt}", shape=shape, vp=vp, vs=vs, rho=rho, dx=10.0, dz=10.0, dt=1e-3,
         nt=nt, accuracy=accuracy, freq=25.0, isx=n // 2, isz=n // 2,
         rsx=np.linspace(accuracy + 1, n - accuracy - 2, nr).astype(np.int64).reshape(1, nr),
-        rsz=np.full((1, nr), accuracy + 5, np.int64),
+        rsz=np.full((1, nr), accuracy + 5, np.int64), MT="explosive", src_scale=1.0,
         pml=pml_parameter(3000.0, 1732.0, 10.0, 25.0, 20, dims=2), surface=[True] * 4)

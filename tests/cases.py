@@ -97,7 +97,7 @@ def oracle3d(c, wavelet=None):
 
 
 def case2d(shape=(80, 72), N=2, hetero=True, npml=10, nt=200, dtype=np.float32, dx=10.0, dz=10.0,
-           dt=1e-3, freq=25.0, seed=1, surface=(True,) * 4, nrec=None):
+           dt=1e-3, freq=25.0, seed=1, surface=(True,) * 4, nrec=None, MT=None, src_scale=1.0):
     nx, nz = shape
     if hetero:
         vp, vs, rho = layered_model(shape, seed, dtype=dtype)
@@ -112,12 +112,18 @@ def case2d(shape=(80, 72), N=2, hetero=True, npml=10, nt=200, dtype=np.float32, 
     if nrec:
         c["rsx"] = np.linspace(N + 2, nx - N - 3, nrec).astype(np.int64).reshape(1, nrec)
         c["rsz"] = np.full((1, nrec), N + 5, dtype=np.int64)
+    if MT is not None:
+        c["MT"] = MT
+        c["src_scale"] = src_scale
     return c
 
 
 def product2d(c, **kw):
     import torch
     from seiswave_taichi_b200.Elastic2D_CPML import ElasticWAVE
+    if "MT" in c:
+        kw.setdefault("MT", c["MT"])
+        kw.setdefault("src_scale", c["src_scale"])
     w = ElasticWAVE(c["vs"], c["vp"], c["rho"], c["dx"], c["dz"], c["dt"], c["isx"], c["isz"], c["rsx"],
                     c["rsz"], c["nt"], c["N"], c["freq"],
                     torch.float64 if c["dtype"] == np.float64 else torch.float32, **kw)
@@ -127,10 +133,16 @@ def product2d(c, **kw):
 
 def oracle2d(c, wavelet=None):
     from oracle.oracle import Oracle2D
-    rsx = int(np.asarray(c["rsx"]).reshape(-1)[0])
-    rsz = int(np.asarray(c["rsz"]).reshape(-1)[0])
-    return Oracle2D(c["vs"], c["vp"], c["rho"], c["dx"], c["dz"], c["dt"], c["isx"], c["isz"], rsx, rsz,
-                    c["nt"], c["N"], c["freq"], c["surface"], c["pml"], dtype=c["dtype"], wavelet=wavelet)
+    rx = np.asarray(c["rsx"]).reshape(-1)
+    rz = np.asarray(c["rsz"]).reshape(-1)
+    table = None if rx.size == 1 and np.ndim(c["rsx"]) == 0 else rx * c["shape"][1] + rz
+    mt = None
+    if "MT" in c:
+        from seiswave_taichi_b200.Elastic2D_CPML import moment_2d
+        mt = moment_2d(c["MT"])
+    return Oracle2D(c["vs"], c["vp"], c["rho"], c["dx"], c["dz"], c["dt"], c["isx"], c["isz"], int(rx[0]),
+                    int(rz[0]), c["nt"], c["N"], c["freq"], c["surface"], c["pml"], dtype=c["dtype"],
+                    wavelet=wavelet, MT=mt, rec_index=table)
 
 
 def to_np(t):

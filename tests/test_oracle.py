@@ -194,3 +194,25 @@ def test_oracle_cpml_absorbs():
         o.run("VS", k * 50, 50)
         energies.append(float(np.sum(o.vx.astype(np.float64) ** 2 + o.vz.astype(np.float64) ** 2)))
     assert energies[-1] < 1e-3 * max(energies)
+
+
+def test_oracle_2d_moment_source_and_receiver_table():
+    """The 2D moment-tensor source injects -w*M into the stresses at the start
+    of each step; the receiver table samples the scheme's component after the
+    stress phase (the last row equals the final field at those cells)."""
+    from cases import case2d, oracle2d
+    from seiswave_taichi_b200 import BaseFun
+    c = case2d(nt=60, hetero=False, MT=[[1.0, 0.0], [0.0, 1.0]], nrec=9, src_scale=1e5)
+    wav = BaseFun.series("ricker2", 60, c["dt"], c["freq"], 1e5, t0=np.float32(1.5) / np.float32(c["freq"]))
+    o = oracle2d(c, wavelet=wav).run("VS", 0, 60)
+    # linear in the source: twice the wavelet gives twice the traces
+    o2 = oracle2d(c, wavelet=(2 * wav).astype(np.float32)).run("VS", 0, 60)
+    np.testing.assert_allclose(o2.data, 2 * o.data, rtol=1e-6, atol=1e-30)
+    assert np.abs(o.data).max() > 0
+    idx = np.asarray(c["rsx"]).reshape(-1) * c["shape"][1] + np.asarray(c["rsz"]).reshape(-1)
+    assert o.data.shape == (60, 9)
+    np.testing.assert_array_equal(o.data[59], o.vz.reshape(-1)[idx])
+    # an explosive source in a homogeneous medium is mirror-symmetric in x
+    # about the source's sxx/szz position (x half point, i + 1/2): vx(i+1/2+d) = -vx(i+1/2-d)
+    i0 = c["isx"]
+    np.testing.assert_allclose(o.szz[i0 + 5, :], o.szz[i0 - 5, :], rtol=0, atol=1e-6 * np.abs(o.szz).max())
