@@ -215,6 +215,25 @@ SW_API int sw_step_amp(sw_plan* plan, int32_t it, double amplitude, void* stream
  * replayed from a cached CUDA graph when use_graph != 0. */
 SW_API int sw_run(sw_plan* plan, int32_t it0, int32_t nsteps, int32_t use_graph, void* stream);
 
+/* ---- batches of 2D shots (no reference counterpart) -------------------------
+ * Many shots of uneven grid sizes (one sw2d_desc each, sharing scheme VS or
+ * SV, dtype, order and nt_max; velocity receivers) stepped together: per time
+ * step one launch of the velocity phase and one of the stress phase cover
+ * every tile of every shot, and sw_batch_run replays the whole step sequence
+ * from one cached CUDA graph.  It replaces a Python loop over the reference's
+ * ElasticWAVE objects, each running `for i in range(nt): update_SSG_VS(i)`
+ * (Elastic2D_CPML.py:128-200).  Each shot's result equals its own sw_run. */
+typedef struct sw_batch sw_batch;
+#define SW_BATCH_TILES 4 /* tile shapes the autotuner picks from (sw_batch_info) */
+SW_API int sw2d_batch_create(const sw2d_desc* shots, int32_t nshots, sw_batch** batch);
+/* Tile shape index 0..SW_BATCH_TILES-1: (x rows, z columns) 8x32, 4x32, 16x32, 4x64. */
+SW_API int sw_batch_set_tile(sw_batch* batch, int32_t tile);
+/* info[0] tile index, [1] SW_BATCH_TILES, [2] tiles per launch, [3] rows, [4] columns,
+ * [5] shots.  info must hold 6 int32. */
+SW_API int sw_batch_info(sw_batch* batch, int32_t* info);
+SW_API int sw_batch_run(sw_batch* batch, int32_t it0, int32_t nsteps, int32_t use_graph, void* stream);
+SW_API int sw_batch_destroy(sw_batch* batch);
+
 /* ---- 2D adjoint (no reference counterpart) --------------------------------
  * Hand-written discrete adjoint of the SW2D_SSG_VS time loop with a
  * SW_SRC_MOMENT (or no) source and vz receivers, for gradients of a seismogram

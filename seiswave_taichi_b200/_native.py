@@ -31,7 +31,8 @@ EXPORTS = (
     "sw_plan_set_tile", "sw_abi_sizeof", "sw_plan_destroy", "sw_step", "sw_step_amp",
     "sw_run", "sw_check_finite", "sw_plan_status", "sw_plan_info", "sw_plan_set_path",
     "sw_plan_set_exact", "sw_count_nonfinite_noalloc", "sw2d_snapshot_elems", "sw2d_record",
-    "sw2d_adjoint_run",
+    "sw2d_adjoint_run", "sw2d_batch_create", "sw_batch_set_tile", "sw_batch_info", "sw_batch_run",
+    "sw_batch_destroy",
 )
 
 
@@ -127,6 +128,11 @@ def load() -> C.CDLL:
         "sw2d_snapshot_elems": (C.c_int, [vp, C.POINTER(C.c_int64)]),
         "sw2d_record": (C.c_int, [vp, C.c_int32, C.c_int32, vp, vp]),
         "sw2d_adjoint_run": (C.c_int, [vp, C.POINTER(Adjoint2D), C.c_int32, C.c_int32, vp, vp]),
+        "sw2d_batch_create": (C.c_int, [C.POINTER(Desc2D), C.c_int32, C.POINTER(vp)]),
+        "sw_batch_set_tile": (C.c_int, [vp, C.c_int32]),
+        "sw_batch_info": (C.c_int, [vp, C.POINTER(C.c_int32)]),
+        "sw_batch_run": (C.c_int, [vp, C.c_int32, C.c_int32, C.c_int32, vp]),
+        "sw_batch_destroy": (C.c_int, [vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -28,6 +28,9 @@ template <typename T> cudaError_t sw3_spml_step(const P3<T>&, int, int, bool, cu
 template <typename T> cudaError_t sw2_step(const P2<T>&, int, int, int, T, bool, bool, bool, cudaStream_t);
 template <typename T> cudaError_t sw2_moment_inject(const P2<T>&, int, cudaStream_t);
 template <typename T>
+cudaError_t sw2b_step(const Batch2<T>&, int, int, int, int, int, bool, bool, cudaStream_t);
+void sw2b_tile_shape(int cfg, int* bx, int* bz);
+template <typename T>
 struct A2 {
   T* f[5];
   T* mem[2];
@@ -901,6 +904,190 @@ int sw2d_adjoint_run(sw_plan* pl, const sw2d_adjoint_desc* d, int32_t it0, int32
   cudaError_t e = pl->dtype == SW_F32 ? adjoint2<float>(pl, pl->p2f, d, it0, nsteps, (const float*)snap, st)
                                       : adjoint2<double>(pl, pl->p2d, d, it0, nsteps, (const double*)snap, st);
   if (e != cudaSuccess) return cuda_fail(e, "sw2d_adjoint_run");
+  return SW_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// batches of 2D shots of uneven sizes
+// ---------------------------------------------------------------------------
+struct sw_batch {
+  int nshots = 0, scheme = 0, dtype = 0, order = 0, nt_max = 0;
+  bool fold = true;                       // next-step moment source folded into the stress pass
+  std::vector<sw_plan*> plans;            // per-shot validated plans
+  void* d_shots = nullptr;                // device P2<T>[nshots]
+  int2* d_work = nullptr;                 // device, per tile shape: one work item per block
+  long long work_off[SW_BATCH_TILES] = {};
+  int total[SW_BATCH_TILES] = {};
+  int cfg = 0;
+  long long cells = 0;
+  cudaStream_t cap_stream = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  int g_it0 = -1, g_n = -1, g_cfg = -1;
+};
+
+namespace {
+
+template <typename T>
+sw::Batch2<T> batch_view(const sw_batch* b) {
+  return sw::Batch2<T>{(const sw::P2<T>*)b->d_shots, b->d_work + b->work_off[b->cfg], b->nshots};
+}
+
+cudaError_t batch_sequence(sw_batch* b, int it0, int n, cudaStream_t st) {
+  for (int s = 0; s < n; ++s) {
+    const int it = it0 + s;
+    const bool pre = s == 0 || !b->fold, nxt = b->fold && s != n - 1;
+    cudaError_t e = b->dtype == SW_F32
+                        ? sw::sw2b_step<float>(batch_view<float>(b), b->scheme, b->order, b->cfg, b->total[b->cfg],
+                                               it, pre, nxt, st)
+                        : sw::sw2b_step<double>(batch_view<double>(b), b->scheme, b->order, b->cfg,
+                                                b->total[b->cfg], it, pre, nxt, st);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+void batch_free(sw_batch* b) {
+  if (!b) return;
+  if (b->gexec) cudaGraphExecDestroy(b->gexec);
+  if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
+  if (b->d_shots) cudaFree(b->d_shots);
+  if (b->d_work) cudaFree(b->d_work);
+  for (sw_plan* p : b->plans) sw_plan_destroy(p);
+  delete b;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sw2d_batch_create(const sw2d_desc* shots, int32_t nshots, sw_batch** out) {
+  g_err.clear();
+  if (!shots || !out || nshots <= 0) return fail(SW_ERR_ARG, "sw2d_batch_create: empty batch or null output");
+  *out = nullptr;
+  const sw2d_desc& d0 = shots[0];
+  if (d0.scheme != SW2D_SSG_VS && d0.scheme != SW2D_SSG_SV)
+    return fail(SW_ERR_UNSUPPORTED, "sw2d_batch_create: batches run the SSG_VS or SSG_SV scheme");
+  sw_batch* b = new sw_batch();
+  b->nshots = nshots; b->scheme = d0.scheme; b->dtype = d0.dtype; b->order = d0.order; b->nt_max = d0.nt_max;
+  for (int s = 0; s < nshots; ++s) {
+    const sw2d_desc& d = shots[s];
+    if (d.scheme != d0.scheme || d.dtype != d0.dtype || d.order != d0.order || d.nt_max != d0.nt_max) {
+      batch_free(b);
+      return fail(SW_ERR_ARG, "sw2d_batch_create: shot " + std::to_string(s) +
+                                  " differs from shot 0 in scheme, dtype, order or nt_max");
+    }
+    sw_plan* pl = nullptr;
+    int rc = sw2d_plan_create(&d, &pl);
+    if (rc != SW_OK) {
+      std::string m = g_err;
+      batch_free(b);
+      return fail(rc, "sw2d_batch_create: shot " + std::to_string(s) + ": " + m);
+    }
+    b->plans.push_back(pl);
+    if (!pl->gather_in_stress || (long long)d.rec.nrec > (long long)d.nx * d.nz) {
+      batch_free(b);
+      return fail(SW_ERR_UNSUPPORTED, "sw2d_batch_create: shot " + std::to_string(s) +
+                                          ": batch receivers record a velocity field, at most one per cell");
+    }
+    b->cells += (long long)d.nx * d.nz;
+  }
+  const size_t psz = b->dtype == SW_F32 ? sizeof(sw::P2<float>) : sizeof(sw::P2<double>);
+  std::vector<char> host(psz * nshots);
+  for (int s = 0; s < nshots; ++s) {
+    if (b->dtype == SW_F32) memcpy(host.data() + psz * s, &b->plans[s]->p2f, psz);
+    else memcpy(host.data() + psz * s, &b->plans[s]->p2d, psz);
+  }
+  // work items, shot by shot, tile rows (x) outer, tile columns (z) inner
+  std::vector<int2> work;
+  for (int c = 0; c < SW_BATCH_TILES; ++c) {
+    int bx, bz;
+    sw::sw2b_tile_shape(c, &bx, &bz);
+    b->work_off[c] = (long long)work.size();
+    for (int s = 0; s < nshots; ++s) {
+      const int tx = (shots[s].nx + bx - 1) / bx, tz = (shots[s].nz + bz - 1) / bz;
+      if (tx > 0xffff || tz > 0xffff) {
+        batch_free(b);
+        return fail(SW_ERR_ARG, "sw2d_batch_create: shot " + std::to_string(s) + " has too many tiles");
+      }
+      for (int x = 0; x < tx; ++x)
+        for (int z = 0; z < tz; ++z) work.push_back(make_int2(s, (x << 16) | z));
+    }
+    const long long tot = (long long)work.size() - b->work_off[c];
+    if (tot > 0x7fffffffLL) {
+      batch_free(b);
+      return fail(SW_ERR_ARG, "sw2d_batch_create: batch too large for one launch");
+    }
+    b->total[c] = (int)tot;
+  }
+  cudaError_t e = cudaMalloc(&b->d_shots, psz * nshots);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_work, work.size() * sizeof(int2));
+  if (e == cudaSuccess) e = cudaMemcpy(b->d_shots, host.data(), psz * nshots, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(b->d_work, work.data(), work.size() * sizeof(int2), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    batch_free(b);
+    return cuda_fail(e, "sw2d_batch_create");
+  }
+  *out = b;
+  return SW_OK;
+}
+
+int sw_batch_set_tile(sw_batch* b, int32_t cfg) {
+  if (!b) return fail(SW_ERR_ARG, "null batch");
+  if (cfg < 0 || cfg >= SW_BATCH_TILES) return fail(SW_ERR_ARG, "sw_batch_set_tile: tile shape index out of range");
+  b->cfg = cfg;
+  return SW_OK;
+}
+
+int sw_batch_info(sw_batch* b, int32_t* info) {
+  if (!b || !info) return fail(SW_ERR_ARG, "null batch or output");
+  int bx, bz;
+  sw::sw2b_tile_shape(b->cfg, &bx, &bz);
+  info[0] = b->cfg;
+  info[1] = SW_BATCH_TILES;
+  info[2] = b->total[b->cfg];
+  info[3] = bx;
+  info[4] = bz;
+  info[5] = b->nshots;
+  return SW_OK;
+}
+
+int sw_batch_run(sw_batch* b, int32_t it0, int32_t nsteps, int32_t use_graph, void* stream) {
+  if (!b) return fail(SW_ERR_ARG, "null batch");
+  if (it0 < 0 || nsteps < 0 || (long long)it0 + nsteps > b->nt_max)
+    return fail(SW_ERR_ARG, "sw_batch_run: steps outside 0..nt_max-1");
+  if (nsteps == 0) return SW_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e;
+  if (!use_graph) {
+    e = batch_sequence(b, it0, nsteps, st);
+    return e == cudaSuccess ? SW_OK : cuda_fail(e, "sw_batch_run");
+  }
+  if (!(b->gexec && b->g_it0 == it0 && b->g_n == nsteps && b->g_cfg == b->cfg)) {
+    if (b->gexec) { cudaGraphExecDestroy(b->gexec); b->gexec = nullptr; }
+    if (!b->cap_stream) {
+      e = cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking);
+      if (e != cudaSuccess) return cuda_fail(e, "sw_batch_run: capture stream");
+    }
+    e = cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return cuda_fail(e, "sw_batch_run: begin capture");
+    cudaError_t le = batch_sequence(b, it0, nsteps, b->cap_stream);
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(b->cap_stream, &g);
+    if (le != cudaSuccess) { if (g) cudaGraphDestroy(g); return cuda_fail(le, "sw_batch_run: capture"); }
+    if (e != cudaSuccess) return cuda_fail(e, "sw_batch_run: end capture");
+    e = cudaGraphInstantiate(&b->gexec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) { b->gexec = nullptr; return cuda_fail(e, "sw_batch_run: instantiate"); }
+    b->g_it0 = it0; b->g_n = nsteps; b->g_cfg = b->cfg;
+  }
+  e = cudaGraphLaunch(b->gexec, st);
+  return e == cudaSuccess ? SW_OK : cuda_fail(e, "sw_batch_run: graph launch");
+}
+
+int sw_batch_destroy(sw_batch* b) {
+  batch_free(b);
   return SW_OK;
 }
 

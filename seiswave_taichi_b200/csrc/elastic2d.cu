@@ -18,13 +18,10 @@ constexpr int T2Z = 32;
 constexpr int T2X = 8;
 
 // ---------------------------------------------------------------------------
+// velocity update of cell (i, j), 0 <= i < nx, 0 <= j < nz
 template <typename T, int N, int SCHEME>
-__global__ void __launch_bounds__(T2Z * T2X)
-k2_velocity(const __grid_constant__ P2<T> p, int it, T amp, int src_here) {
-  const int j = blockIdx.x * T2Z + threadIdx.x;
-  const int i = blockIdx.y * T2X + threadIdx.y;
+__device__ __forceinline__ void vel2_cell(const P2<T>& p, int i, int j, int it, T amp, int src_here) {
   const int nx = p.nx, nz = p.nz;
-  if (i >= nx || j >= nz) return;
   const long long idx = (long long)i * nz + j;
   const T dx = p.dx, dz = p.dz, dt = p.dt;
   T c[N];
@@ -160,19 +157,10 @@ k2_velocity(const __grid_constant__ P2<T> p, int it, T amp, int src_here) {
   }
 }
 
+// stress update of cell (i, j), then the next step's moment-tensor source
 template <typename T, int N, int SCHEME>
-__global__ void __launch_bounds__(T2Z * T2X)
-k2_stress(const __grid_constant__ P2<T> p, int it, int inject_next) {
-  // receivers of the velocity fields (final for this step, not written here)
-  {
-    const long long b = blockIdx.x + (long long)gridDim.x * blockIdx.y;
-    const long long r = b * (T2Z * T2X) + threadIdx.y * T2Z + threadIdx.x;
-    if (r < p.nrec) store_rec(p.rec_data, p.rec_f64, (long long)it * p.nrec + r, p.f[p.rec_field][p.rec_idx[r]]);
-  }
-  const int j = blockIdx.x * T2Z + threadIdx.x;
-  const int i = blockIdx.y * T2X + threadIdx.y;
+__device__ __forceinline__ void str2_cell(const P2<T>& p, int i, int j, int it, int inject_next) {
   const int nx = p.nx, nz = p.nz;
-  if (i >= nx || j >= nz) return;
   const long long idx = (long long)i * nz + j;
   const T dx = p.dx, dz = p.dz, dt = p.dt;
   T c[N];
@@ -278,6 +266,30 @@ k2_stress(const __grid_constant__ P2<T> p, int it, int inject_next) {
   }
 }
 
+template <typename T, int N, int SCHEME>
+__global__ void __launch_bounds__(T2Z * T2X)
+k2_velocity(const __grid_constant__ P2<T> p, int it, T amp, int src_here) {
+  const int j = blockIdx.x * T2Z + threadIdx.x;
+  const int i = blockIdx.y * T2X + threadIdx.y;
+  if (i >= p.nx || j >= p.nz) return;
+  vel2_cell<T, N, SCHEME>(p, i, j, it, amp, src_here);
+}
+
+template <typename T, int N, int SCHEME>
+__global__ void __launch_bounds__(T2Z * T2X)
+k2_stress(const __grid_constant__ P2<T> p, int it, int inject_next) {
+  // receivers of the velocity fields (final for this step, not written here)
+  {
+    const long long b = blockIdx.x + (long long)gridDim.x * blockIdx.y;
+    const long long r = b * (T2Z * T2X) + threadIdx.y * T2Z + threadIdx.x;
+    if (r < p.nrec) store_rec(p.rec_data, p.rec_f64, (long long)it * p.nrec + r, p.f[p.rec_field][p.rec_idx[r]]);
+  }
+  const int j = blockIdx.x * T2Z + threadIdx.x;
+  const int i = blockIdx.y * T2X + threadIdx.y;
+  if (i >= p.nx || j >= p.nz) return;
+  str2_cell<T, N, SCHEME>(p, i, j, it, inject_next);
+}
+
 // moment-tensor source of step it before the velocity pass
 // (2D form of Elastic3D_SSG_Tensor.py:186-193)
 template <typename T>
@@ -343,6 +355,115 @@ cudaError_t sw2_moment_inject(const P2<T>& p, int it, cudaStream_t st) {
 }
 template cudaError_t sw2_moment_inject<float>(const P2<float>&, int, cudaStream_t);
 template cudaError_t sw2_moment_inject<double>(const P2<double>&, int, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// batched ragged shots: one launch per phase covers every tile of every shot
+// ---------------------------------------------------------------------------
+// the block's shot parameter block, copied once into shared memory so that
+// every thread reads it from there instead of global memory
+template <typename T, int NT>
+__device__ __forceinline__ const P2<T>& stage_shot(const Batch2<T>& bt, int s, P2<T>* sp) {
+  static_assert(sizeof(P2<T>) % 4 == 0, "parameter block size");
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  const uint32_t* src = reinterpret_cast<const uint32_t*>(bt.shots + s);
+  uint32_t* dst = reinterpret_cast<uint32_t*>(sp);
+  for (int q = tid; q < (int)(sizeof(P2<T>) / 4); q += NT) dst[q] = src[q];
+  __syncthreads();
+  return *sp;
+}
+
+template <typename T, int N, int S, int BX, int BZ>
+__global__ void __launch_bounds__(BX * BZ) k2b_velocity(Batch2<T> bt, int it) {
+  __shared__ P2<T> sp;
+  const int2 wk = bt.work[blockIdx.x];
+  const P2<T>& p = stage_shot<T, BX * BZ>(bt, wk.x, &sp);
+  const int j = (wk.y & 0xffff) * BZ + threadIdx.x, i = (wk.y >> 16) * BX + threadIdx.y;
+  if (i >= p.nx || j >= p.nz) return;
+  vel2_cell<T, N, S>(p, i, j, it, (T)0, p.src_kind == SW_SRC_FORCE ? 1 : 0);
+}
+
+template <typename T, int N, int S, int BX, int BZ>
+__global__ void __launch_bounds__(BX * BZ) k2b_stress(Batch2<T> bt, int it, int inject_next) {
+  __shared__ P2<T> sp;
+  const int2 wk = bt.work[blockIdx.x];
+  const P2<T>& p = stage_shot<T, BX * BZ>(bt, wk.x, &sp);
+  const int tx = wk.y >> 16, tz = wk.y & 0xffff;
+  {
+    // receivers of the velocity fields: the shot's first tiles cover them
+    const long long t = (long long)tx * ((p.nz + BZ - 1) / BZ) + tz;
+    const long long r = t * (BX * BZ) + threadIdx.y * BZ + threadIdx.x;
+    if (r < p.nrec) store_rec(p.rec_data, p.rec_f64, (long long)it * p.nrec + r, p.f[p.rec_field][p.rec_idx[r]]);
+  }
+  const int j = tz * BZ + threadIdx.x, i = tx * BX + threadIdx.y;
+  if (i >= p.nx || j >= p.nz) return;
+  str2_cell<T, N, S>(p, i, j, it, (inject_next && p.src_kind == SW_SRC_MOMENT) ? 1 : 0);
+}
+
+template <typename T>
+__global__ void k2b_inject(Batch2<T> bt, int it) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= bt.nshots) return;
+  const P2<T>& p = bt.shots[s];
+  if (p.src_kind != SW_SRC_MOMENT) return;
+  const long long c = (long long)p.si * p.nz + p.sk;
+  const T w = p.wav[it];
+  p.f[2][c] = p.f[2][c] + w * p.mneg[0];
+  p.f[3][c] = p.f[3][c] + w * p.mneg[1];
+  p.f[4][c] = p.f[4][c] + w * p.mneg[2];
+}
+
+// tile shapes (x rows, z columns) the autotuner chooses from
+constexpr int kBatchTiles[SW_BATCH_TILES][2] = {{8, 32}, {4, 32}, {16, 32}, {4, 64}};
+
+template <typename T, int N, int S, int BX, int BZ>
+static cudaError_t launch2b(const Batch2<T>& bt, int total, int it, bool pre, bool nxt, cudaStream_t st) {
+  if (pre) k2b_inject<T><<<(bt.nshots + 127) / 128, 128, 0, st>>>(bt, it);
+  dim3 block(BZ, BX);
+  k2b_velocity<T, N, S, BX, BZ><<<total, block, 0, st>>>(bt, it);
+  k2b_stress<T, N, S, BX, BZ><<<total, block, 0, st>>>(bt, it, nxt ? 1 : 0);
+  return cudaGetLastError();
+}
+
+template <typename T, int N, int S>
+static cudaError_t tile2b(const Batch2<T>& bt, int cfg, int total, int it, bool pre, bool nxt, cudaStream_t st) {
+  switch (cfg) {
+    case 0: return launch2b<T, N, S, 8, 32>(bt, total, it, pre, nxt, st);
+    case 1: return launch2b<T, N, S, 4, 32>(bt, total, it, pre, nxt, st);
+    case 2: return launch2b<T, N, S, 16, 32>(bt, total, it, pre, nxt, st);
+    case 3: return launch2b<T, N, S, 4, 64>(bt, total, it, pre, nxt, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <typename T, int S>
+static cudaError_t order2b(const Batch2<T>& bt, int order, int cfg, int total, int it, bool pre, bool nxt,
+                           cudaStream_t st) {
+  switch (order) {
+    case 1: return tile2b<T, 1, S>(bt, cfg, total, it, pre, nxt, st);
+    case 2: return tile2b<T, 2, S>(bt, cfg, total, it, pre, nxt, st);
+    case 3: return tile2b<T, 3, S>(bt, cfg, total, it, pre, nxt, st);
+    case 4: return tile2b<T, 4, S>(bt, cfg, total, it, pre, nxt, st);
+    case 5: return tile2b<T, 5, S>(bt, cfg, total, it, pre, nxt, st);
+    case 6: return tile2b<T, 6, S>(bt, cfg, total, it, pre, nxt, st);
+    case 7: return tile2b<T, 7, S>(bt, cfg, total, it, pre, nxt, st);
+    case 8: return tile2b<T, 8, S>(bt, cfg, total, it, pre, nxt, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+void sw2b_tile_shape(int cfg, int* bx, int* bz) {
+  *bx = kBatchTiles[cfg][0];
+  *bz = kBatchTiles[cfg][1];
+}
+
+template <typename T>
+cudaError_t sw2b_step(const Batch2<T>& bt, int scheme, int order, int cfg, int total, int it, bool pre, bool nxt,
+                      cudaStream_t st) {
+  if (scheme == SW2D_SSG_VS) return order2b<T, SW2D_SSG_VS>(bt, order, cfg, total, it, pre, nxt, st);
+  return order2b<T, SW2D_SSG_SV>(bt, order, cfg, total, it, pre, nxt, st);
+}
+template cudaError_t sw2b_step<float>(const Batch2<float>&, int, int, int, int, int, bool, bool, cudaStream_t);
+template cudaError_t sw2b_step<double>(const Batch2<double>&, int, int, int, int, int, bool, bool, cudaStream_t);
 
 template cudaError_t sw2_step<float>(const P2<float>&, int, int, int, float, bool, bool, bool, cudaStream_t);
 template cudaError_t sw2_step<double>(const P2<double>&, int, int, int, double, bool, bool, bool, cudaStream_t);

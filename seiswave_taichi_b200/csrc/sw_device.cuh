@@ -84,6 +84,17 @@ struct P2 {
   T mneg[3];                // moment-tensor source: -M_xx, -M_zz, -M_xz
 };
 
+// a batch of 2D shots: per-shot parameter blocks in device memory and, for
+// the current tile shape, one work item per block: x = shot, y = tile row
+// (x direction) << 16 | tile column (z direction)
+#define SW_BATCH_TILES 4
+template <typename T>
+struct Batch2 {
+  const P2<T>* shots;
+  const int2* work;
+  int nshots;
+};
+
 template <typename T>
 __device__ __forceinline__ T ldg(const T* p) { return __ldg(p); }
 

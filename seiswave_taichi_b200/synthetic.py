@@ -146,3 +146,25 @@ def config1(n=400, nt=1000, accuracy=2):
         rsx=np.linspace(accuracy + 1, n - accuracy - 2, nr).astype(np.int64).reshape(1, nr),
         rsz=np.full((1, nr), accuracy + 5, np.int64), MT="explosive", src_scale=1.0,
         pml=pml_parameter(3000.0, 1732.0, 10.0, 25.0, 20, dims=2), surface=[True] * 4)
+
+
+def config4(nshots=64, nt=1500, accuracy=2, seed=0, nx_range=(600, 1200), nz_range=(300, 500)):
+    """Batched 2D workload: nshots seeded heterogeneous models of uneven sizes
+    (nx ~ U[600, 1200], nz ~ U[300, 500], dx = dz = 10 m), layered vp
+    1500-4500 m/s with a +10% Gaussian anomaly, explosive 15 Hz Ricker2 source
+    below the surface at the model centre, receivers every 4 cells at
+    z = N + 5, dt = 1 ms, 20-cell CPML.  Returns a list of per-shot dicts."""
+    rng = np.random.default_rng(seed)
+    shots = []
+    for s in range(nshots):
+        nx = int(rng.integers(nx_range[0], nx_range[1] + 1))
+        nz = int(rng.integers(nz_range[0], nz_range[1] + 1))
+        vp, vs, rho = layered((nx, nz), 1500.0, 4500.0, nlayers=8, seed=seed + 100 + s, anomaly=0.10)
+        rx = np.arange(accuracy + 21, nx - accuracy - 21, 4, dtype=np.int64)
+        shots.append(dict(
+            name=f"2d-batch-{nshots}shots-nt{nt}", shape=(nx, nz), vp=vp, vs=vs, rho=rho, dx=10.0, dz=10.0,
+            dt=1e-3, nt=nt, accuracy=accuracy, freq=15.0, isx=nx // 2, isz=accuracy + 25,
+            rsx=rx.reshape(1, -1), rsz=np.full((1, rx.size), accuracy + 5, np.int64), MT="explosive",
+            src_scale=1.0, pml=pml_parameter(float(vp.max()), float(vs.max()), 10.0, 15.0, 20, dims=2),
+            surface=[True] * 4))
+    return shots
