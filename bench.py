@@ -110,22 +110,42 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def build_solver(cfg, torch, exact=True):
+def build_solver(cfg, torch, exact=True, dtype=None, coef64=False):
     from seiswave_taichi_b200.Elastic3D_SSG_Tensor import ElasticWAVE
     w = ElasticWAVE(cfg["vs"], cfg["vp"], cfg["rho"], cfg["dx"], cfg["dy"], cfg["dz"], cfg["dt"],
                     cfg["isx"], cfg["isy"], cfg["isz"], cfg["rsx"], cfg["rsy"], cfg["rsz"], cfg["MT"],
-                    cfg["src_scale"], cfg["nt"], cfg["accuracy"], cfg["freq"], torch.float32, exact=exact)
+                    cfg["src_scale"], cfg["nt"], cfg["accuracy"], cfg["freq"], dtype or torch.float32, exact=exact,
+                    coef64=coef64)
     w.SetADEPML3D(cfg["surface"], cfg["pml"])
     return w
 
 
-def build_solver2d(cfg, torch):
+def build_solver2d(cfg, torch, dtype=None, coef64=False):
     from seiswave_taichi_b200.Elastic2D_CPML import ElasticWAVE
     w = ElasticWAVE(cfg["vs"], cfg["vp"], cfg["rho"], cfg["dx"], cfg["dz"], cfg["dt"], cfg["isx"],
                     cfg["isz"], cfg["rsx"], cfg["rsz"], cfg["nt"], cfg["accuracy"], cfg["freq"],
-                    torch.float32, MT=cfg.get("MT"), src_scale=cfg.get("src_scale", 1.0))
+                    dtype or torch.float32, MT=cfg.get("MT"), src_scale=cfg.get("src_scale", 1.0), coef64=coef64)
     w.SetADEPML2D(cfg["surface"], cfg["pml"])
     return w
+
+
+def fp64_error(cfg, w32, torch):
+    """Relative L2 error of the f32 run's traces and final vx against float64
+    runs of the same scheme: with the f32-rounded stencil coefficients (the
+    reference's own f64 mode) and with float64 coefficients."""
+    three_d = len(cfg["shape"]) == 3
+    out = {}
+    for tag, c64 in (("f64_run_f32_coef", False), ("f64_run_f64_coef", True)):
+        w = (build_solver(cfg, torch, dtype=torch.float64, coef64=c64) if three_d
+             else build_solver2d(cfg, torch, dtype=torch.float64, coef64=c64))
+        w.run(cfg["nt"])
+        torch.cuda.synchronize()
+        d64, d32 = w.data.double(), w32.data.double()
+        v64, v32 = w.vx.double(), w32.vx.double()
+        out[tag] = {"traces_rel_l2": float(torch.linalg.norm(d32 - d64) / torch.linalg.norm(d64)),
+                    "final_vx_rel_l2": float(torch.linalg.norm(v32 - v64) / torch.linalg.norm(v64))}
+        del w
+    return out
 
 
 def algorithmic_bytes(cfg, npml=20):
@@ -226,6 +246,7 @@ def main(argv=None):
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="config2", choices=["config2", "config1", "config3"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the float64 error runs")
     args = ap.parse_args(argv)
     args.warmup = max(args.warmup, 3)
 
@@ -340,14 +361,17 @@ def main(argv=None):
                 "parity": "traces within 1e-5 rel. L2 of the oracle over 400 steps; fields within 1e-4"}
         del wf
 
+    # error of the f32 result (the last timed run) against float64 runs
+    err64 = fp64_error(cfg, w, torch) if rank == 0 and not args.no_fp64 else None
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(cfg)
 
-    # per run: velocity + stress kernel per time step, plus the 3D pre-step
+    # per run: velocity + stress kernel per time step, plus the first step's
     # moment-tensor injection (receivers and next-step sources ride inside the
     # stress kernel); w.reset() zeroes the state with torch fills
-    launches_per_run = 2 * nt + (1 if three_d else 0)
+    launches_per_run = 2 * nt + 1
     info = w._plan.info() if three_d else {"path": "two_pass"}
     kname = {"staged": "k3s_velocity + k3s_stress", "two_pass": "k3_velocity + k3_stress",
              "fused": "k3_fused"}.get(info["path"], info["path"]) if three_d else "k2_velocity + k2_stress"
@@ -373,6 +397,7 @@ def main(argv=None):
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
             "fast_mode": fast,
+            "fp64_error": err64,
         }
         print(json.dumps(line), flush=True)
     if dist:

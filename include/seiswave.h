@@ -234,6 +234,53 @@ SW_API int sw_batch_info(sw_batch* batch, int32_t* info);
 SW_API int sw_batch_run(sw_batch* batch, int32_t it0, int32_t nsteps, int32_t use_graph, void* stream);
 SW_API int sw_batch_destroy(sw_batch* batch);
 
+/* ---- learned thin absorbing layer, 2D (no reference counterpart) ------------
+ * A network corrects the five fields of the outer SW_ABC_DEPTH cells of a 2D
+ * VS solver after each time step; it runs on top of a thin CPML built by the
+ * reference's SetADEPML2D (Elastic2D_CPML.py:392-528), which stays the
+ * fallback.  One network per face (0 x-low, 1 x-high, 2 z-low, 3 z-high):
+ * inputs are the fields / scale on the 3x3 stencil around the cell in the
+ * face's frame plus a one-hot of the cell's depth; two tanh layers of
+ * SW_ABC_HIDDEN; five outputs times oscale are added to the fields.  Parameter
+ * block per face: W1[H][I] b1[H] W2[H][H] b2[H] W3[5][H] b3[5] (float32). */
+#define SW_ABC_DEPTH 6
+#define SW_ABC_INPUTS (45 + SW_ABC_DEPTH)
+#define SW_ABC_HIDDEN 32
+#define SW_ABC_PARAMS (SW_ABC_HIDDEN * SW_ABC_INPUTS + SW_ABC_HIDDEN + SW_ABC_HIDDEN * SW_ABC_HIDDEN + \
+                       SW_ABC_HIDDEN + 5 * SW_ABC_HIDDEN + 5)
+typedef struct sw_abc_desc {
+  int32_t ncell;             /* layer cells                                     */
+  const int32_t* cell;       /* device, linear index of each layer cell         */
+  const int8_t* face;        /* device, its face 0..3                           */
+  const int8_t* depth;       /* device, its distance to the face 0..DEPTH-1     */
+  const float* params;       /* device, 4 x SW_ABC_PARAMS                       */
+  float scale[5];            /* input scales of the fields vx vz sxx szz sxz    */
+  float oscale[5];           /* output scales: field_q += y_q * oscale_q        */
+  float* delta;              /* device scratch, ncell x 5                       */
+} sw_abc_desc;
+/* Add the network's corrections to the plan's fields (float32 2D plans). */
+SW_API int sw2d_abc_correct(sw_plan* plan, const sw_abc_desc* abc, void* stream);
+/* Network inputs of every layer cell from the plan's fields: x is ncell x SW_ABC_INPUTS. */
+SW_API int sw2d_abc_features(sw_plan* plan, const sw_abc_desc* abc, float* x, void* stream);
+/* Training: loss += mean over n samples of |net(x) - y|^2 (sum over the 5
+ * outputs) and grad += its gradient with respect to one face's parameters. */
+SW_API int sw_mlp_grad(const float* params, const float* x, const float* y, int64_t n, float* grad, float* loss,
+                       void* stream);
+/* y = net(x) for n samples of one face. */
+SW_API int sw_mlp_forward(const float* params, const float* x, int64_t n, float* y, void* stream);
+/* grad += sum over n samples of (d net(x_s) / d params)^T dy_s: the
+ * parameter gradient for given output adjoints dy (n x 5). */
+SW_API int sw_mlp_backward(const float* params, const float* x, const float* dy, int64_t n, float* grad,
+                           void* stream);
+/* Adjoint of one sw2d_abc_correct for training through the time loop.
+ * fields: the uncorrected state (five (nx, nz) arrays packed back to back, as
+ * the first five of a sw2d_record snapshot slot); adj: the five adjoint field
+ * arrays, which hold the adjoint of the corrected state on entry and of the
+ * uncorrected state on return; ybar (ncell x 5) receives the adjoint of the
+ * network outputs (feed it with the layer's inputs to sw_mlp_backward). */
+SW_API int sw2d_abc_adjoint(sw_plan* plan, const sw_abc_desc* abc, const float* fields, float* const* adj,
+                            float* ybar, void* stream);
+
 /* ---- 2D adjoint (no reference counterpart) --------------------------------
  * Hand-written discrete adjoint of the SW2D_SSG_VS time loop with a
  * SW_SRC_MOMENT (or no) source and vz receivers, for gradients of a seismogram

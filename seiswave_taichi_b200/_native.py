@@ -32,8 +32,21 @@ EXPORTS = (
     "sw_run", "sw_check_finite", "sw_plan_status", "sw_plan_info", "sw_plan_set_path",
     "sw_plan_set_exact", "sw_count_nonfinite_noalloc", "sw2d_snapshot_elems", "sw2d_record",
     "sw2d_adjoint_run", "sw2d_batch_create", "sw_batch_set_tile", "sw_batch_info", "sw_batch_run",
-    "sw_batch_destroy",
+    "sw_batch_destroy", "sw2d_abc_correct", "sw2d_abc_features", "sw_mlp_grad", "sw_mlp_forward",
+    "sw_mlp_backward", "sw2d_abc_adjoint",
 )
+
+SW_ABC_DEPTH = 6
+SW_ABC_INPUTS = 45 + SW_ABC_DEPTH
+SW_ABC_HIDDEN = 32
+SW_ABC_PARAMS = (SW_ABC_HIDDEN * SW_ABC_INPUTS + SW_ABC_HIDDEN + SW_ABC_HIDDEN * SW_ABC_HIDDEN + SW_ABC_HIDDEN
+                 + 5 * SW_ABC_HIDDEN + 5)
+
+
+class AbcDesc(C.Structure):
+    _fields_ = [("ncell", C.c_int32), ("cell", C.c_void_p), ("face", C.c_void_p), ("depth", C.c_void_p),
+                ("params", C.c_void_p), ("scale", C.c_float * 5), ("oscale", C.c_float * 5),
+                ("delta", C.c_void_p)]
 
 
 class Adjoint2D(C.Structure):
@@ -133,6 +146,12 @@ def load() -> C.CDLL:
         "sw_batch_info": (C.c_int, [vp, C.POINTER(C.c_int32)]),
         "sw_batch_run": (C.c_int, [vp, C.c_int32, C.c_int32, C.c_int32, vp]),
         "sw_batch_destroy": (C.c_int, [vp]),
+        "sw2d_abc_correct": (C.c_int, [vp, C.POINTER(AbcDesc), vp]),
+        "sw2d_abc_features": (C.c_int, [vp, C.POINTER(AbcDesc), vp, vp]),
+        "sw_mlp_grad": (C.c_int, [vp, vp, vp, C.c_int64, vp, vp, vp]),
+        "sw_mlp_forward": (C.c_int, [vp, vp, C.c_int64, vp, vp]),
+        "sw_mlp_backward": (C.c_int, [vp, vp, vp, C.c_int64, vp, vp]),
+        "sw2d_abc_adjoint": (C.c_int, [vp, C.POINTER(AbcDesc), vp, C.POINTER(vp), vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -41,6 +41,25 @@ struct A2 {
   const T* snap1;
 };
 template <typename T> cudaError_t sw2_adjoint_step(const P2<T>&, const A2<T>&, int, int, cudaStream_t);
+struct AbcArgs {
+  const int* cell;
+  const int8_t* face;
+  const int8_t* depth;
+  int ncell;
+  int nx, nz;
+  const float* f[5];
+  float* fw[5];
+  float scale[5];
+  float oscale[5];
+  const float* params;
+  float* delta;
+  float* x_out;
+};
+cudaError_t abc_correct(const AbcArgs&, cudaStream_t);
+cudaError_t abc_features(const AbcArgs&, cudaStream_t);
+cudaError_t mlp_grad(const float*, const float*, const float*, long long, float*, float*, int, cudaStream_t);
+cudaError_t abc_adjoint(const AbcArgs&, float* const*, float*, cudaStream_t);
+cudaError_t mlp_forward_batch(const float*, const float*, long long, float*, cudaStream_t);
 }  // namespace sw
 
 namespace {
@@ -905,6 +924,92 @@ int sw2d_adjoint_run(sw_plan* pl, const sw2d_adjoint_desc* d, int32_t it0, int32
                                       : adjoint2<double>(pl, pl->p2d, d, it0, nsteps, (const double*)snap, st);
   if (e != cudaSuccess) return cuda_fail(e, "sw2d_adjoint_run");
   return SW_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// learned thin absorbing layer (2D)
+// ---------------------------------------------------------------------------
+namespace {
+
+int abc_args(sw_plan* pl, const sw_abc_desc* d, const char* who, sw::AbcArgs* a) {
+  if (!pl || !d) return fail(SW_ERR_ARG, std::string(who) + ": null plan or descriptor");
+  if (pl->dim != 2 || pl->dtype != SW_F32)
+    return fail(SW_ERR_UNSUPPORTED, std::string(who) + ": the learned layer runs on float32 2D plans");
+  if (d->ncell < 0 || (d->ncell > 0 && (!d->cell || !d->face || !d->depth || !d->params || !d->delta)))
+    return fail(SW_ERR_ARG, std::string(who) + ": layer tables, parameters or scratch missing");
+  for (int f = 0; f < 5; ++f)
+    if (!(d->scale[f] > 0.f) || !(d->oscale[f] >= 0.f))
+      return fail(SW_ERR_ARG, std::string(who) + ": field scales must be positive");
+  *a = sw::AbcArgs{};
+  a->cell = d->cell; a->face = d->face; a->depth = d->depth; a->ncell = d->ncell;
+  a->nx = pl->p2f.nx; a->nz = pl->p2f.nz;
+  for (int f = 0; f < 5; ++f) {
+    a->f[f] = pl->p2f.f[f];
+    a->fw[f] = pl->p2f.f[f];
+    a->scale[f] = d->scale[f];
+    a->oscale[f] = d->oscale[f];
+  }
+  a->params = d->params;
+  a->delta = d->delta;
+  return SW_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sw2d_abc_correct(sw_plan* pl, const sw_abc_desc* d, void* stream) {
+  sw::AbcArgs a;
+  int rc = abc_args(pl, d, "sw2d_abc_correct", &a);
+  if (rc != SW_OK) return rc;
+  cudaError_t e = sw::abc_correct(a, (cudaStream_t)stream);
+  return e == cudaSuccess ? SW_OK : cuda_fail(e, "sw2d_abc_correct");
+}
+
+int sw2d_abc_features(sw_plan* pl, const sw_abc_desc* d, float* x, void* stream) {
+  sw::AbcArgs a;
+  int rc = abc_args(pl, d, "sw2d_abc_features", &a);
+  if (rc != SW_OK) return rc;
+  if (d->ncell > 0 && !x) return fail(SW_ERR_ARG, "sw2d_abc_features: null output");
+  a.x_out = x;
+  cudaError_t e = sw::abc_features(a, (cudaStream_t)stream);
+  return e == cudaSuccess ? SW_OK : cuda_fail(e, "sw2d_abc_features");
+}
+
+int sw_mlp_grad(const float* params, const float* x, const float* y, int64_t n, float* grad, float* loss,
+                void* stream) {
+  if (n < 0 || (n > 0 && (!params || !x || !y || !grad || !loss))) return fail(SW_ERR_ARG, "sw_mlp_grad: arguments");
+  cudaError_t e = sw::mlp_grad(params, x, y, n, grad, loss, 0, (cudaStream_t)stream);
+  return e == cudaSuccess ? SW_OK : cuda_fail(e, "sw_mlp_grad");
+}
+
+int sw_mlp_backward(const float* params, const float* x, const float* dy, int64_t n, float* grad, void* stream) {
+  if (n < 0 || (n > 0 && (!params || !x || !dy || !grad))) return fail(SW_ERR_ARG, "sw_mlp_backward: arguments");
+  cudaError_t e = sw::mlp_grad(params, x, dy, n, grad, nullptr, 1, (cudaStream_t)stream);
+  return e == cudaSuccess ? SW_OK : cuda_fail(e, "sw_mlp_backward");
+}
+
+int sw2d_abc_adjoint(sw_plan* pl, const sw_abc_desc* d, const float* fields, float* const* adj, float* ybar,
+                     void* stream) {
+  sw::AbcArgs a;
+  int rc = abc_args(pl, d, "sw2d_abc_adjoint", &a);
+  if (rc != SW_OK) return rc;
+  if (d->ncell > 0 && (!fields || !adj || !ybar)) return fail(SW_ERR_ARG, "sw2d_abc_adjoint: null argument");
+  const long long nc = (long long)a.nx * a.nz;
+  for (int f = 0; f < 5; ++f) {
+    if (d->ncell > 0 && !adj[f]) return fail(SW_ERR_ARG, "sw2d_abc_adjoint: adjoint field missing");
+    a.f[f] = fields + f * nc;
+  }
+  cudaError_t e = sw::abc_adjoint(a, adj, ybar, (cudaStream_t)stream);
+  return e == cudaSuccess ? SW_OK : cuda_fail(e, "sw2d_abc_adjoint");
+}
+
+int sw_mlp_forward(const float* params, const float* x, int64_t n, float* y, void* stream) {
+  if (n < 0 || (n > 0 && (!params || !x || !y))) return fail(SW_ERR_ARG, "sw_mlp_forward: arguments");
+  cudaError_t e = sw::mlp_forward_batch(params, x, n, y, (cudaStream_t)stream);
+  return e == cudaSuccess ? SW_OK : cuda_fail(e, "sw_mlp_forward");
 }
 
 }  // extern "C"
