@@ -143,6 +143,47 @@ __device__ __forceinline__ float4 divc4(float4 v, float d, float r, int fast) {
   return make_float4(div_c(v.x, d, r, fast), div_c(v.y, d, r, fast), div_c(v.z, d, r, fast),
                      div_c(v.w, d, r, fast));
 }
+// Exact division of a group of stencil sums by the constant spacings.  When
+// the spacings' Markstein path is verified (fast != 0) and every lane is zero
+// or of magnitude in [2^-100, 2^100), the whole group runs as one branch-free
+// block: the same correction div_c applies to such lanes, with zeros passed
+// through unchanged (so the sign of zero is kept).  Otherwise every lane is
+// divided in double precision and rounded once to float -- the correctly
+// rounded float quotient for every finite float input (innocuous double
+// rounding, 53 >= 2*24+2), the same result div_c gives -- again without a
+// per-lane branch.  Keeping range tests off the per-lane path leaves the
+// group's independent lanes free to interleave.
+__device__ __forceinline__ bool mk_ok(float x) {
+  const unsigned u = __float_as_uint(x) & 0x7fffffffu;
+  return (u - 0x0D800000u < 0x64000000u) | (u == 0u);
+}
+__device__ __forceinline__ float dd_div(float x, float d) {
+  const float y = __double2float_rn(__ddiv_rn((double)x, (double)d));
+  return x == 0.f ? x : y;
+}
+__device__ __forceinline__ float mk_div(float x, float d, float r) {
+  const float q = __fmul_rn(x, r);
+  const float e = __fmaf_rn(-q, d, x);
+  const float y = __fmaf_rn(e, r, q);
+  return x == 0.f ? x : y;
+}
+template <int K>
+__device__ __forceinline__ void div_group(float4 (&v)[K], const float (&d)[K], const float (&r)[K], int fast) {
+  bool ok = fast != 0;
+#pragma unroll
+  for (int k = 0; k < K; ++k) ok = ok & mk_ok(v[k].x) & mk_ok(v[k].y) & mk_ok(v[k].z) & mk_ok(v[k].w);
+  if (ok) {
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+      v[k] = make_float4(mk_div(v[k].x, d[k], r[k]), mk_div(v[k].y, d[k], r[k]), mk_div(v[k].z, d[k], r[k]),
+                         mk_div(v[k].w, d[k], r[k]));
+  } else {
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+      v[k] = make_float4(dd_div(v[k].x, d[k]), dd_div(v[k].y, d[k]), dd_div(v[k].z, d[k]), dd_div(v[k].w, d[k]));
+  }
+}
+
 // exact mode divides the stencil sum by the spacing; fast mode folded it into c
 template <bool EX>
 __device__ __forceinline__ float4 dv4(float4 v, float d, float r, int fast) {
@@ -330,30 +371,59 @@ k3s_velocity(const __grid_constant__ P3<float> p, const __grid_constant__ Staged
         const size_t gi = (size_t)i * nyz + (size_t)j * nz + k;
         const float4 rc = ld4(r0 + o_xx), rn = ld4(r0 + o_xx + G::TZ);
         // derivatives of the three components (Dx3fm/Dy3bm/Dz3bm etc.)
-        float4 a1 = dv4<EX>(dxq<N, EX>(pxx, o_xx, cx), dx, rdx, fast);
-        float4 a2 = dv4<EX>(dyq<N, false, EX>(sxy_p(i), o_y, G::TZ, cy), dy, rdy, fast);
-        float4 a3 = dv4<EX>(dzq<N, false, EX>(sxz_p(i), o_z, cz), dz, rdz, fast);
-        float4 b1 = dv4<EX>(dxq<N, EX>(pxy, o_y, cx), dx, rdx, fast);
-        float4 b2 = dv4<EX>(dyq<N, true, EX>(syy_p(i), o_y, G::TZ, cy), dy, rdy, fast);
-        float4 b3 = dv4<EX>(dzq<N, false, EX>(syz_p(i), o_yz, cz), dz, rdz, fast);
-        float4 c1 = dv4<EX>(dxq<N, EX>(pxz, o_z, cx), dx, rdx, fast);
-        float4 c2 = dv4<EX>(dyq<N, false, EX>(syz_p(i), o_yz, G::WZ, cy), dy, rdy, fast);
-        float4 c3 = dv4<EX>(dzq<N, true, EX>(szz_p(i), o_z, cz), dz, rdz, fast);
+        float4 dv[9] = {dxq<N, EX>(pxx, o_xx, cx),
+                        dyq<N, false, EX>(sxy_p(i), o_y, G::TZ, cy),
+                        dzq<N, false, EX>(sxz_p(i), o_z, cz),
+                        dxq<N, EX>(pxy, o_y, cx),
+                        dyq<N, true, EX>(syy_p(i), o_y, G::TZ, cy),
+                        dzq<N, false, EX>(syz_p(i), o_yz, cz),
+                        dxq<N, EX>(pxz, o_z, cx),
+                        dyq<N, false, EX>(syz_p(i), o_yz, G::WZ, cy),
+                        dzq<N, true, EX>(szz_p(i), o_z, cz)};
+        if (EX) {
+          const float hd[9] = {dx, dy, dz, dx, dy, dz, dx, dy, dz};
+          const float hr[9] = {rdx, rdy, rdz, rdx, rdy, rdz, rdx, rdy, rdz};
+          div_group<9>(dv, hd, hr, fast);
+        }
+        float4 a1 = dv[0], a2 = dv[1], a3 = dv[2], b1 = dv[3], b2 = dv[4], b3 = dv[5], c1 = dv[6], c2 = dv[7],
+               c3 = dv[8];
         float4 vx = ldg4(p.f[0] + gi), vy = ldg4(p.f[1] + gi), vz = ldg4(p.f[2] + gi);
         if (interior) {
           const float4 r1c = ld4(r1 + o_xx), r1n = ld4(r1 + o_xx + G::TZ);
+          // numerators and densities of the 12 updates, then their quotients
+          // as one group (see div_group: no per-lane range branch)
+          float tn[12], td[12];
 #pragma unroll
           for (int e = 0; e < 4; ++e) {
             const float rce = g4(rc, e), rne = g4(rn, e);
-            float t = (g4(a1, e) + g4(a3, e) + g4(a2, e)) * dt;
-            s4(vx, e, g4(vx, e) + dvv<EX>(t, rce));
-            const float rhy = 0.5f * (rce + rne);
-            t = (g4(b1, e) + g4(b2, e) + g4(b3, e)) * dt;
-            s4(vy, e, g4(vy, e) + dvv<EX>(t, rhy));
-            const float r4 = 0.25f * (rce + rne + g4(r1n, e) + g4(r1c, e));
+            tn[e] = (g4(a1, e) + g4(a3, e) + g4(a2, e)) * dt;
+            td[e] = rce;
+            tn[4 + e] = (g4(b1, e) + g4(b2, e) + g4(b3, e)) * dt;
+            td[4 + e] = 0.5f * (rce + rne);
             const float sum = TENSOR ? (g4(c1, e) + g4(c2, e) + g4(c3, e)) : (g4(c3, e) + g4(c1, e) + g4(c2, e));
-            t = sum * dt;
-            s4(vz, e, g4(vz, e) + dvv<EX>(t, r4));
+            tn[8 + e] = sum * dt;
+            td[8 + e] = 0.25f * (rce + rne + g4(r1n, e) + g4(r1c, e));
+          }
+          if (EX) {
+            bool okq = true;
+#pragma unroll
+            for (int q = 0; q < 12; ++q) okq = okq & mk_ok(tn[q]);
+            if (okq) {
+#pragma unroll
+              for (int q = 0; q < 12; ++q) tn[q] = tn[q] == 0.f ? tn[q] : __fdiv_rn(tn[q], td[q]);
+            } else {
+#pragma unroll
+              for (int q = 0; q < 12; ++q) tn[q] = dd_div(tn[q], td[q]);
+            }
+          } else {
+#pragma unroll
+            for (int q = 0; q < 12; ++q) tn[q] = __fdividef(tn[q], td[q]);
+          }
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            s4(vx, e, g4(vx, e) + tn[e]);
+            s4(vy, e, g4(vy, e) + tn[4 + e]);
+            s4(vz, e, g4(vz, e) + tn[8 + e]);
           }
         } else {
           QuadPml q{xi, yj, i, j, k, p.fl[0][i], fy};
@@ -571,16 +641,23 @@ k3s_stress(const __grid_constant__ P3<float> p, const __grid_constant__ StagedMa
         const float4 u0 = ld4(m0p + o_m), u1 = ld4(mu_p(i + 1) + o_m), unj = ld4(m0p + o_m + G::WM);
         const float4 u0s = ld4(m0p + o_m + 4);  // mu[k+4 .. k+7] for the k+1 neighbour
         const float unk[4] = {u0.y, u0.z, u0.w, u0s.x};
-        // derivatives
-        float4 e1 = dv4<EX>(dxq<N, EX>(pvx, o_v, cx), dx, rdx, fast);                 // dvx/dx
-        float4 e2 = dv4<EX>(dyq<N, false, EX>(vyi, o_v, G::WZ, cy), dy, rdy, fast);   // dvy/dy
-        float4 e3 = dv4<EX>(dzq<N, false, EX>(vzi, o_v, cz), dz, rdz, fast);          // dvz/dz
-        float4 f1 = dv4<EX>(dxq<N, EX>(pvy, o_v, cx), dx, rdx, fast);                 // dvy/dx
-        float4 f2 = dv4<EX>(dyq<N, true, EX>(vxi, o_v, G::WZ, cy), dy, rdy, fast);    // dvx/dy
-        float4 h1 = dv4<EX>(dxq<N, EX>(pvz, o_v, cx), dx, rdx, fast);                 // dvz/dx
-        float4 h2 = dv4<EX>(dzq<N, true, EX>(vxi, o_v, cz), dz, rdz, fast);           // dvx/dz
-        float4 q1 = dv4<EX>(dyq<N, true, EX>(vzi, o_v, G::WZ, cy), dy, rdy, fast);    // dvz/dy
-        float4 q2 = dv4<EX>(dzq<N, true, EX>(vyi, o_v, cz), dz, rdz, fast);           // dvy/dz
+        // derivatives: dvx/dx dvy/dy dvz/dz dvy/dx dvx/dy dvz/dx dvx/dz dvz/dy dvy/dz
+        float4 dv[9] = {dxq<N, EX>(pvx, o_v, cx),
+                        dyq<N, false, EX>(vyi, o_v, G::WZ, cy),
+                        dzq<N, false, EX>(vzi, o_v, cz),
+                        dxq<N, EX>(pvy, o_v, cx),
+                        dyq<N, true, EX>(vxi, o_v, G::WZ, cy),
+                        dxq<N, EX>(pvz, o_v, cx),
+                        dzq<N, true, EX>(vxi, o_v, cz),
+                        dyq<N, true, EX>(vzi, o_v, G::WZ, cy),
+                        dzq<N, true, EX>(vyi, o_v, cz)};
+        if (EX) {
+          const float hd[9] = {dx, dy, dz, dx, dy, dx, dz, dy, dz};
+          const float hr[9] = {rdx, rdy, rdz, rdx, rdy, rdx, rdz, rdy, rdz};
+          div_group<9>(dv, hd, hr, fast);
+        }
+        float4 e1 = dv[0], e2 = dv[1], e3 = dv[2], f1 = dv[3], f2 = dv[4], h1 = dv[5], h2 = dv[6], q1 = dv[7],
+               q2 = dv[8];
         if (interior) {
 #pragma unroll
           for (int e = 0; e < 4; ++e) {
