@@ -238,6 +238,23 @@ def run_reference(args, rank, world):
     return 0
 
 
+def max_over_ranks(ms: float, dist, device="cuda") -> float:
+    """The slowest rank's device time: every rank takes part, in the same
+    order, and gets the maximum (a no-op on one process)."""
+    if dist is None:
+        return ms
+    import torch
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_value(world: int, ncell: int, nt: int, steps: int, ms: float) -> float:
+    """Gcell-updates/s of the whole job: every rank runs its own replica of
+    the workload (weak scaling), timed by the slowest rank."""
+    return world * ncell * nt * steps / (ms * 1e-3) / 1e9
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -290,13 +307,9 @@ def main(argv=None):
             one_run()
         e1.record(stream)
         torch.cuda.synchronize()
-    ms_total = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([ms_total], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_total = float(t.item())
+    ms_total = max_over_ranks(e0.elapsed_time(e1), dist)
     ms_step = ms_total / args.steps
-    value = world * ncell * nt * args.steps / (ms_total * 1e-3) / 1e9
+    value = whole_job_value(world, ncell, nt, args.steps, ms_total)
 
     # roofline of one time step (velocity + stress pass)
     peak, peak_kind = peaks()
@@ -328,12 +341,8 @@ def main(argv=None):
         e2e_run()
     e1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = world * ncell * nt * args.steps / (e2e_ms * 1e-3) / 1e9
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), dist)
+    e2e_value = whole_job_value(world, ncell, nt, args.steps, e2e_ms)
 
     # the opt-in fast numeric mode (exact=False) on the same workload
     fast = None
@@ -349,13 +358,9 @@ def main(argv=None):
             wf.run(nt)
         e1.record(stream)
         torch.cuda.synchronize()
-        f_ms = e0.elapsed_time(e1)
-        if dist:
-            t = torch.tensor([f_ms], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            f_ms = float(t.item())
+        f_ms = max_over_ranks(e0.elapsed_time(e1), dist)
         f_tstep = f_ms / args.steps / nt
-        fast = {"value": world * ncell * nt * args.steps / (f_ms * 1e-3) / 1e9, "unit": "Gcell-updates/s",
+        fast = {"value": whole_job_value(world, ncell, nt, args.steps, f_ms), "unit": "Gcell-updates/s",
                 "ms_per_step": f_ms / args.steps,
                 "roofline_frac": alg / (f_tstep * 1e-3) / 1e9 / peak,
                 "parity": "traces within 1e-5 rel. L2 of the oracle over 400 steps; fields within 1e-4"}
