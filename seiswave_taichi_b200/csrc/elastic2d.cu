@@ -41,35 +41,49 @@ __device__ __forceinline__ void vel2_cell(const P2<T>& p, int i, int j, int it, 
   const bool any_slab = (xi >= 0 || zj >= 0);
 
   if (SCHEME == SW2D_SSG_VS) {
-    // vx at (i, j): :144-154
-    if (i >= N + 1 && i < nx - N && j >= N + 1 && j < nz - N) {
-      T dsxxdx = div_c(dx_bm<T, N>(sxx, idx, nz, c), dx, p.rd[0], p.fast_div & 1);
-      T dsxzdz = div_c(dz_bm<T, N>(sxz, idx, c), dz, p.rd[1], p.fast_div & 1);
+    // vx at (i, j) :144-154; vz at (i+1/2, j+1/2) :156-167, then the source :170
+    const bool ux = i >= N + 1 && i < nx - N && j >= N + 1 && j < nz - N;
+    const bool uz = i >= N && i < nx - N - 1 && j >= N && j < nz - N - 1;
+    const bool src = src_here && i == p.si && j == p.sk;
+    // stencil sums of both components, divided by the spacings as one group
+    T sd[4] = {0, 0, 0, 0};
+    if (ux) {
+      sd[0] = dx_bm<T, N>(sxx, idx, nz, c);
+      sd[1] = dz_bm<T, N>(sxz, idx, c);
+    }
+    if (uz) {
+      sd[2] = dx_fm<T, N>(sxz, idx, nz, c);
+      sd[3] = dz_fm<T, N>(szz, idx, c);
+    }
+    {
+      const T hd[4] = {dx, dz, dx, dz};
+      const T hr[4] = {p.rd[0], p.rd[1], p.rd[0], p.rd[1]};
+      divc_group<4>(sd, hd, hr, p.fast_div & 1);
+    }
+    T tq[2] = {0, 0}, td[2] = {1, 1};
+    if (ux) {
+      T dsxxdx = sd[0], dsxzdz = sd[1];
       if (any_slab && ((fx & 1) || (fz & 1))) {
         if (xi >= 0) pml2(mx(p, 0, xi, j), cfx[CB * nx + i], cfx[CA * nx + i], cfx[CK * nx + i], dsxxdx);
         if (zj >= 0) pml2(mz(p, 0, i, zj), cfz[CB * nz + j], cfz[CA * nz + j], cfz[CK * nz + j], dsxzdz);
       }
-      T t = (dsxxdx + dsxzdz) * dt;
-      t = div_v(t, ldg(rho + idx));
-      vx[idx] = vx[idx] + t;
+      tq[0] = (dsxxdx + dsxzdz) * dt;
+      td[0] = ldg(rho + idx);
     }
-    // vz at (i+1/2, j+1/2): :156-167, then the source :170
-    const bool upd = i >= N && i < nx - N - 1 && j >= N && j < nz - N - 1;
-    const bool src = src_here && i == p.si && j == p.sk;
-    if (upd || src) {
-      T v = vz[idx];
-      if (upd) {
-        const T rh = (T)0.25 * (ldg(rho + idx) + ldg(rho + idx + 1) + ldg(rho + idx + nz + 1) + ldg(rho + idx + nz));
-        T dsxzdx = div_c(dx_fm<T, N>(sxz, idx, nz, c), dx, p.rd[0], p.fast_div & 1);
-        T dszzdz = div_c(dz_fm<T, N>(szz, idx, c), dz, p.rd[1], p.fast_div & 1);
-        if (any_slab && ((fx & 2) || (fz & 2))) {
-          if (xi >= 0) pml2(mx(p, 1, xi, j), cfx[CBH * nx + i], cfx[CAH * nx + i], cfx[CKH * nx + i], dsxzdx);
-          if (zj >= 0) pml2(mz(p, 1, i, zj), cfz[CBH * nz + j], cfz[CAH * nz + j], cfz[CKH * nz + j], dszzdz);
-        }
-        T t = (dszzdz + dsxzdx) * dt;
-        t = div_v(t, rh);
-        v = v + t;
+    if (uz) {
+      td[1] = (T)0.25 * (ldg(rho + idx) + ldg(rho + idx + 1) + ldg(rho + idx + nz + 1) + ldg(rho + idx + nz));
+      T dsxzdx = sd[2], dszzdz = sd[3];
+      if (any_slab && ((fx & 2) || (fz & 2))) {
+        if (xi >= 0) pml2(mx(p, 1, xi, j), cfx[CBH * nx + i], cfx[CAH * nx + i], cfx[CKH * nx + i], dsxzdx);
+        if (zj >= 0) pml2(mz(p, 1, i, zj), cfz[CBH * nz + j], cfz[CAH * nz + j], cfz[CKH * nz + j], dszzdz);
       }
+      tq[1] = (dszzdz + dsxzdx) * dt;
+    }
+    divv_group<2>(tq, td);
+    if (ux) vx[idx] = vx[idx] + tq[0];
+    if (uz || src) {
+      T v = vz[idx];
+      if (uz) v = v + tq[1];
       if (src) {
         T t = dt * p.wav[it];
         t = div_v(t, ldg(rho + idx));
@@ -78,23 +92,47 @@ __device__ __forceinline__ void vel2_cell(const P2<T>& p, int i, int j, int it, 
       vz[idx] = v;
     }
   } else if (SCHEME == SW2D_SSG_SV) {
-    // vx at (i+1/2, j): :218-229, then the source :245
-    const bool upd = i >= N && i < nx - N - 1 && j >= N + 1 && j < nz - N;
+    // vx at (i+1/2, j) :218-229, then the source :245; vz at (i, j+1/2) :231-242
+    const bool ux = i >= N && i < nx - N - 1 && j >= N + 1 && j < nz - N;
+    const bool uz = i >= N + 1 && i < nx - N && j >= N && j < nz - N - 1;
     const bool src = src_here && i == p.si && j == p.sk;
-    if (upd || src) {
-      T v = vx[idx];
-      if (upd) {
-        T dsxxdx = div_c(dx_fm<T, N>(sxx, idx, nz, c), dx, p.rd[0], p.fast_div & 1);
-        T dsxzdz = div_c(dz_bm<T, N>(sxz, idx, c), dz, p.rd[1], p.fast_div & 1);
-        const T rhx = (ldg(rho + idx) + ldg(rho + idx + nz)) / (T)2;
-        if (any_slab && ((fx & 2) || (fz & 1))) {
-          if (xi >= 0) pml2(mx(p, 0, xi, j), cfx[CBH * nx + i], cfx[CAH * nx + i], cfx[CKH * nx + i], dsxxdx);
-          if (zj >= 0) pml2(mz(p, 0, i, zj), cfz[CB * nz + j], cfz[CA * nz + j], cfz[CK * nz + j], dsxzdz);
-        }
-        T t = (dsxxdx + dsxzdz) * dt;
-        t = div_v(t, rhx);
-        v = v + t;
+    T sd[4] = {0, 0, 0, 0};
+    if (ux) {
+      sd[0] = dx_fm<T, N>(sxx, idx, nz, c);
+      sd[1] = dz_bm<T, N>(sxz, idx, c);
+    }
+    if (uz) {
+      sd[2] = dx_bm<T, N>(sxz, idx, nz, c);
+      sd[3] = dz_fm<T, N>(szz, idx, c);
+    }
+    {
+      const T hd[4] = {dx, dz, dx, dz};
+      const T hr[4] = {p.rd[0], p.rd[1], p.rd[0], p.rd[1]};
+      divc_group<4>(sd, hd, hr, p.fast_div & 1);
+    }
+    T tq[2] = {0, 0}, td[2] = {1, 1};
+    if (ux) {
+      T dsxxdx = sd[0], dsxzdz = sd[1];
+      td[0] = (ldg(rho + idx) + ldg(rho + idx + nz)) / (T)2;
+      if (any_slab && ((fx & 2) || (fz & 1))) {
+        if (xi >= 0) pml2(mx(p, 0, xi, j), cfx[CBH * nx + i], cfx[CAH * nx + i], cfx[CKH * nx + i], dsxxdx);
+        if (zj >= 0) pml2(mz(p, 0, i, zj), cfz[CB * nz + j], cfz[CA * nz + j], cfz[CK * nz + j], dsxzdz);
       }
+      tq[0] = (dsxxdx + dsxzdz) * dt;
+    }
+    if (uz) {
+      td[1] = (T)0.5 * (ldg(rho + idx) + ldg(rho + idx + 1));
+      T dsxzdx = sd[2], dszzdz = sd[3];
+      if (any_slab && ((fx & 1) || (fz & 2))) {
+        if (xi >= 0) pml2(mx(p, 1, xi, j), cfx[CB * nx + i], cfx[CA * nx + i], cfx[CK * nx + i], dsxzdx);
+        if (zj >= 0) pml2(mz(p, 1, i, zj), cfz[CBH * nz + j], cfz[CAH * nz + j], cfz[CKH * nz + j], dszzdz);
+      }
+      tq[1] = (dszzdz + dsxzdx) * dt;
+    }
+    divv_group<2>(tq, td);
+    if (ux || src) {
+      T v = vx[idx];
+      if (ux) v = v + tq[0];
       if (src) {
         T t = dt * p.wav[it];
         t = div_v(t, ldg(rho + idx));
@@ -102,19 +140,7 @@ __device__ __forceinline__ void vel2_cell(const P2<T>& p, int i, int j, int it, 
       }
       vx[idx] = v;
     }
-    // vz at (i, j+1/2): :231-242
-    if (i >= N + 1 && i < nx - N && j >= N && j < nz - N - 1) {
-      const T rhz = (T)0.5 * (ldg(rho + idx) + ldg(rho + idx + 1));
-      T dsxzdx = div_c(dx_bm<T, N>(sxz, idx, nz, c), dx, p.rd[0], p.fast_div & 1);
-      T dszzdz = div_c(dz_fm<T, N>(szz, idx, c), dz, p.rd[1], p.fast_div & 1);
-      if (any_slab && ((fx & 1) || (fz & 2))) {
-        if (xi >= 0) pml2(mx(p, 1, xi, j), cfx[CB * nx + i], cfx[CA * nx + i], cfx[CK * nx + i], dsxzdx);
-        if (zj >= 0) pml2(mz(p, 1, i, zj), cfz[CBH * nz + j], cfz[CAH * nz + j], cfz[CKH * nz + j], dszzdz);
-      }
-      T t = (dszzdz + dsxzdx) * dt;
-      t = div_v(t, rhz);
-      vz[idx] = vz[idx] + t;
-    }
+    if (uz) vz[idx] = vz[idx] + tq[1];
   } else {  // SW2D_RSG, :292-323
     const bool upd = i >= N + 1 && i < nx - N && j >= N + 1 && j < nz - N;
     const bool src = src_here && (i == p.si || i == p.si - 1) && (j == p.sk || j == p.sk - 1);
@@ -181,13 +207,28 @@ __device__ __forceinline__ void str2_cell(const P2<T>& p, int i, int j, int it, 
   const bool any_slab = (xi >= 0 || zj >= 0);
 
   if (SCHEME == SW2D_SSG_VS) {
-    // sxx szz at (i+1/2, j): :172-186
-    if (i >= N && i < nx - N - 1 && j >= N + 1 && j < nz - N) {
+    // sxx szz at (i+1/2, j) :172-186; sxz at (i, j+1/2) :188-199
+    const bool un = i >= N && i < nx - N - 1 && j >= N + 1 && j < nz - N;
+    const bool us = i >= N + 1 && i < nx - N && j >= N && j < nz - N - 1;
+    T sd[4] = {0, 0, 0, 0};
+    if (un) {
+      sd[0] = dx_fm<T, N>(vx, idx, nz, c);
+      sd[1] = dz_bm<T, N>(vz, idx, c);
+    }
+    if (us) {
+      sd[2] = dx_bm<T, N>(vz, idx, nz, c);
+      sd[3] = dz_fm<T, N>(vx, idx, c);
+    }
+    {
+      const T hd[4] = {dx, dz, dx, dz};
+      const T hr[4] = {p.rd[0], p.rd[1], p.rd[0], p.rd[1]};
+      divc_group<4>(sd, hd, hr, p.fast_div & 1);
+    }
+    if (un) {
       const T lhx = (T)0.5 * (ldg(lam + idx) + ldg(lam + idx + nz));
       const T mhx = (T)0.5 * (ldg(mu + idx) + ldg(mu + idx + nz));
       const T lpm = lhx + (T)2 * mhx;
-      T dvxdx = div_c(dx_fm<T, N>(vx, idx, nz, c), dx, p.rd[0], p.fast_div & 1);
-      T dvzdz = div_c(dz_bm<T, N>(vz, idx, c), dz, p.rd[1], p.fast_div & 1);
+      T dvxdx = sd[0], dvzdz = sd[1];
       if (any_slab && ((fx & 2) || (fz & 1))) {
         if (xi >= 0) pml2(mx(p, 2, xi, j), cfx[CBH * nx + i], cfx[CAH * nx + i], cfx[CKH * nx + i], dvxdx);
         if (zj >= 0) pml2(mz(p, 2, i, zj), cfz[CB * nz + j], cfz[CA * nz + j], cfz[CK * nz + j], dvzdz);
@@ -195,11 +236,9 @@ __device__ __forceinline__ void str2_cell(const P2<T>& p, int i, int j, int it, 
       sxx[idx] = sxx[idx] + (lpm * dvxdx + lhx * dvzdz) * dt;
       szz[idx] = szz[idx] + (lpm * dvzdz + lhx * dvxdx) * dt;
     }
-    // sxz at (i, j+1/2): :188-199
-    if (i >= N + 1 && i < nx - N && j >= N && j < nz - N - 1) {
+    if (us) {
       const T mhz = (T)0.5 * (ldg(mu + idx + 1) + ldg(mu + idx));
-      T dvzdx = div_c(dx_bm<T, N>(vz, idx, nz, c), dx, p.rd[0], p.fast_div & 1);
-      T dvxdz = div_c(dz_fm<T, N>(vx, idx, c), dz, p.rd[1], p.fast_div & 1);
+      T dvzdx = sd[2], dvxdz = sd[3];
       if (any_slab && ((fx & 1) || (fz & 2))) {
         if (xi >= 0) pml2(mx(p, 3, xi, j), cfx[CB * nx + i], cfx[CA * nx + i], cfx[CK * nx + i], dvzdx);
         if (zj >= 0) pml2(mz(p, 3, i, zj), cfz[CBH * nz + j], cfz[CAH * nz + j], cfz[CKH * nz + j], dvxdz);
@@ -207,12 +246,25 @@ __device__ __forceinline__ void str2_cell(const P2<T>& p, int i, int j, int it, 
       sxz[idx] = sxz[idx] + mhz * (dvxdz + dvzdx) * dt;
     }
   } else if (SCHEME == SW2D_SSG_SV) {
-    // sxx szz at (i, j): :247-260
-    if (i >= N + 1 && i < nx - N && j >= N + 1 && j < nz - N) {
+    // sxx szz at (i, j) :247-260; sxz at (i+1/2, j+1/2) :262-273
+    const bool un = i >= N + 1 && i < nx - N && j >= N + 1 && j < nz - N;
+    const bool us = un;
+    T sd[4] = {0, 0, 0, 0};
+    if (un) {
+      sd[0] = dx_bm<T, N>(vx, idx, nz, c);
+      sd[1] = dz_bm<T, N>(vz, idx, c);
+      sd[2] = dx_fm<T, N>(vz, idx, nz, c);
+      sd[3] = dz_fm<T, N>(vx, idx, c);
+    }
+    {
+      const T hd[4] = {dx, dz, dx, dz};
+      const T hr[4] = {p.rd[0], p.rd[1], p.rd[0], p.rd[1]};
+      divc_group<4>(sd, hd, hr, p.fast_div & 1);
+    }
+    if (un) {
       const T lm = ldg(lam + idx);
       const T lpm = ldg(lam + idx) + (T)2 * ldg(mu + idx);
-      T dvxdx = div_c(dx_bm<T, N>(vx, idx, nz, c), dx, p.rd[0], p.fast_div & 1);
-      T dvzdz = div_c(dz_bm<T, N>(vz, idx, c), dz, p.rd[1], p.fast_div & 1);
+      T dvxdx = sd[0], dvzdz = sd[1];
       if (any_slab && ((fx & 1) || (fz & 1))) {
         if (xi >= 0) pml2(mx(p, 2, xi, j), cfx[CB * nx + i], cfx[CA * nx + i], cfx[CK * nx + i], dvxdx);
         if (zj >= 0) pml2(mz(p, 2, i, zj), cfz[CB * nz + j], cfz[CA * nz + j], cfz[CK * nz + j], dvzdz);
@@ -220,11 +272,9 @@ __device__ __forceinline__ void str2_cell(const P2<T>& p, int i, int j, int it, 
       sxx[idx] = sxx[idx] + (lpm * dvxdx + lm * dvzdz) * dt;
       szz[idx] = szz[idx] + (lpm * dvzdz + lm * dvxdx) * dt;
     }
-    // sxz at (i+1/2, j+1/2): :262-273
-    if (i >= N + 1 && i < nx - N && j >= N + 1 && j < nz - N) {
+    if (us) {
       const T m4 = (T)0.25 * (ldg(mu + idx + 1) + ldg(mu + idx) + ldg(mu + idx + nz + 1) + ldg(mu + idx + nz));
-      T dvzdx = div_c(dx_fm<T, N>(vz, idx, nz, c), dx, p.rd[0], p.fast_div & 1);
-      T dvxdz = div_c(dz_fm<T, N>(vx, idx, c), dz, p.rd[1], p.fast_div & 1);
+      T dvzdx = sd[2], dvxdz = sd[3];
       if (any_slab && ((fx & 2) || (fz & 2))) {
         if (xi >= 0) pml2(mx(p, 3, xi, j), cfx[CBH * nx + i], cfx[CAH * nx + i], cfx[CKH * nx + i], dvzdx);
         if (zj >= 0) pml2(mz(p, 3, i, zj), cfz[CBH * nz + j], cfz[CAH * nz + j], cfz[CKH * nz + j], dvxdz);

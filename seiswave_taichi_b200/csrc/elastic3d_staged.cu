@@ -153,20 +153,6 @@ __device__ __forceinline__ float4 divc4(float4 v, float d, float r, int fast) {
 // rounding, 53 >= 2*24+2), the same result div_c gives -- again without a
 // per-lane branch.  Keeping range tests off the per-lane path leaves the
 // group's independent lanes free to interleave.
-__device__ __forceinline__ bool mk_ok(float x) {
-  const unsigned u = __float_as_uint(x) & 0x7fffffffu;
-  return (u - 0x0D800000u < 0x64000000u) | (u == 0u);
-}
-__device__ __forceinline__ float dd_div(float x, float d) {
-  const float y = __double2float_rn(__ddiv_rn((double)x, (double)d));
-  return x == 0.f ? x : y;
-}
-__device__ __forceinline__ float mk_div(float x, float d, float r) {
-  const float q = __fmul_rn(x, r);
-  const float e = __fmaf_rn(-q, d, x);
-  const float y = __fmaf_rn(e, r, q);
-  return x == 0.f ? x : y;
-}
 template <int K>
 __device__ __forceinline__ void div_group(float4 (&v)[K], const float (&d)[K], const float (&r)[K], int fast) {
   bool ok = fast != 0;

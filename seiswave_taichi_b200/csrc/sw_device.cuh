@@ -151,6 +151,67 @@ __device__ __forceinline__ float div_c(float x, float d, float r, int fast) {
 }
 __device__ __forceinline__ double div_c(double x, double d, double, int) { return div_v(x, d); }
 
+// ---- groups of exact quotients without a per-lane range branch -------------
+// mk_ok: x is zero or of magnitude in [2^-100, 2^100), where div_c's
+// Markstein correction and IEEE division are used; mk_div: that correction
+// with zeros passed through (the sign of zero kept); dd_div: the quotient
+// divided in double precision and rounded once, correctly rounded for every
+// finite float x and positive float d (innocuous double rounding).  A group
+// tests all its lanes once and then runs one branch-free block, so the
+// independent lanes can interleave; every lane gets the bits div_c / div_v
+// would give it.
+__device__ __forceinline__ bool mk_ok(float x) {
+  const unsigned u = __float_as_uint(x) & 0x7fffffffu;
+  return (u - 0x0D800000u < 0x64000000u) | (u == 0u);
+}
+__device__ __forceinline__ float dd_div(float x, float d) {
+  const float y = __double2float_rn(__ddiv_rn((double)x, (double)d));
+  return x == 0.f ? x : y;
+}
+__device__ __forceinline__ float mk_div(float x, float d, float r) {
+  const float q = __fmul_rn(x, r);
+  const float e = __fmaf_rn(-q, d, x);
+  const float y = __fmaf_rn(e, r, q);
+  return x == 0.f ? x : y;
+}
+template <int K>
+__device__ __forceinline__ void divc_group(float (&x)[K], const float (&d)[K], const float (&r)[K], int fast) {
+  bool ok = fast != 0;
+#pragma unroll
+  for (int k = 0; k < K; ++k) ok = ok & mk_ok(x[k]);
+  if (ok) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) x[k] = mk_div(x[k], d[k], r[k]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < K; ++k) x[k] = dd_div(x[k], d[k]);
+  }
+}
+template <int K>
+__device__ __forceinline__ void divc_group(double (&x)[K], const double (&d)[K], const double (&r)[K], int fast) {
+#pragma unroll
+  for (int k = 0; k < K; ++k) x[k] = div_c(x[k], d[k], r[k], fast);
+}
+// quotients by per-cell positive divisors (densities), grouped likewise
+template <int K>
+__device__ __forceinline__ void divv_group(float (&x)[K], const float (&d)[K]) {
+  bool ok = true;
+#pragma unroll
+  for (int k = 0; k < K; ++k) ok = ok & mk_ok(x[k]);
+  if (ok) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) x[k] = x[k] == 0.f ? x[k] : __fdiv_rn(x[k], d[k]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < K; ++k) x[k] = dd_div(x[k], d[k]);
+  }
+}
+template <int K>
+__device__ __forceinline__ void divv_group(double (&x)[K], const double (&d)[K]) {
+#pragma unroll
+  for (int k = 0; k < K; ++k) x[k] = div_v(x[k], d[k]);
+}
+
 // receiver sample in the trace's element type
 template <typename T>
 __device__ __forceinline__ void store_rec(void* data, int f64, long long at, T v) {
