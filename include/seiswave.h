@@ -310,6 +310,27 @@ SW_API int sw2d_record(sw_plan* plan, int32_t it0, int32_t nsteps, void* snap, v
 SW_API int sw2d_adjoint_run(sw_plan* plan, const sw2d_adjoint_desc* adj, int32_t it0, int32_t nsteps,
                             const void* snap, void* stream);
 
+/* ---- 3D adjoint (no reference counterpart) --------------------------------
+ * The same for the SW3D_CPML_TENSOR scheme (Elastic3D_SSG_Tensor.py:166-345),
+ * orders 1..4: sw3d_record runs forward steps it0..it0+nsteps-1 with the
+ * exact register-queue kernels and stores nsteps+1 snapshots of
+ * sw3d_snapshot_elems() elements; sw3d_adjoint_run steps the adjoint state
+ * back over them. */
+typedef struct sw3d_adjoint_desc {
+  void* field[9];            /* adjoint of vx vy vz sxx syy szz sxy sxz syz    */
+  void* mem[3];              /* adjoint memory variables, layout of sw3d_desc.mem */
+  void* tmp[9];              /* scratch, (nx, ny, nz) each                      */
+  void* grad[8];             /* per-cell sums, added to: G_vx (coefficient dt/rho
+                                of vx), G_vy (dt/rho_y), G_vz (dt/rho_4), G_lpm,
+                                G_lhx (normal stresses), G_xy, G_xz, G_yz (the
+                                shear stresses' averaged mu)                    */
+  const void* residual;      /* (nt_max, nrec): d misfit / d data              */
+} sw3d_adjoint_desc;
+SW_API int sw3d_snapshot_elems(sw_plan* plan, int64_t* elems);
+SW_API int sw3d_record(sw_plan* plan, int32_t it0, int32_t nsteps, void* snap, void* stream);
+SW_API int sw3d_adjoint_run(sw_plan* plan, const sw3d_adjoint_desc* adj, int32_t it0, int32_t nsteps,
+                            const void* snap, void* stream);
+
 /* Scan every wavefield for NaN/Inf; blocks on the stream.  *nonfinite is set
  * to the number of non-finite values found (0 when the state is finite);
  * returns SW_ERR_NONFINITE when it is non-zero. */

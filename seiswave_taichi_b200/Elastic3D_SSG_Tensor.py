@@ -53,3 +53,11 @@ class ElasticWAVE(Elastic3DBase):
     def update_SSG(self, nt: int):
         """One time step (Elastic3D_SSG_Tensor.py:166-345)."""
         self._step(nt)
+
+    def forward_op(self, vp, vs, rho, checkpoint_every: int = 100):
+        """Differentiable seismogram: the (nt, nrec) traces as a function of
+        the vp, vs, rho tensors (device, the solver's dtype), with the
+        hand-written 3D adjoint as backward (no reference counterpart;
+        exact numerics, orders 1..4)."""
+        from .adjoint import ForwardOp3D
+        return ForwardOp3D.apply(vp, vs, rho, self, int(checkpoint_every))

@@ -33,7 +33,7 @@ EXPORTS = (
     "sw_plan_set_exact", "sw_count_nonfinite_noalloc", "sw2d_snapshot_elems", "sw2d_record",
     "sw2d_adjoint_run", "sw2d_batch_create", "sw_batch_set_tile", "sw_batch_info", "sw_batch_run",
     "sw_batch_destroy", "sw2d_abc_correct", "sw2d_abc_features", "sw_mlp_grad", "sw_mlp_forward",
-    "sw_mlp_backward", "sw2d_abc_adjoint",
+    "sw_mlp_backward", "sw2d_abc_adjoint", "sw3d_snapshot_elems", "sw3d_record", "sw3d_adjoint_run",
 )
 
 SW_ABC_DEPTH = 6
@@ -47,6 +47,11 @@ class AbcDesc(C.Structure):
     _fields_ = [("ncell", C.c_int32), ("cell", C.c_void_p), ("face", C.c_void_p), ("depth", C.c_void_p),
                 ("params", C.c_void_p), ("scale", C.c_float * 5), ("oscale", C.c_float * 5),
                 ("delta", C.c_void_p)]
+
+
+class Adjoint3D(C.Structure):
+    _fields_ = [("field", C.c_void_p * 9), ("mem", C.c_void_p * 3), ("tmp", C.c_void_p * 9),
+                ("grad", C.c_void_p * 8), ("residual", C.c_void_p)]
 
 
 class Adjoint2D(C.Structure):
@@ -152,6 +157,9 @@ def load() -> C.CDLL:
         "sw_mlp_forward": (C.c_int, [vp, vp, C.c_int64, vp, vp]),
         "sw_mlp_backward": (C.c_int, [vp, vp, vp, C.c_int64, vp, vp]),
         "sw2d_abc_adjoint": (C.c_int, [vp, C.POINTER(AbcDesc), vp, C.POINTER(vp), vp, vp]),
+        "sw3d_snapshot_elems": (C.c_int, [vp, C.POINTER(C.c_int64)]),
+        "sw3d_record": (C.c_int, [vp, C.c_int32, C.c_int32, vp, vp]),
+        "sw3d_adjoint_run": (C.c_int, [vp, C.POINTER(Adjoint3D), C.c_int32, C.c_int32, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -149,3 +149,128 @@ class ForwardOp2D(torch.autograd.Function):
         g_vs = g_mu * 2 * rho * vs - g_lam * 4 * rho * vs
         g_rh = g_rho + g_mu * vs * vs + g_lam * (vp * vp - 2 * vs * vs)
         return g_vp.to(vp.dtype), g_vs.to(vs.dtype), g_rh.to(rho.dtype), None, None
+
+
+# ---- 3D (CPML moment-tensor scheme) ---------------------------------------------
+F3 = ("vx", "vy", "vz", "sxx", "syy", "szz", "sxy", "sxz", "syz")
+
+
+class Adjoint3D:
+    """Checkpointed forward + adjoint driver for one 3D moment-tensor
+    solver (Elastic3D_SSG_Tensor, exact numerics, orders 1..4)."""
+
+    def __init__(self, wave, checkpoint_every: int = 100):
+        if not getattr(wave, "exact", True):
+            raise ValueError("the 3D adjoint transposes the exact step: build the solver with exact=True")
+        self.w = wave
+        self.K = int(checkpoint_every)
+        if self.K < 1:
+            raise ValueError("checkpoint_every must be >= 1")
+        self.plan = wave._plan or wave._build_plan()
+        n = C.c_int64(0)
+        N.check(N.load().sw3d_snapshot_elems(self.plan.handle, C.byref(n)))
+        self.snap_elems = int(n.value)
+        self.checkpoints = []
+
+    def _state(self):
+        w = self.w
+        return [getattr(w, f) for f in F3] + [m for m in w._mem if m is not None]
+
+    def forward(self, nt: int | None = None) -> torch.Tensor:
+        w = self.w
+        nt = w.nt if nt is None else int(nt)
+        self.nt = nt
+        w.reset()
+        st = w._stream()
+        self.checkpoints = []
+        for it0 in range(0, nt, self.K):
+            n = min(self.K, nt - it0)
+            self.checkpoints.append((it0, n, [t.clone() for t in self._state()]))
+            self.plan.run(it0, n, False, st)
+        return w.data[:nt].clone()
+
+    def backward(self, residual: torch.Tensor):
+        w = self.w
+        dev, dt_ = w.rho.device, w.rho.dtype
+        shape = w.gridsize
+        res = torch.zeros(w.data.shape, dtype=dt_, device=dev)
+        res[: residual.shape[0]] = residual.to(dt_)
+        z = lambda: torch.zeros(shape, dtype=dt_, device=dev)
+        adj_f = [z() for _ in range(9)]
+        adj_m = [torch.zeros_like(m) if m is not None else None for m in w._mem]
+        tmp = [z() for _ in range(9)]
+        grad = [z() for _ in range(8)]
+        snap = torch.empty((self.K + 1) * self.snap_elems, dtype=dt_, device=dev)
+        d = N.Adjoint3D()
+        for q in range(9):
+            d.field[q] = adj_f[q].data_ptr()
+            d.tmp[q] = tmp[q].data_ptr()
+        for q in range(8):
+            d.grad[q] = grad[q].data_ptr()
+        for q in range(3):
+            d.mem[q] = adj_m[q].data_ptr() if adj_m[q] is not None else None
+        d.residual = res.data_ptr()
+        st = w._stream()
+        lib = N.load()
+        for it0, n, saved in reversed(self.checkpoints):
+            for dst, src in zip(self._state(), saved):
+                dst.copy_(src)
+            N.check(lib.sw3d_record(self.plan.handle, it0, n, C.c_void_p(snap.data_ptr()), C.c_void_p(st)))
+            N.check(lib.sw3d_adjoint_run(self.plan.handle, C.byref(d), it0, n, C.c_void_p(snap.data_ptr()),
+                                         C.c_void_p(st)))
+        return coefficient_chain3(w.rho, grad)
+
+
+def coefficient_chain3(rho, grad):
+    """(g_rho, g_lam, g_mu) from the 3D per-cell coefficient sums
+    (Elastic3D_SSG_Tensor.py's averages: vx unaveraged rho, vy the y pair,
+    vz the x-y quad; normal stresses lam/mu over i, i+1; mu_xy = (mu[j+1] +
+    2 mu + mu[i+1])/4, mu_xz = (2 mu + mu[i+1] + mu[j+1])/4,
+    mu_yz = (mu[j+1] + 2 mu + mu[k+1])/4)."""
+    g0, g1, g2, g3, g4, g5, g6, g7 = grad
+    g_rho = (-g0 / (rho * rho)).clone()
+    ry = 0.5 * (rho[:, :-1] + rho[:, 1:])
+    q = 0.5 * (-g1[:, :-1] / (ry * ry))
+    g_rho[:, :-1] += q
+    g_rho[:, 1:] += q
+    r4 = 0.25 * (rho[:-1, :-1] + rho[:-1, 1:] + rho[1:, 1:] + rho[1:, :-1])
+    q = 0.25 * (-g2[:-1, :-1] / (r4 * r4))
+    g_rho[:-1, :-1] += q
+    g_rho[:-1, 1:] += q
+    g_rho[1:, 1:] += q
+    g_rho[1:, :-1] += q
+    g_lam = torch.zeros_like(rho)
+    g_mu = torch.zeros_like(rho)
+    hl = 0.5 * (g4 + g3)[:-1]
+    g_lam[:-1] += hl
+    g_lam[1:] += hl
+    g_mu[:-1] += g3[:-1]
+    g_mu[1:] += g3[:-1]
+    g_mu += 0.5 * (g5 + g6 + g7)
+    g_mu[:, 1:] += 0.25 * (g5 + g6 + g7)[:, :-1]
+    g_mu[1:] += 0.25 * (g5 + g6)[:-1]
+    g_mu[:, :, 1:] += 0.25 * g7[:, :, :-1]
+    return g_rho, g_lam, g_mu
+
+
+class ForwardOp3D(torch.autograd.Function):
+    """3D traces = F(vp, vs, rho) through the B200 kernels, with the 3D
+    adjoint as its backward."""
+
+    @staticmethod
+    def forward(ctx, vp, vs, rho, wave, checkpoint_every):
+        wave.set_model(vp.detach(), vs.detach(), rho.detach())
+        drv = Adjoint3D(wave, checkpoint_every)
+        out = drv.forward()
+        ctx.drv = drv
+        ctx.save_for_backward(vp.detach(), vs.detach(), rho.detach())
+        return out
+
+    @staticmethod
+    def backward(ctx, grad_out):
+        vp, vs, rho = ctx.saved_tensors
+        g_rho, g_lam, g_mu = ctx.drv.backward(grad_out.contiguous())
+        g_vp = g_lam * 2 * rho * vp
+        g_vs = g_mu * 2 * rho * vs - g_lam * 4 * rho * vs
+        g_rh = g_rho + g_mu * vs * vs + g_lam * (vp * vp - 2 * vs * vs)
+        return g_vp.to(vp.dtype), g_vs.to(vs.dtype), g_rh.to(rho.dtype), None, None

@@ -41,6 +41,17 @@ struct A2 {
   const T* snap1;
 };
 template <typename T> cudaError_t sw2_adjoint_step(const P2<T>&, const A2<T>&, int, int, cudaStream_t);
+template <typename T>
+struct A3 {
+  T* f[9];
+  T* mem[3];
+  T* tmp[9];
+  T* grad[8];
+  const T* res;
+  const T* snap0;
+  const T* snap1;
+};
+template <typename T> cudaError_t sw3_adjoint_step(const P3<T>&, const A3<T>&, int, int, cudaStream_t);
 struct AbcArgs {
   const int* cell;
   const int8_t* face;
@@ -877,9 +888,116 @@ cudaError_t adjoint2(sw_plan* pl, const sw::P2<T>& p, const sw2d_adjoint_desc* d
   return cudaSuccess;
 }
 
+int adjoint3_plan_ok(sw_plan* pl, const char* who) {
+  if (!pl) return fail(SW_ERR_ARG, std::string(who) + ": null plan");
+  if (pl->dim != 3 || pl->scheme != SW3D_CPML_TENSOR)
+    return fail(SW_ERR_UNSUPPORTED, std::string(who) + ": the 3D adjoint covers the CPML moment-tensor scheme");
+  if (pl->order > 4) return fail(SW_ERR_UNSUPPORTED, std::string(who) + ": the 3D adjoint covers orders 1..4");
+  return SW_OK;
+}
+
+template <typename T>
+long long snap3_elems(const sw::P3<T>& p) {
+  return 9LL * p.nx * p.ny * p.nz + 6 * (p.mcomp[0] + p.mcomp[1] + p.mcomp[2]);
+}
+
+template <typename T>
+cudaError_t snap3_store(const sw::P3<T>& p, T* slot, cudaStream_t st) {
+  const long long nc = (long long)p.nx * p.ny * p.nz;
+  cudaError_t e = cudaSuccess;
+  for (int q = 0; q < 9 && e == cudaSuccess; ++q)
+    e = cudaMemcpyAsync(slot + q * nc, p.f[q], nc * sizeof(T), cudaMemcpyDeviceToDevice, st);
+  long long off = 9 * nc;
+  for (int a = 0; a < 3 && e == cudaSuccess; ++a) {
+    if (p.mcomp[a] > 0)
+      e = cudaMemcpyAsync(slot + off, p.mem[a], 6 * p.mcomp[a] * sizeof(T), cudaMemcpyDeviceToDevice, st);
+    off += 6 * p.mcomp[a];
+  }
+  return e;
+}
+
+template <typename T>
+cudaError_t record3(sw_plan* pl, const sw::P3<T>& p, int it0, int n, T* snap, cudaStream_t st) {
+  const long long se = snap3_elems(p);
+  sw::P3<T> q = p;
+  if (!pl->gather_in_stress) q.nrec = 0;
+  for (int k = 0; k < n; ++k) {
+    const int it = it0 + k;
+    cudaError_t e = sw::sw3_moment_inject<T>(p, it, st);
+    if (e == cudaSuccess) e = snap3_store(p, snap + k * se, st);
+    if (e == cudaSuccess) e = sw::sw3_velocity<T>(q, pl->order, it, true, false, st);
+    if (e == cudaSuccess) e = sw::sw3_stress<T>(q, pl->order, it, false, st);
+    if (e == cudaSuccess && !pl->gather_in_stress) e = sw::sw3_gather<T>(p, it, st);
+    if (e != cudaSuccess) return e;
+  }
+  return snap3_store(p, snap + (long long)n * se, st);
+}
+
+template <typename T>
+cudaError_t adjoint3(sw_plan* pl, const sw::P3<T>& p, const sw3d_adjoint_desc* d, int it0, int n, const T* snap,
+                     cudaStream_t st) {
+  sw::A3<T> a{};
+  for (int q = 0; q < 9; ++q) a.f[q] = (T*)d->field[q];
+  for (int q = 0; q < 3; ++q) a.mem[q] = (T*)d->mem[q];
+  for (int q = 0; q < 9; ++q) a.tmp[q] = (T*)d->tmp[q];
+  for (int q = 0; q < 8; ++q) a.grad[q] = (T*)d->grad[q];
+  a.res = (const T*)d->residual;
+  const long long se = snap3_elems(p);
+  for (int k = n - 1; k >= 0; --k) {
+    a.snap0 = snap + k * se;
+    a.snap1 = snap + (k + 1) * se;
+    cudaError_t e = sw::sw3_adjoint_step<T>(p, a, pl->order, it0 + k, st);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
 }  // namespace
 
 extern "C" {
+
+int sw3d_snapshot_elems(sw_plan* pl, int64_t* elems) {
+  int rc = adjoint3_plan_ok(pl, "sw3d_snapshot_elems");
+  if (rc != SW_OK) return rc;
+  if (!elems) return fail(SW_ERR_ARG, "sw3d_snapshot_elems: null output");
+  *elems = pl->dtype == SW_F32 ? snap3_elems(pl->p3f) : snap3_elems(pl->p3d);
+  return SW_OK;
+}
+
+int sw3d_record(sw_plan* pl, int32_t it0, int32_t nsteps, void* snap, void* stream) {
+  int rc = adjoint3_plan_ok(pl, "sw3d_record");
+  if (rc != SW_OK) return rc;
+  if ((rc = check_it(pl, it0, nsteps)) != SW_OK) return rc;
+  if (!snap || !aligned(snap, dsize(pl->dtype))) return fail(SW_ERR_ARG, "sw3d_record: snapshot buffer");
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e = pl->dtype == SW_F32 ? record3<float>(pl, pl->p3f, it0, nsteps, (float*)snap, st)
+                                      : record3<double>(pl, pl->p3d, it0, nsteps, (double*)snap, st);
+  return e == cudaSuccess ? SW_OK : cuda_fail(e, "sw3d_record");
+}
+
+int sw3d_adjoint_run(sw_plan* pl, const sw3d_adjoint_desc* d, int32_t it0, int32_t nsteps, const void* snap,
+                     void* stream) {
+  int rc = adjoint3_plan_ok(pl, "sw3d_adjoint_run");
+  if (rc != SW_OK) return rc;
+  if ((rc = check_it(pl, it0, nsteps)) != SW_OK) return rc;
+  const int esz = dsize(pl->dtype);
+  if (!d || !snap || !aligned(snap, esz)) return fail(SW_ERR_ARG, "sw3d_adjoint_run: descriptor or snapshots");
+  for (int q = 0; q < 9; ++q)
+    if (!d->field[q] || !aligned(d->field[q], esz) || !d->tmp[q] || !aligned(d->tmp[q], esz))
+      return fail(SW_ERR_ARG, "sw3d_adjoint_run: adjoint field or scratch pointer");
+  for (int q = 0; q < 8; ++q)
+    if (!d->grad[q] || !aligned(d->grad[q], esz)) return fail(SW_ERR_ARG, "sw3d_adjoint_run: gradient pointer");
+  for (int a = 0; a < 3; ++a) {
+    const long long mc = pl->dtype == SW_F32 ? pl->p3f.mcomp[a] : pl->p3d.mcomp[a];
+    if (mc > 0 && !d->mem[a]) return fail(SW_ERR_ARG, "sw3d_adjoint_run: adjoint memory variables missing");
+  }
+  const int nrec = pl->dtype == SW_F32 ? pl->p3f.nrec : pl->p3d.nrec;
+  if (nrec > 0 && !d->residual) return fail(SW_ERR_ARG, "sw3d_adjoint_run: residual missing");
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e = pl->dtype == SW_F32 ? adjoint3<float>(pl, pl->p3f, d, it0, nsteps, (const float*)snap, st)
+                                      : adjoint3<double>(pl, pl->p3d, d, it0, nsteps, (const double*)snap, st);
+  return e == cudaSuccess ? SW_OK : cuda_fail(e, "sw3d_adjoint_run");
+}
 
 int sw2d_snapshot_elems(sw_plan* pl, int64_t* elems) {
   int rc = adjoint_plan_ok(pl, "sw2d_snapshot_elems");
