@@ -281,6 +281,34 @@ SW_API int sw_mlp_backward(const float* params, const float* x, const float* dy,
 SW_API int sw2d_abc_adjoint(sw_plan* plan, const sw_abc_desc* abc, const float* fields, float* const* adj,
                             float* ybar, void* stream);
 
+/* 3D layer: the same on the six faces of a SW3D_CPML_TENSOR solver; inputs
+ * are the nine fields / scale at the cell and its two neighbours along the
+ * face's inward normal plus the depth one-hot; nine outputs. */
+#define SW_ABC3_INPUTS (27 + SW_ABC_DEPTH)
+#define SW_ABC3_PARAMS (SW_ABC_HIDDEN * SW_ABC3_INPUTS + SW_ABC_HIDDEN + SW_ABC_HIDDEN * SW_ABC_HIDDEN + \
+                        SW_ABC_HIDDEN + 9 * SW_ABC_HIDDEN + 9)
+typedef struct sw_abc3_desc {
+  int32_t ncell;
+  const int32_t* cell;       /* device, linear index (i*ny + j)*nz + k          */
+  const int8_t* face;        /* device, face 0..5 (x-low, x-high, y-low, ...)   */
+  const int8_t* depth;       /* device, distance to the face 0..DEPTH-1         */
+  const float* params;       /* device, 6 x SW_ABC3_PARAMS                      */
+  float scale[9];            /* input scales: vx vy vz sxx syy szz sxy sxz syz  */
+  float oscale[9];           /* output scales                                   */
+  float* delta;              /* device scratch, ncell x 9                       */
+} sw_abc3_desc;
+SW_API int sw3d_abc_correct(sw_plan* plan, const sw_abc3_desc* abc, void* stream);
+SW_API int sw3d_abc_features(sw_plan* plan, const sw_abc3_desc* abc, float* x, void* stream);
+/* fields: nine (nx, ny, nz) arrays packed back to back (a sw3d_record slot's
+ * first part); adj: the nine adjoint field arrays, updated in place. */
+SW_API int sw3d_abc_adjoint(sw_plan* plan, const sw_abc3_desc* abc, const float* fields, float* const* adj,
+                            float* ybar, void* stream);
+SW_API int sw3d_mlp_grad(const float* params, const float* x, const float* y, int64_t n, float* grad, float* loss,
+                         void* stream);
+SW_API int sw3d_mlp_forward(const float* params, const float* x, int64_t n, float* y, void* stream);
+SW_API int sw3d_mlp_backward(const float* params, const float* x, const float* dy, int64_t n, float* grad,
+                             void* stream);
+
 /* ---- 2D adjoint (no reference counterpart) --------------------------------
  * Hand-written discrete adjoint of the SW2D_SSG_VS time loop with a
  * SW_SRC_MOMENT (or no) source and vz receivers, for gradients of a seismogram

@@ -34,6 +34,8 @@ EXPORTS = (
     "sw2d_adjoint_run", "sw2d_batch_create", "sw_batch_set_tile", "sw_batch_info", "sw_batch_run",
     "sw_batch_destroy", "sw2d_abc_correct", "sw2d_abc_features", "sw_mlp_grad", "sw_mlp_forward",
     "sw_mlp_backward", "sw2d_abc_adjoint", "sw3d_snapshot_elems", "sw3d_record", "sw3d_adjoint_run",
+    "sw3d_abc_correct", "sw3d_abc_features", "sw3d_abc_adjoint", "sw3d_mlp_grad", "sw3d_mlp_forward",
+    "sw3d_mlp_backward",
 )
 
 SW_ABC_DEPTH = 6
@@ -42,10 +44,20 @@ SW_ABC_HIDDEN = 32
 SW_ABC_PARAMS = (SW_ABC_HIDDEN * SW_ABC_INPUTS + SW_ABC_HIDDEN + SW_ABC_HIDDEN * SW_ABC_HIDDEN + SW_ABC_HIDDEN
                  + 5 * SW_ABC_HIDDEN + 5)
 
+SW_ABC3_INPUTS = 27 + SW_ABC_DEPTH
+SW_ABC3_PARAMS = (SW_ABC_HIDDEN * SW_ABC3_INPUTS + SW_ABC_HIDDEN + SW_ABC_HIDDEN * SW_ABC_HIDDEN + SW_ABC_HIDDEN
+                  + 9 * SW_ABC_HIDDEN + 9)
+
 
 class AbcDesc(C.Structure):
     _fields_ = [("ncell", C.c_int32), ("cell", C.c_void_p), ("face", C.c_void_p), ("depth", C.c_void_p),
                 ("params", C.c_void_p), ("scale", C.c_float * 5), ("oscale", C.c_float * 5),
+                ("delta", C.c_void_p)]
+
+
+class Abc3Desc(C.Structure):
+    _fields_ = [("ncell", C.c_int32), ("cell", C.c_void_p), ("face", C.c_void_p), ("depth", C.c_void_p),
+                ("params", C.c_void_p), ("scale", C.c_float * 9), ("oscale", C.c_float * 9),
                 ("delta", C.c_void_p)]
 
 
@@ -160,6 +172,12 @@ def load() -> C.CDLL:
         "sw3d_snapshot_elems": (C.c_int, [vp, C.POINTER(C.c_int64)]),
         "sw3d_record": (C.c_int, [vp, C.c_int32, C.c_int32, vp, vp]),
         "sw3d_adjoint_run": (C.c_int, [vp, C.POINTER(Adjoint3D), C.c_int32, C.c_int32, vp, vp]),
+        "sw3d_abc_correct": (C.c_int, [vp, C.POINTER(Abc3Desc), vp]),
+        "sw3d_abc_features": (C.c_int, [vp, C.POINTER(Abc3Desc), vp, vp]),
+        "sw3d_abc_adjoint": (C.c_int, [vp, C.POINTER(Abc3Desc), vp, C.POINTER(vp), vp, vp]),
+        "sw3d_mlp_grad": (C.c_int, [vp, vp, vp, C.c_int64, vp, vp, vp]),
+        "sw3d_mlp_forward": (C.c_int, [vp, vp, C.c_int64, vp, vp]),
+        "sw3d_mlp_backward": (C.c_int, [vp, vp, vp, C.c_int64, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -70,6 +70,25 @@ cudaError_t abc_correct(const AbcArgs&, cudaStream_t);
 cudaError_t abc_features(const AbcArgs&, cudaStream_t);
 cudaError_t mlp_grad(const float*, const float*, const float*, long long, float*, float*, int, cudaStream_t);
 cudaError_t abc_adjoint(const AbcArgs&, float* const*, float*, cudaStream_t);
+struct AbcArgs3 {
+  const int* cell;
+  const int8_t* face;
+  const int8_t* depth;
+  int ncell;
+  int nx, ny, nz;
+  const float* f[9];
+  float* fw[9];
+  float scale[9];
+  float oscale[9];
+  const float* params;
+  float* delta;
+  float* x_out;
+};
+cudaError_t abc3_correct(const AbcArgs3&, cudaStream_t);
+cudaError_t abc3_features(const AbcArgs3&, cudaStream_t);
+cudaError_t abc3_adjoint(const AbcArgs3&, float* const*, float*, cudaStream_t);
+cudaError_t mlp3_grad(const float*, const float*, const float*, long long, float*, float*, int, cudaStream_t);
+cudaError_t mlp3_forward_batch(const float*, const float*, long long, float*, cudaStream_t);
 cudaError_t mlp_forward_batch(const float*, const float*, long long, float*, cudaStream_t);
 }  // namespace sw
 
@@ -1101,6 +1120,89 @@ int sw_mlp_grad(const float* params, const float* x, const float* y, int64_t n, 
   if (n < 0 || (n > 0 && (!params || !x || !y || !grad || !loss))) return fail(SW_ERR_ARG, "sw_mlp_grad: arguments");
   cudaError_t e = sw::mlp_grad(params, x, y, n, grad, loss, 0, (cudaStream_t)stream);
   return e == cudaSuccess ? SW_OK : cuda_fail(e, "sw_mlp_grad");
+}
+
+}  // extern "C"
+
+namespace {
+
+int abc3_args(sw_plan* pl, const sw_abc3_desc* d, const char* who, sw::AbcArgs3* a) {
+  if (!pl || !d) return fail(SW_ERR_ARG, std::string(who) + ": null plan or descriptor");
+  if (pl->dim != 3 || pl->dtype != SW_F32 || pl->scheme != SW3D_CPML_TENSOR)
+    return fail(SW_ERR_UNSUPPORTED, std::string(who) + ": the 3D learned layer runs on float32 moment-tensor plans");
+  if (d->ncell < 0 || (d->ncell > 0 && (!d->cell || !d->face || !d->depth || !d->params || !d->delta)))
+    return fail(SW_ERR_ARG, std::string(who) + ": layer tables, parameters or scratch missing");
+  for (int f = 0; f < 9; ++f)
+    if (!(d->scale[f] > 0.f) || !(d->oscale[f] >= 0.f))
+      return fail(SW_ERR_ARG, std::string(who) + ": field scales must be positive");
+  *a = sw::AbcArgs3{};
+  a->cell = d->cell; a->face = d->face; a->depth = d->depth; a->ncell = d->ncell;
+  a->nx = pl->p3f.nx; a->ny = pl->p3f.ny; a->nz = pl->p3f.nz;
+  for (int f = 0; f < 9; ++f) {
+    a->f[f] = pl->p3f.f[f];
+    a->fw[f] = pl->p3f.f[f];
+    a->scale[f] = d->scale[f];
+    a->oscale[f] = d->oscale[f];
+  }
+  a->params = d->params;
+  a->delta = d->delta;
+  return SW_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sw3d_abc_correct(sw_plan* pl, const sw_abc3_desc* d, void* stream) {
+  sw::AbcArgs3 a;
+  int rc = abc3_args(pl, d, "sw3d_abc_correct", &a);
+  if (rc != SW_OK) return rc;
+  cudaError_t e = sw::abc3_correct(a, (cudaStream_t)stream);
+  return e == cudaSuccess ? SW_OK : cuda_fail(e, "sw3d_abc_correct");
+}
+
+int sw3d_abc_features(sw_plan* pl, const sw_abc3_desc* d, float* x, void* stream) {
+  sw::AbcArgs3 a;
+  int rc = abc3_args(pl, d, "sw3d_abc_features", &a);
+  if (rc != SW_OK) return rc;
+  if (d->ncell > 0 && !x) return fail(SW_ERR_ARG, "sw3d_abc_features: null output");
+  a.x_out = x;
+  cudaError_t e = sw::abc3_features(a, (cudaStream_t)stream);
+  return e == cudaSuccess ? SW_OK : cuda_fail(e, "sw3d_abc_features");
+}
+
+int sw3d_abc_adjoint(sw_plan* pl, const sw_abc3_desc* d, const float* fields, float* const* adj, float* ybar,
+                     void* stream) {
+  sw::AbcArgs3 a;
+  int rc = abc3_args(pl, d, "sw3d_abc_adjoint", &a);
+  if (rc != SW_OK) return rc;
+  if (d->ncell > 0 && (!fields || !adj || !ybar)) return fail(SW_ERR_ARG, "sw3d_abc_adjoint: null argument");
+  const long long nc = (long long)a.nx * a.ny * a.nz;
+  for (int f = 0; f < 9; ++f) {
+    if (d->ncell > 0 && !adj[f]) return fail(SW_ERR_ARG, "sw3d_abc_adjoint: adjoint field missing");
+    a.f[f] = fields + f * nc;
+  }
+  cudaError_t e = sw::abc3_adjoint(a, adj, ybar, (cudaStream_t)stream);
+  return e == cudaSuccess ? SW_OK : cuda_fail(e, "sw3d_abc_adjoint");
+}
+
+int sw3d_mlp_grad(const float* params, const float* x, const float* y, int64_t n, float* grad, float* loss,
+                  void* stream) {
+  if (n < 0 || (n > 0 && (!params || !x || !y || !grad || !loss))) return fail(SW_ERR_ARG, "sw3d_mlp_grad: arguments");
+  cudaError_t e = sw::mlp3_grad(params, x, y, n, grad, loss, 0, (cudaStream_t)stream);
+  return e == cudaSuccess ? SW_OK : cuda_fail(e, "sw3d_mlp_grad");
+}
+
+int sw3d_mlp_forward(const float* params, const float* x, int64_t n, float* y, void* stream) {
+  if (n < 0 || (n > 0 && (!params || !x || !y))) return fail(SW_ERR_ARG, "sw3d_mlp_forward: arguments");
+  cudaError_t e = sw::mlp3_forward_batch(params, x, n, y, (cudaStream_t)stream);
+  return e == cudaSuccess ? SW_OK : cuda_fail(e, "sw3d_mlp_forward");
+}
+
+int sw3d_mlp_backward(const float* params, const float* x, const float* dy, int64_t n, float* grad, void* stream) {
+  if (n < 0 || (n > 0 && (!params || !x || !dy || !grad))) return fail(SW_ERR_ARG, "sw3d_mlp_backward: arguments");
+  cudaError_t e = sw::mlp3_grad(params, x, dy, n, grad, nullptr, 1, (cudaStream_t)stream);
+  return e == cudaSuccess ? SW_OK : cuda_fail(e, "sw3d_mlp_backward");
 }
 
 int sw_mlp_backward(const float* params, const float* x, const float* dy, int64_t n, float* grad, void* stream) {
