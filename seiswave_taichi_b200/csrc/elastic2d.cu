@@ -46,15 +46,16 @@ __device__ __forceinline__ void vel2_cell(const P2<T>& p, int i, int j, int it, 
     const bool uz = i >= N && i < nx - N - 1 && j >= N && j < nz - N - 1;
     const bool src = src_here && i == p.si && j == p.sk;
     // stencil sums of both components, divided by the spacings as one group
-    T sd[4] = {0, 0, 0, 0};
-    if (ux) {
-      sd[0] = dx_bm<T, N>(sxx, idx, nz, c);
-      sd[1] = dz_bm<T, N>(sxz, idx, c);
-    }
-    if (uz) {
-      sd[2] = dx_fm<T, N>(sxz, idx, nz, c);
-      sd[3] = dz_fm<T, N>(szz, idx, c);
-    }
+    const long long row = (long long)i * nz;
+    T t0[2 * N], t1[2 * N], t2[2 * N], t3[2 * N];
+    taps_x<T, N>(t0, sxx, i - N, j, nx, nz);      // Dx2bm sxx at vx
+    taps_z<T, N>(t1, sxz, row, j - N, nz);        // Dz2bm sxz at vx
+    taps_x<T, N>(t2, sxz, i - N + 1, j, nx, nz);  // Dx2fm sxz at vz
+    taps_z<T, N>(t3, szz, row, j - N + 1, nz);    // Dz2fm szz at vz
+    const long long i1 = (long long)min(i + 1, nx - 1) * nz, j1 = min(j + 1, nz - 1);
+    const T r00 = ldg(rho + idx), r01 = ldg(rho + row + j1), r11 = ldg(rho + i1 + j1), r10 = ldg(rho + i1 + j);
+    T sd[4] = {ux ? tapsum<T, N>(t0, c) : (T)0, ux ? tapsum<T, N>(t1, c) : (T)0,
+               uz ? tapsum<T, N>(t2, c) : (T)0, uz ? tapsum<T, N>(t3, c) : (T)0};
     {
       const T hd[4] = {dx, dz, dx, dz};
       const T hr[4] = {p.rd[0], p.rd[1], p.rd[0], p.rd[1]};
@@ -68,10 +69,10 @@ __device__ __forceinline__ void vel2_cell(const P2<T>& p, int i, int j, int it, 
         if (zj >= 0) pml2(mz(p, 0, i, zj), cfz[CB * nz + j], cfz[CA * nz + j], cfz[CK * nz + j], dsxzdz);
       }
       tq[0] = (dsxxdx + dsxzdz) * dt;
-      td[0] = ldg(rho + idx);
+      td[0] = r00;
     }
     if (uz) {
-      td[1] = (T)0.25 * (ldg(rho + idx) + ldg(rho + idx + 1) + ldg(rho + idx + nz + 1) + ldg(rho + idx + nz));
+      td[1] = (T)0.25 * (r00 + r01 + r11 + r10);
       T dsxzdx = sd[2], dszzdz = sd[3];
       if (any_slab && ((fx & 2) || (fz & 2))) {
         if (xi >= 0) pml2(mx(p, 1, xi, j), cfx[CBH * nx + i], cfx[CAH * nx + i], cfx[CKH * nx + i], dsxzdx);
@@ -96,15 +97,14 @@ __device__ __forceinline__ void vel2_cell(const P2<T>& p, int i, int j, int it, 
     const bool ux = i >= N && i < nx - N - 1 && j >= N + 1 && j < nz - N;
     const bool uz = i >= N + 1 && i < nx - N && j >= N && j < nz - N - 1;
     const bool src = src_here && i == p.si && j == p.sk;
-    T sd[4] = {0, 0, 0, 0};
-    if (ux) {
-      sd[0] = dx_fm<T, N>(sxx, idx, nz, c);
-      sd[1] = dz_bm<T, N>(sxz, idx, c);
-    }
-    if (uz) {
-      sd[2] = dx_bm<T, N>(sxz, idx, nz, c);
-      sd[3] = dz_fm<T, N>(szz, idx, c);
-    }
+    const long long row = (long long)i * nz;
+    T t0[2 * N], t1[2 * N], t2[2 * N], t3[2 * N];
+    taps_x<T, N>(t0, sxx, i - N + 1, j, nx, nz);  // Dx2fm sxx at vx
+    taps_z<T, N>(t1, sxz, row, j - N, nz);        // Dz2bm sxz at vx
+    taps_x<T, N>(t2, sxz, i - N, j, nx, nz);      // Dx2bm sxz at vz
+    taps_z<T, N>(t3, szz, row, j - N + 1, nz);    // Dz2fm szz at vz
+    T sd[4] = {ux ? tapsum<T, N>(t0, c) : (T)0, ux ? tapsum<T, N>(t1, c) : (T)0,
+               uz ? tapsum<T, N>(t2, c) : (T)0, uz ? tapsum<T, N>(t3, c) : (T)0};
     {
       const T hd[4] = {dx, dz, dx, dz};
       const T hr[4] = {p.rd[0], p.rd[1], p.rd[0], p.rd[1]};
@@ -210,15 +210,14 @@ __device__ __forceinline__ void str2_cell(const P2<T>& p, int i, int j, int it, 
     // sxx szz at (i+1/2, j) :172-186; sxz at (i, j+1/2) :188-199
     const bool un = i >= N && i < nx - N - 1 && j >= N + 1 && j < nz - N;
     const bool us = i >= N + 1 && i < nx - N && j >= N && j < nz - N - 1;
-    T sd[4] = {0, 0, 0, 0};
-    if (un) {
-      sd[0] = dx_fm<T, N>(vx, idx, nz, c);
-      sd[1] = dz_bm<T, N>(vz, idx, c);
-    }
-    if (us) {
-      sd[2] = dx_bm<T, N>(vz, idx, nz, c);
-      sd[3] = dz_fm<T, N>(vx, idx, c);
-    }
+    const long long row = (long long)i * nz;
+    T t0[2 * N], t1[2 * N], t2[2 * N], t3[2 * N];
+    taps_x<T, N>(t0, vx, i - N + 1, j, nx, nz);   // Dx2fm vx at sxx
+    taps_z<T, N>(t1, vz, row, j - N, nz);         // Dz2bm vz at sxx
+    taps_x<T, N>(t2, vz, i - N, j, nx, nz);       // Dx2bm vz at sxz
+    taps_z<T, N>(t3, vx, row, j - N + 1, nz);     // Dz2fm vx at sxz
+    T sd[4] = {un ? tapsum<T, N>(t0, c) : (T)0, un ? tapsum<T, N>(t1, c) : (T)0,
+               us ? tapsum<T, N>(t2, c) : (T)0, us ? tapsum<T, N>(t3, c) : (T)0};
     {
       const T hd[4] = {dx, dz, dx, dz};
       const T hr[4] = {p.rd[0], p.rd[1], p.rd[0], p.rd[1]};
@@ -249,13 +248,14 @@ __device__ __forceinline__ void str2_cell(const P2<T>& p, int i, int j, int it, 
     // sxx szz at (i, j) :247-260; sxz at (i+1/2, j+1/2) :262-273
     const bool un = i >= N + 1 && i < nx - N && j >= N + 1 && j < nz - N;
     const bool us = un;
-    T sd[4] = {0, 0, 0, 0};
-    if (un) {
-      sd[0] = dx_bm<T, N>(vx, idx, nz, c);
-      sd[1] = dz_bm<T, N>(vz, idx, c);
-      sd[2] = dx_fm<T, N>(vz, idx, nz, c);
-      sd[3] = dz_fm<T, N>(vx, idx, c);
-    }
+    const long long row = (long long)i * nz;
+    T t0[2 * N], t1[2 * N], t2[2 * N], t3[2 * N];
+    taps_x<T, N>(t0, vx, i - N, j, nx, nz);       // Dx2bm vx at sxx
+    taps_z<T, N>(t1, vz, row, j - N, nz);         // Dz2bm vz at sxx
+    taps_x<T, N>(t2, vz, i - N + 1, j, nx, nz);   // Dx2fm vz at sxz
+    taps_z<T, N>(t3, vx, row, j - N + 1, nz);     // Dz2fm vx at sxz
+    T sd[4] = {un ? tapsum<T, N>(t0, c) : (T)0, un ? tapsum<T, N>(t1, c) : (T)0,
+               un ? tapsum<T, N>(t2, c) : (T)0, un ? tapsum<T, N>(t3, c) : (T)0};
     {
       const T hd[4] = {dx, dz, dx, dz};
       const T hr[4] = {p.rd[0], p.rd[1], p.rd[0], p.rd[1]};
