@@ -347,13 +347,74 @@ def run_batch(args, rank, world, local):
     return 0
 
 
+def run_thin_layer(args, rank, world, local):
+    """Config 5's cost comparison on one GPU: forward runs of a 256^3
+    interior (seeded layered vp 2000-5000 m/s, dx = 10 m, dt = 0.8 ms,
+    moment-tensor 12 Hz Ricker2, 1500 steps) inside a 20-cell CPML (300^3
+    grid) and inside the 6-cell thin layer with its network corrections
+    (272^3 grid), shot after shot.  value: interior Gcell-updates/s of the
+    learned-layer runs; the line reports both shots/s and their ratio.  The
+    network's cost does not depend on its weights, so an untrained one is
+    timed."""
+    import torch
+    from seiswave_taichi_b200 import learned_abc3d as LA
+    from seiswave_taichi_b200.synthetic import layered
+    torch.cuda.set_device(local)
+    n, nt, pad20, pad6 = 256, int(os.environ.get("SEISWAVE_CONFIG5_STEPS", "1500")), 22, 8
+    vp, vs, rho = layered((n, n, n), 2000.0, 5000.0, nlayers=8, seed=rank, anomaly=0.05)
+    h, dt, f0 = 10.0, 8e-4, 12.0
+    out = {}
+    for tag, P, npml in (("cpml20", pad20, 20), ("learned6", pad6, 6)):
+        m = [np.pad(a, P, mode="edge") for a in (vp, vs, rho)]
+        c = m[0].shape[0] // 2
+        w = LA.solver3d(*m, h, dt, c, c, c, nt, npml=npml, freq=f0)
+        abc = LA.LearnedABC3D(scale=(1e-9,) * 3 + (1.0,) * 6, oscale=(1e-12,) * 9) if tag == "learned6" else None
+
+        def shot():
+            w.reset()
+            if abc is None:
+                w.run(nt)
+            else:
+                abc.run(w, nt)
+
+        for _ in range(max(1, args.warmup // 3)):
+            shot()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            shot()
+        e1.record()
+        torch.cuda.synchronize()
+        out[tag] = e0.elapsed_time(e1) / args.steps
+        del w
+    if rank == 0:
+        cells = n ** 3
+        line = {
+            "metric": "Gcell-updates/s", "value": cells * nt / (out["learned6"] * 1e-3) / 1e9,
+            "unit": "Gcell-updates/s (interior cells)", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": out["learned6"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"3d-thin-layer-vs-cpml20-{n}^3-nt{nt}", "interior": [n, n, n],
+                       "grids": {"cpml20": n + 2 * pad20, "learned6": n + 2 * pad6}, "time_steps": nt},
+            "shots_per_s": {"learned6": 1e3 / out["learned6"], "cpml20": 1e3 / out["cpml20"]},
+            "learned_over_cpml20": out["cpml20"] / out["learned6"],
+            "note": "shots run one after the other (no 3D shot batching); error gate measured on small grids "
+                    "in tests/test_learned_abc3d.py",
+            "gpu_launches": args.steps * (2 * nt + 2 * nt + 1),
+        }
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="config2", choices=["config2", "config1", "config3", "config4"])
+    ap.add_argument("--config", default="config2", choices=["config2", "config1", "config3", "config4", "config5"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the float64 error runs")
     args = ap.parse_args(argv)
@@ -367,6 +428,8 @@ def main(argv=None):
         return run_reference(args, rank, world)
     if args.config == "config4":
         return run_batch(args, rank, world, local)
+    if args.config == "config5":
+        return run_thin_layer(args, rank, world, local)
 
     import torch
     torch.cuda.set_device(local)

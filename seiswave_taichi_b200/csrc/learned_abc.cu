@@ -34,23 +34,131 @@ using Net3 = Net<SW_ABC3_INPUTS, 9>;
 static_assert(Net2::N == SW_ABC_PARAMS, "2D parameter block layout");
 static_assert(Net3::N == SW_ABC3_PARAMS, "3D parameter block layout");
 
+// The networks' tanh, from tanh(x) = 1 - 2 / (exp(2|x|) + 1) with the sign of
+// x put back, on the fast exponential and division intrinsics (absolute error
+// below 1e-6; 1 for |x| beyond the float exponential's range).  Training and
+// the correction use this one function, and the backward passes take
+// 1 - h^2 as its derivative.
+__device__ __forceinline__ float act(float s) {
+  const float e = __expf(2.f * fabsf(s));
+  return copysignf(1.f - __fdividef(2.f, e + 1.f), s);
+}
+
+// Every pre-activation is b_o followed by fused multiply-adds over k in
+// increasing order, so the generic form below and the transposed
+// shared-memory form of the correction kernels give identical bits.
 template <class NT>
 __device__ __forceinline__ void mlp_forward(const float* P, const float* x, float* h1, float* h2, float* y) {
   for (int o = 0; o < NT::NH; ++o) {
     float s = P[NT::B1 + o];
-    for (int k = 0; k < NT::NI; ++k) s += P[NT::W1 + o * NT::NI + k] * x[k];
-    h1[o] = tanhf(s);
+    for (int k = 0; k < NT::NI; ++k) s = fmaf(P[NT::W1 + o * NT::NI + k], x[k], s);
+    h1[o] = act(s);
   }
   for (int o = 0; o < NT::NH; ++o) {
     float s = P[NT::B2 + o];
-    for (int k = 0; k < NT::NH; ++k) s += P[NT::W2 + o * NT::NH + k] * h1[k];
-    h2[o] = tanhf(s);
+    for (int k = 0; k < NT::NH; ++k) s = fmaf(P[NT::W2 + o * NT::NH + k], h1[k], s);
+    h2[o] = act(s);
   }
   for (int o = 0; o < NT::NO; ++o) {
     float s = P[NT::B3 + o];
-    for (int k = 0; k < NT::NH; ++k) s += P[NT::W3 + o * NT::NH + k] * h2[k];
+    for (int k = 0; k < NT::NH; ++k) s = fmaf(P[NT::W3 + o * NT::NH + k], h2[k], s);
     y[o] = s;
   }
+}
+
+// Transposed block of one face in shared memory for the correction kernels:
+// W1t[NI][NH] b1[NH] W2t[NH][NH] b2[NH] W3t[NH][NOP] b3[NOP], NOP = NO
+// rounded up to 4 (zero padded), so a warp reads four consecutive outputs'
+// weights of one input with one 16-byte broadcast load.
+template <class NT>
+struct TNet {
+  static constexpr int NI = NT::NI, NH = NT::NH, NO = NT::NO, NOP = (NO + 3) & ~3;
+  static constexpr int W1 = 0, B1 = W1 + NI * NH, W2 = B1 + NH, B2 = W2 + NH * NH, W3 = B2 + NH,
+                       B3 = W3 + NH * NOP, N = B3 + NOP;
+  static_assert(N % 4 == 0 && NH % 4 == 0, "16-byte rows");
+  // parameter of the packed block behind transposed slot q, or -1 (padding)
+  __device__ static int src(int q) {
+    if (q < B1) { const int k = q / NH, o = q - k * NH; return NT::W1 + o * NI + k; }
+    if (q < W2) return NT::B1 + (q - B1);
+    if (q < B2) { const int r = q - W2, k = r / NH, o = r - k * NH; return NT::W2 + o * NH + k; }
+    if (q < W3) return NT::B2 + (q - B2);
+    if (q < B3) { const int r = q - W3, k = r / NOP, o = r - k * NOP; return o < NO ? NT::W3 + o * NH + k : -1; }
+    const int o = q - B3;
+    return o < NO ? NT::B3 + o : -1;
+  }
+};
+
+template <class NT>
+__device__ void tnet_load(float* T, const float* __restrict__ params, int nface) {
+  using TN = TNet<NT>;
+  for (int q = threadIdx.x; q < nface * TN::N; q += blockDim.x) {
+    const int f = q / TN::N, r = TN::src(q - f * TN::N);
+    T[q] = r < 0 ? 0.f : params[f * NT::N + r];
+  }
+}
+
+// bias block b[K] into s
+template <int K>
+__device__ __forceinline__ void tload(const float* __restrict__ b, float (&s)[K]) {
+#pragma unroll
+  for (int o = 0; o < K; o += 4) {
+    const float4 v = *reinterpret_cast<const float4*>(b + o);
+    s[o] = v.x; s[o + 1] = v.y; s[o + 2] = v.z; s[o + 3] = v.w;
+  }
+}
+
+// s += W^T col for a transposed W[nin][K]; col holds this thread's inputs at
+// stride CT (its own column of the block's buffer)
+template <int K, int NIN, int U, int CT>
+__device__ __forceinline__ void tdense(const float* __restrict__ W, const float* col, float (&s)[K]) {
+#pragma unroll U
+  for (int k = 0; k < NIN; ++k) {
+    const float xk = col[k * CT];
+#pragma unroll
+    for (int o = 0; o < K; o += 4) {
+      const float4 v = *reinterpret_cast<const float4*>(W + k * K + o);
+      s[o] = fmaf(v.x, xk, s[o]); s[o + 1] = fmaf(v.y, xk, s[o + 1]);
+      s[o + 2] = fmaf(v.z, xk, s[o + 2]); s[o + 3] = fmaf(v.w, xk, s[o + 3]);
+    }
+  }
+}
+
+// forward pass of one cell from the transposed block T; col holds the NI
+// inputs on entry and is reused for the hidden layers
+template <class NT, int CT>
+__device__ __forceinline__ void mlp_forward_t(const float* __restrict__ T, float* col, float* y) {
+  using TN = TNet<NT>;
+  float s[TN::NH];
+  tload(T + TN::B1, s);
+  tdense<TN::NH, TN::NI, 3, CT>(T + TN::W1, col, s);
+#pragma unroll
+  for (int o = 0; o < TN::NH; ++o) col[o * CT] = act(s[o]);
+  tload(T + TN::B2, s);
+  tdense<TN::NH, TN::NH, 4, CT>(T + TN::W2, col, s);
+#pragma unroll
+  for (int o = 0; o < TN::NH; ++o) col[o * CT] = act(s[o]);
+  float t[TN::NOP];
+  tload(T + TN::B3, t);
+  tdense<TN::NOP, TN::NH, 4, CT>(T + TN::W3, col, t);
+#pragma unroll
+  for (int o = 0; o < TN::NO; ++o) y[o] = t[o];
+}
+
+// correction-kernel blocks: the faces' transposed blocks, then one column of
+// max(NI, NH) floats per thread
+constexpr int CT2 = 256, CT3 = 384;
+template <class NT>
+constexpr size_t corr_smem(int nface, int ct) {
+  return sizeof(float) * ((size_t)nface * TNet<NT>::N + (size_t)ct * (NT::NI > NT::NH ? NT::NI : NT::NH));
+}
+
+// correction-kernel grid: the whole layer in a grid-stride loop over two
+// blocks per SM, so each block fills its transposed weights once
+static int corr_grid(int ncell, int threads) {
+  int dev = 0, nsm = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const long long need = ((long long)ncell + threads - 1) / threads;
+  return (int)std::max<long long>(1, std::min<long long>(need, 2LL * nsm));
 }
 
 // adjoint of the first pre-activation (g1) from the output adjoint ybar
@@ -117,17 +225,22 @@ __device__ __forceinline__ void abc_features(const AbcArgs& a, int c, float* x) 
 }
 
 // corrections of every layer cell from the current fields (no field written)
-__global__ void k_abc_delta(const AbcArgs a) {
-  __shared__ float P[4 * SW_ABC_PARAMS];
-  for (int q = threadIdx.x; q < 4 * SW_ABC_PARAMS; q += blockDim.x) P[q] = a.params[q];
+// dynamic shared memory: the four faces' transposed blocks
+__global__ void __launch_bounds__(CT2) k_abc_delta(const AbcArgs a) {
+  extern __shared__ float4 T2v[];
+  float* T = reinterpret_cast<float*>(T2v);
+  float* col = T + 4 * TNet<Net2>::N + threadIdx.x;
+  tnet_load<Net2>(T, a.params, 4);
   __syncthreads();
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= a.ncell) return;
-  float x[Net2::NI], h1[Net2::NH], h2[Net2::NH], y[Net2::NO];
-  abc_features(a, c, x);
-  mlp_forward<Net2>(P + a.face[c] * SW_ABC_PARAMS, x, h1, h2, y);
+  for (int c = blockIdx.x * CT2 + threadIdx.x; c < a.ncell; c += gridDim.x * CT2) {
+    float x[Net2::NI], y[Net2::NO];
+    abc_features(a, c, x);
 #pragma unroll
-  for (int f = 0; f < 5; ++f) a.delta[(long long)c * 5 + f] = y[f] * a.oscale[f];
+    for (int k = 0; k < Net2::NI; ++k) col[k * CT2] = x[k];
+    mlp_forward_t<Net2, CT2>(T + a.face[c] * TNet<Net2>::N, col, y);
+#pragma unroll
+    for (int f = 0; f < 5; ++f) a.delta[(long long)c * 5 + f] = y[f] * a.oscale[f];
+  }
 }
 
 __global__ void k_abc_apply(const AbcArgs a) {
@@ -206,9 +319,15 @@ cudaError_t abc_adjoint(const AbcArgs& a, float* const* lam_host, float* ybar, c
 
 cudaError_t abc_correct(const AbcArgs& a, cudaStream_t st) {
   if (a.ncell == 0) return cudaSuccess;
-  const int nb = (a.ncell + 127) / 128;
-  k_abc_delta<<<nb, 128, 0, st>>>(a);
-  k_abc_apply<<<nb, 128, 0, st>>>(a);
+  static bool init = false;
+  const int sm = (int)corr_smem<Net2>(4, CT2);
+  if (!init) {
+    cudaError_t e = cudaFuncSetAttribute(k_abc_delta, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e != cudaSuccess) return e;
+    init = true;
+  }
+  k_abc_delta<<<corr_grid(a.ncell, CT2), CT2, sm, st>>>(a);
+  k_abc_apply<<<(a.ncell + 127) / 128, 128, 0, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -267,17 +386,21 @@ __device__ __forceinline__ void abc3_features(const AbcArgs3& a, int c, float* x
 }
 
 // dynamic shared memory: the six faces' parameter blocks
-__global__ void k_abc3_delta(const AbcArgs3 a) {
-  extern __shared__ float P3s[];
-  for (int q = threadIdx.x; q < 6 * SW_ABC3_PARAMS; q += blockDim.x) P3s[q] = a.params[q];
+__global__ void __launch_bounds__(CT3) k_abc3_delta(const AbcArgs3 a) {
+  extern __shared__ float4 T3v[];
+  float* T = reinterpret_cast<float*>(T3v);
+  float* col = T + 6 * TNet<Net3>::N + threadIdx.x;
+  tnet_load<Net3>(T, a.params, 6);
   __syncthreads();
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= a.ncell) return;
-  float x[Net3::NI], h1[Net3::NH], h2[Net3::NH], y[Net3::NO];
-  abc3_features(a, c, x);
-  mlp_forward<Net3>(P3s + a.face[c] * SW_ABC3_PARAMS, x, h1, h2, y);
+  for (int c = blockIdx.x * CT3 + threadIdx.x; c < a.ncell; c += gridDim.x * CT3) {
+    float x[Net3::NI], y[Net3::NO];
+    abc3_features(a, c, x);
 #pragma unroll
-  for (int f = 0; f < 9; ++f) a.delta[(long long)c * 9 + f] = y[f] * a.oscale[f];
+    for (int k = 0; k < Net3::NI; ++k) col[k * CT3] = x[k];
+    mlp_forward_t<Net3, CT3>(T + a.face[c] * TNet<Net3>::N, col, y);
+#pragma unroll
+    for (int f = 0; f < 9; ++f) a.delta[(long long)c * 9 + f] = y[f] * a.oscale[f];
+  }
 }
 
 __global__ void k_abc3_apply(const AbcArgs3 a) {
@@ -330,13 +453,14 @@ __global__ void k_abc3_xbar(const AbcArgs3 a, const LamK<9> lam, const float* __
 }
 
 static size_t abc3_smem() { return sizeof(float) * 6 * SW_ABC3_PARAMS; }
+static size_t abc3_tsmem() { return corr_smem<Net3>(6, CT3); }
 
 static cudaError_t abc3_init() {
   static bool init = false;
   if (init) return cudaSuccess;
-  const int sm = (int)abc3_smem();
-  cudaError_t e = cudaFuncSetAttribute(k_abc3_delta, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_abc3_xbar, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  cudaError_t e = cudaFuncSetAttribute(k_abc3_delta, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)abc3_tsmem());
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_abc3_xbar, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)abc3_smem());
   if (e == cudaSuccess) init = true;
   return e;
 }
@@ -345,9 +469,8 @@ cudaError_t abc3_correct(const AbcArgs3& a, cudaStream_t st) {
   if (a.ncell == 0) return cudaSuccess;
   cudaError_t e = abc3_init();
   if (e != cudaSuccess) return e;
-  const int nb = (a.ncell + 127) / 128;
-  k_abc3_delta<<<nb, 128, abc3_smem(), st>>>(a);
-  k_abc3_apply<<<nb, 128, 0, st>>>(a);
+  k_abc3_delta<<<corr_grid(a.ncell, CT3), CT3, abc3_tsmem(), st>>>(a);
+  k_abc3_apply<<<(a.ncell + 127) / 128, 128, 0, st>>>(a);
   return cudaGetLastError();
 }
 
