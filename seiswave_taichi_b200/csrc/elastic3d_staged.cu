@@ -197,6 +197,99 @@ struct QuadPml {
   uint8_t fx, fy;
 };
 
+// Memory variables of one quad on the slabs it lies in, components
+// c0 .. c0+2 of each axis: x and y slab rows as float4, z slab per cell.
+// quad_mem_load issues every load before any update, so the latencies of the
+// up to nine rows overlap instead of forming one load-update-store chain per
+// component and axis; quad_mem_store writes them back after the updates.
+struct QuadMem {
+  float4 x[3], y[3];
+  float z[3][4];
+  int zk[4];
+};
+
+__device__ __forceinline__ float* memx_ptr(const P3<float>& p, const QuadPml& q, int comp) {
+  return p.mem[0] + comp * p.mcomp[0] + ((size_t)q.xi * p.ny + q.j) * p.nz + q.k;
+}
+__device__ __forceinline__ float* memy_ptr(const P3<float>& p, const QuadPml& q, int comp) {
+  return p.mem[1] + comp * p.mcomp[1] + ((size_t)q.i * p.sn[1] + q.yj) * p.nz + q.k;
+}
+__device__ __forceinline__ float* memz_ptr(const P3<float>& p, const QuadPml& q, int comp, int zk) {
+  return p.mem[2] + comp * p.mcomp[2] + ((size_t)q.i * p.ny + q.j) * p.sn[2] + zk;
+}
+
+__device__ __forceinline__ void quad_mem_load(const P3<float>& p, const QuadPml& q, int c0, QuadMem& m) {
+#pragma unroll
+  for (int e = 0; e < 4; ++e) m.zk[e] = q.k + e < p.nz ? slab_index(q.k + e, p.nz, p.lo[2], p.hi[2]) : -1;
+  if (q.xi >= 0) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) m.x[c] = ld4(memx_ptr(p, q, c0 + c));
+  }
+  if (q.yj >= 0) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) m.y[c] = ld4(memy_ptr(p, q, c0 + c));
+  }
+#pragma unroll
+  for (int e = 0; e < 4; ++e)
+    if (m.zk[e] >= 0) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) m.z[c][e] = *memz_ptr(p, q, c0 + c, m.zk[e]);
+    }
+}
+
+__device__ __forceinline__ void quad_mem_store(const P3<float>& p, const QuadPml& q, int c0, const QuadMem& m) {
+  if (q.xi >= 0) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) st4(memx_ptr(p, q, c0 + c), m.x[c]);
+  }
+  if (q.yj >= 0) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) st4(memy_ptr(p, q, c0 + c), m.y[c]);
+  }
+#pragma unroll
+  for (int e = 0; e < 4; ++e)
+    if (m.zk[e] >= 0) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) *memz_ptr(p, q, c0 + c, m.zk[e]) = m.z[c][e];
+    }
+}
+
+// CPML of one derivative quad d on axis AX from the preloaded memory
+// variables (component c of m), updated in place
+template <int AX, bool EX>
+__device__ __forceinline__ void pml_quad_m(const P3<float>& p, const QuadPml& q, int c, int half, const int* pm,
+                                           float4& d, QuadMem& m) {
+  const float* cf = p.cf[AX];
+  const int n = AX == 0 ? p.nx : AX == 1 ? p.ny : p.nz;
+  const int ob = half ? CBH : CB, oa = half ? CAH : CA, ok = half ? CKH : CK;
+  if (AX == 0 || AX == 1) {
+    const int si = AX == 0 ? q.xi : q.yj;
+    if (si < 0) return;
+    const int idx = AX == 0 ? q.i : q.j;
+    const float b = __ldg(cf + ob * n + idx), a = __ldg(cf + oa * n + idx), kk = __ldg(cf + ok * n + idx);
+    float4& o = AX == 0 ? m.x[c] : m.y[c];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      if (!pm[e]) continue;
+      const float de = g4(d, e);
+      const float psi = b * g4(o, e) + a * de;
+      s4(o, e, psi);
+      s4(d, e, dvv<EX>(de, kk) + psi);
+    }
+  } else {
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      if (!pm[e] || m.zk[e] < 0) continue;
+      const int kk_ = q.k + e;
+      const float b = __ldg(cf + ob * n + kk_), a = __ldg(cf + oa * n + kk_), kk = __ldg(cf + ok * n + kk_);
+      const float de = g4(d, e);
+      const float psi = b * m.z[c][e] + a * de;
+      m.z[c][e] = psi;
+      s4(d, e, dvv<EX>(de, kk) + psi);
+    }
+  }
+}
+
 template <int AX, bool EX>
 __device__ __forceinline__ void pml_quad(const P3<float>& p, const QuadPml& q, int comp, int half, const int* pm,
                                          float4& d) {
@@ -414,6 +507,8 @@ k3s_velocity(const __grid_constant__ P3<float> p, const __grid_constant__ Staged
         } else {
           QuadPml q{xi, yj, i, j, k, p.fl[0][i], fy};
           const bool anyslab = xi >= 0 || yj >= 0 || zslab;
+          QuadMem mm;
+          if (anyslab) quad_mem_load(p, q, 0, mm);
           // vx (x half, y int, z int): i in [N, nx-N-1), j in [N+1, ny-N), k in [N+1, nz-N)
           if (i < nx - N - 1 && j >= N + 1 && j < ny - N) {
             int pm[4], upd[4];
@@ -423,9 +518,9 @@ k3s_velocity(const __grid_constant__ P3<float> p, const __grid_constant__ Staged
               pm[e] = upd[e] && ((q.fx & 2) || (fy & 1) || (fz[e] & 1));
             }
             if (anyslab) {
-              pml_quad<0, EX>(p, q, 0, 1, pm, a1);
-              pml_quad<1, EX>(p, q, 0, 0, pm, a2);
-              pml_quad<2, EX>(p, q, 0, 0, pm, a3);
+              pml_quad_m<0, EX>(p, q, 0, 1, pm, a1, mm);
+              pml_quad_m<1, EX>(p, q, 0, 0, pm, a2, mm);
+              pml_quad_m<2, EX>(p, q, 0, 0, pm, a3, mm);
             }
 #pragma unroll
             for (int e = 0; e < 4; ++e)
@@ -443,9 +538,9 @@ k3s_velocity(const __grid_constant__ P3<float> p, const __grid_constant__ Staged
               pm[e] = upd[e] && ((q.fx & 1) || (fy & 2) || (fz[e] & 1));
             }
             if (anyslab) {
-              pml_quad<0, EX>(p, q, 1, 0, pm, b1);
-              pml_quad<1, EX>(p, q, 1, 1, pm, b2);
-              pml_quad<2, EX>(p, q, 1, 0, pm, b3);
+              pml_quad_m<0, EX>(p, q, 1, 0, pm, b1, mm);
+              pml_quad_m<1, EX>(p, q, 1, 1, pm, b2, mm);
+              pml_quad_m<2, EX>(p, q, 1, 0, pm, b3, mm);
             }
 #pragma unroll
             for (int e = 0; e < 4; ++e)
@@ -465,9 +560,9 @@ k3s_velocity(const __grid_constant__ P3<float> p, const __grid_constant__ Staged
               pm[e] = upd[e] && ((q.fx & 1) || (fy & 1) || (fz[e] & 2));
             }
             if (anyslab) {
-              pml_quad<0, EX>(p, q, 2, 0, pm, c1);
-              pml_quad<1, EX>(p, q, 2, 0, pm, c2);
-              pml_quad<2, EX>(p, q, 2, 1, pm, c3);
+              pml_quad_m<0, EX>(p, q, 2, 0, pm, c1, mm);
+              pml_quad_m<1, EX>(p, q, 2, 0, pm, c2, mm);
+              pml_quad_m<2, EX>(p, q, 2, 1, pm, c3, mm);
             }
 #pragma unroll
             for (int e = 0; e < 4; ++e)
@@ -479,6 +574,7 @@ k3s_velocity(const __grid_constant__ P3<float> p, const __grid_constant__ Staged
                 s4(vz, e, g4(vz, e) + dvv<EX>(t, r4));
               }
           }
+          if (anyslab) quad_mem_store(p, q, 0, mm);
           // point force (Elastic3D_SSG_CPML.py:245), after the update
           if (force_here && i == p.si && j == p.sj && p.sk >= k && p.sk < k + 4) {
             const int e = p.sk - k;
@@ -665,6 +761,8 @@ k3s_stress(const __grid_constant__ P3<float> p, const __grid_constant__ StagedMa
         } else {
           QuadPml q{xi, yj, i, j, k, p.fl[0][i], fy};
           const bool anyslab = xi >= 0 || yj >= 0 || zslab;
+          QuadMem mm;
+          if (anyslab) quad_mem_load(p, q, 3, mm);
           // normal stresses: i, j, k in [N+1, n-N)
           if (i >= N + 1 && j >= N + 1 && j < ny - N) {
             int pm[4], upd[4];
@@ -674,9 +772,9 @@ k3s_stress(const __grid_constant__ P3<float> p, const __grid_constant__ StagedMa
               pm[e] = upd[e] && ((q.fx | fy | fz[e]) & 1);
             }
             if (anyslab) {
-              pml_quad<0, EX>(p, q, 3, 0, pm, e1);
-              pml_quad<1, EX>(p, q, 3, 0, pm, e2);
-              pml_quad<2, EX>(p, q, 3, 0, pm, e3);
+              pml_quad_m<0, EX>(p, q, 0, 0, pm, e1, mm);
+              pml_quad_m<1, EX>(p, q, 0, 0, pm, e2, mm);
+              pml_quad_m<2, EX>(p, q, 0, 0, pm, e3, mm);
             }
 #pragma unroll
             for (int e = 0; e < 4; ++e)
@@ -699,8 +797,8 @@ k3s_stress(const __grid_constant__ P3<float> p, const __grid_constant__ StagedMa
               pm[e] = upd[e] && ((q.fx & 2) || (fy & 2) || (fz[e] & 1));
             }
             if (anyslab) {
-              pml_quad<0, EX>(p, q, 4, 1, pm, f1);
-              pml_quad<1, EX>(p, q, 4, 1, pm, f2);
+              pml_quad_m<0, EX>(p, q, 1, 1, pm, f1, mm);
+              pml_quad_m<1, EX>(p, q, 1, 1, pm, f2, mm);
             }
 #pragma unroll
             for (int e = 0; e < 4; ++e)
@@ -719,8 +817,8 @@ k3s_stress(const __grid_constant__ P3<float> p, const __grid_constant__ StagedMa
               pm[e] = upd[e] && ((q.fx & 2) || (fy & 1) || (fz[e] & 2));
             }
             if (anyslab) {
-              pml_quad<0, EX>(p, q, 5, 1, pm, h1);
-              pml_quad<2, EX>(p, q, 4, 1, pm, h2);
+              pml_quad_m<0, EX>(p, q, 2, 1, pm, h1, mm);
+              pml_quad_m<2, EX>(p, q, 1, 1, pm, h2, mm);
             }
 #pragma unroll
             for (int e = 0; e < 4; ++e)
@@ -739,8 +837,8 @@ k3s_stress(const __grid_constant__ P3<float> p, const __grid_constant__ StagedMa
               pm[e] = upd[e] && ((q.fx & 1) || (fy & 2) || (fz[e] & 2));
             }
             if (anyslab) {
-              pml_quad<1, EX>(p, q, 5, 1, pm, q1);
-              pml_quad<2, EX>(p, q, 5, 1, pm, q2);
+              pml_quad_m<1, EX>(p, q, 2, 1, pm, q1, mm);
+              pml_quad_m<2, EX>(p, q, 2, 1, pm, q2, mm);
             }
 #pragma unroll
             for (int e = 0; e < 4; ++e)
@@ -750,6 +848,7 @@ k3s_stress(const __grid_constant__ P3<float> p, const __grid_constant__ StagedMa
                 s4(syz, e, g4(syz, e) + m4 * (g4(q1, e) + g4(q2, e)) * dt);
               }
           }
+          if (anyslab) quad_mem_store(p, q, 3, mm);
           if (src) {
             // next step's moment-tensor source (Elastic3D_SSG_Tensor.py:186-193)
             const int e = p.sk - k;
