@@ -19,7 +19,8 @@ def _cases():
                    src_scale=1e5) for q, s in enumerate(SHAPES)]
 
 
-def test_fwi_step_equals_per_shot_autograd(cuda):
+@pytest.mark.parametrize("streams", [1, 3])
+def test_fwi_step_equals_per_shot_autograd(cuda, streams):
     from seiswave_taichi_b200.fwi import FWIStep
     cs = _cases()
     # observed data from perturbed models
@@ -28,7 +29,7 @@ def test_fwi_step_equals_per_shot_autograd(cuda):
         w = product2d(c)
         d_obs.append(w.forward_op(w.vp * 1.03, w.vs * 0.98, w.rho).detach())
     waves = [product2d(c) for c in cs]
-    step = FWIStep(waves, checkpoint_every=40, autotune=False)
+    step = FWIStep(waves, checkpoint_every=40, autotune=False, streams=streams)
     misfit, grads = step(d_obs)
     tot = 0.0
     for c, ob, (gvp, gvs, grh) in zip(cs, d_obs, grads):
@@ -38,7 +39,7 @@ def test_fwi_step_equals_per_shot_autograd(cuda):
         rh = w.rho.clone().requires_grad_(True)
         loss = 0.5 * ((w.forward_op(vp, vs, rh, checkpoint_every=40) - ob) ** 2).sum()
         loss.backward()
-        tot += float(loss)
+        tot += float(loss.detach())
         for a, b in ((gvp, vp.grad), (gvs, vs.grad), (grh, rh.grad)):
             np.testing.assert_allclose(a.cpu().numpy(), b.cpu().numpy(), rtol=1e-12, atol=1e-12 * float(b.abs().max()))
     assert misfit == pytest.approx(tot, rel=1e-12)
