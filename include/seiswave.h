@@ -165,13 +165,17 @@ SW_API int sw_plan_set_tile(sw_plan* plan, int32_t x_chunk);
 
 /* Block until the stream is idle and report a device-side failure recorded
  * by the plan's kernels since creation (SW_ERR_TIMEOUT: a bounded wait for
- * TMA data gave up).  No reference counterpart (the reference has no error
+ * TMA data, or a grid barrier of the 2D persistent run, gave up).  No reference counterpart (the reference has no error
  * path); it is the status read the drivers' loops can add after run(). */
 SW_API int sw_plan_status(sw_plan* plan, void* stream);
 
 /* Describe the plan's execution path: info[0] current path of sw_step/sw_run
- * (0 register-queue two-pass kernels, 1 TMA-staged two-pass kernels, 2 fused
- * single-pass kernel), [1] constant-divisor fast path verified, [2] staged
+ * (0 register-queue two-pass kernels, 2D: two launches per step, 1 TMA-staged
+ * two-pass kernels, 2 fused single-pass kernel, 3 2D persistent: sw_run is
+ * one cooperative launch for all its steps, the phases separated by a
+ * bounded grid barrier; opt-in, as the two launches per step replayed from
+ * a CUDA graph are faster on B200 at every grid size measured; sw_step
+ * keeps the two launches), [1] constant-divisor fast path verified, [2] staged
  * path available, [3] its grid, [4] its x-chunk length, [5] fused path set
  * up, [6] its grid, [7] its x-chunk length, [8] exact numerics (see
  * sw_plan_set_exact).  info must hold 9 int32. */

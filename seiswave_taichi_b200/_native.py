@@ -279,7 +279,7 @@ class Plan:
         """Synchronize and raise if a kernel recorded a device-side failure."""
         check(load().sw_plan_status(self._h, C.c_void_p(stream)))
 
-    PATHS = {"two_pass": 0, "staged": 1, "fused": 2}
+    PATHS = {"two_pass": 0, "staged": 1, "fused": 2, "persistent": 3}
 
     def info(self) -> dict:
         a = (C.c_int32 * 9)()

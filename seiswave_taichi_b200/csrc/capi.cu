@@ -28,6 +28,8 @@ template <typename T> cudaError_t sw3_spml_step(const P3<T>&, int, int, bool, cu
 template <typename T> cudaError_t sw2_step(const P2<T>&, int, int, int, T, bool, bool, bool, cudaStream_t);
 template <typename T> cudaError_t sw2_moment_inject(const P2<T>&, int, cudaStream_t);
 template <typename T>
+cudaError_t sw2_persistent(const P2<T>&, int, int, int, int, bool, bool, unsigned int*, int*, cudaStream_t);
+template <typename T>
 cudaError_t sw2b_step(const Batch2<T>&, int, int, int, int, int, bool, bool, cudaStream_t);
 void sw2b_tile_shape(int cfg, int* bx, int* bz);
 template <typename T>
@@ -143,8 +145,11 @@ struct sw_plan {
   sw::StagedMaps svm{}, ssm{};
   sw::StagedArgs sa{};
   int staged_grid = 0, staged_N = 0;
-  // 0: register-queue two-pass kernels, 1: staged two-pass, 2: fused single pass
+  // 0: register-queue two-pass kernels (2D: two launches per step), 1: staged
+  // two-pass, 2: fused single pass, 3: 2D persistent (one cooperative launch
+  // per run)
   int path = 0;
+  unsigned int* d_bar = nullptr;  // 2D persistent path: grid-barrier arrival and generation words
 };
 
 namespace {
@@ -555,6 +560,27 @@ cudaError_t enqueue_fused_run(sw_plan* pl, int it0, int nsteps, cudaStream_t st)
   return cudaSuccess;
 }
 
+// 2D persistent path: the barrier words and the error word on first use
+cudaError_t persistent_run2(sw_plan* pl, int it0, int nsteps, cudaStream_t st) {
+  if (!pl->d_bar) {
+    cudaError_t e = cudaMalloc(&pl->d_bar, 2 * sizeof(unsigned int));
+    if (e != cudaSuccess) return e;
+    e = cudaMemset(pl->d_bar, 0, 2 * sizeof(unsigned int));
+    if (e != cudaSuccess) return e;
+  }
+  if (!pl->d_err) {
+    cudaError_t e = cudaMalloc(&pl->d_err, sizeof(int));
+    if (e != cudaSuccess) return e;
+    e = cudaMemset(pl->d_err, 0, sizeof(int));
+    if (e != cudaSuccess) return e;
+  }
+  if (pl->dtype == SW_F32)
+    return sw::sw2_persistent<float>(pl->p2f, pl->scheme, pl->order, it0, nsteps, pl->gather_in_stress,
+                                     pl->gather_in_stress, pl->d_bar, pl->d_err, st);
+  return sw::sw2_persistent<double>(pl->p2d, pl->scheme, pl->order, it0, nsteps, pl->gather_in_stress,
+                                    pl->gather_in_stress, pl->d_bar, pl->d_err, st);
+}
+
 cudaError_t enqueue_sequence(sw_plan* pl, int it0, int nsteps, cudaStream_t st) {
   if (pl->fused && pl->path == 2 && nsteps >= 2) return enqueue_fused_run(pl, it0, nsteps, st);
   for (int s = 0; s < nsteps; ++s) {
@@ -705,7 +731,8 @@ int sw_plan_status(sw_plan* pl, void* stream) {
     int h = 0;
     e = cudaMemcpy(&h, pl->d_err, sizeof h, cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return cuda_fail(e, "sw_plan_status");
-    if (h) return fail(SW_ERR_TIMEOUT, "a bounded device wait gave up (TMA data never arrived)");
+    if (h & 1) return fail(SW_ERR_TIMEOUT, "a bounded device wait gave up (TMA data never arrived)");
+    if (h & 2) return fail(SW_ERR_TIMEOUT, "a bounded device wait gave up (grid barrier of the persistent run)");
   }
   return SW_OK;
 }
@@ -726,7 +753,15 @@ int sw_plan_info(sw_plan* pl, int32_t* info) {
 
 int sw_plan_set_path(sw_plan* pl, int32_t path, int32_t chunk_len) {
   if (!pl) return fail(SW_ERR_ARG, "null plan");
-  if (path < 0 || path > 2) return fail(SW_ERR_ARG, "path must be 0, 1 or 2");
+  if (path < 0 || path > 3) return fail(SW_ERR_ARG, "path must be 0, 1, 2 or 3");
+  if (path == 3) {
+    if (pl->dim != 2) return fail(SW_ERR_UNSUPPORTED, "the persistent path is for 2D plans");
+    int dev = 0, coop = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+    cudaGetLastError();
+    if (!coop) return fail(SW_ERR_UNSUPPORTED, "this device has no cooperative launch");
+  }
   if (path == 1 && !pl->staged) return fail(SW_ERR_UNSUPPORTED, "this plan has no staged path");
   if (path == 2 && !pl->fused) setup_fused(pl);  // allocates the second buffer set on first use
   if (path == 2 && !pl->fused) return fail(SW_ERR_UNSUPPORTED, "this plan has no fused path");
@@ -758,6 +793,7 @@ int sw_plan_destroy(sw_plan* pl) {
   if (pl->d_count) cudaFree(pl->d_count);
   if (pl->fused_buf) cudaFree(pl->fused_buf);
   if (pl->d_err) cudaFree(pl->d_err);
+  if (pl->d_bar) cudaFree(pl->d_bar);
   delete pl;
   return SW_OK;
 }
@@ -787,6 +823,12 @@ int sw_run(sw_plan* pl, int32_t it0, int32_t nsteps, int32_t use_graph, void* st
   if (nsteps == 0) return SW_OK;
   cudaStream_t st = (cudaStream_t)stream;
   cudaError_t e;
+  if (pl->dim == 2 && pl->path == 3) {
+    // one launch for the whole run: nothing to capture
+    e = persistent_run2(pl, it0, nsteps, st);
+    if (e != cudaSuccess) return cuda_fail(e, "sw_run: persistent launch");
+    return SW_OK;
+  }
   if (!use_graph) {
     e = enqueue_sequence(pl, it0, nsteps, st);
     if (e != cudaSuccess) return cuda_fail(e, "sw_run");
