@@ -360,7 +360,9 @@ def run_thin_layer(args, rank, world, local):
     from seiswave_taichi_b200 import learned_abc3d as LA
     from seiswave_taichi_b200.synthetic import layered
     torch.cuda.set_device(local)
-    n, nt, pad20, pad6 = 256, int(os.environ.get("SEISWAVE_CONFIG5_STEPS", "1500")), 22, 8
+    # SEISWAVE_CONFIG5_N / _STEPS shrink the case (profiling captures)
+    n = int(os.environ.get("SEISWAVE_CONFIG5_N", "256"))
+    nt, pad20, pad6 = int(os.environ.get("SEISWAVE_CONFIG5_STEPS", "1500")), 22, 8
     vp, vs, rho = layered((n, n, n), 2000.0, 5000.0, nlayers=8, seed=rank, anomaly=0.05)
     h, dt, f0 = 10.0, 8e-4, 12.0
     out = {}
