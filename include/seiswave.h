@@ -314,23 +314,25 @@ SW_API int sw3d_mlp_backward(const float* params, const float* x, const float* d
                              void* stream);
 
 /* ---- 2D adjoint (no reference counterpart) --------------------------------
- * Hand-written discrete adjoint of the SW2D_SSG_VS time loop with a
- * SW_SRC_MOMENT (or no) source and vz receivers, for gradients of a seismogram
+ * Hand-written discrete adjoint of the SW2D_SSG_VS or SW2D_SSG_SV time loop
+ * (the plan's scheme) with a SW_SRC_MOMENT (or no) source and the scheme's
+ * receivers (vz for VS, vx for SV), for gradients of a seismogram
  * misfit with respect to the material.  sw2d_record runs forward steps
  * it0..it0+nsteps-1 from the plan's current state and stores nsteps+1
  * snapshots of sw2d_snapshot_elems() elements each; sw2d_adjoint_run then
  * steps the adjoint state from it0+nsteps-1 down to it0 using them.  Together
  * they replace one checkpoint segment of the reference loop
- * (Elastic2D_CPML.py:128-200) run backwards. */
+ * (Elastic2D_CPML.py:128-200, :202-275) run backwards. */
 typedef struct sw2d_adjoint_desc {
   void* field[5];            /* adjoint of vx vz sxx szz sxz, (nx, nz) each    */
   void* mem[2];              /* adjoint memory variables, layout of sw2d_desc.mem */
   void* tmp[4];              /* scratch, (nx, nz) each                          */
   void* grad[5];             /* per-cell sums, added to: G_vx (coefficient
-                                dt/rho of vx), G_vz (dt/rho4 of vz), G_lpm
-                                (lambda+2mu at sxx), G_lhx (lambda at sxx),
-                                G_mhz (mu at sxz); see the Python wrapper for
-                                the chain to rho, lambda, mu                    */
+                                dt/rho of vx), G_vz (dt/rho of vz, rho the
+                                scheme's average), G_lpm (lambda+2mu at sxx),
+                                G_lhx (lambda at sxx), G_mhz (mu at sxz); see
+                                the Python wrapper for the chain to rho,
+                                lambda, mu                                      */
   const void* residual;      /* (nt_max, nrec): d misfit / d data              */
 } sw2d_adjoint_desc;
 

@@ -1,6 +1,6 @@
 """Test infrastructure, not product code: a differentiable float64 PyTorch
-restatement of the 2D SSG_VS step (src/Elastic2D_CPML.py:128-200) with the
-moment-tensor source, used as an independent gradient oracle for the
+restatement of the 2D SSG_VS step (src/Elastic2D_CPML.py:128-200) and of the
+SSG_SV step (:202-275) with the moment-tensor source, used as an independent gradient oracle for the
 hand-written adjoint kernels.  torch.autograd differentiates it exactly (to
 float64 rounding), so its gradients with respect to rho, lambda and mu are the
 discrete adjoint's reference values.  CPU only, small grids.
@@ -135,5 +135,72 @@ class TwinVS2D:
             szz = szz + _pad(dszz, i0, i1, j0, j1, nx, nz)
             sxz = sxz + _pad(dsxz, k0, k1, l0, l1, nx, nz)
             out.append(vz.reshape(-1)[self.rec])
+        self.final = (vx, vz, sxx, szz, sxz)
+        return torch.stack(out)
+
+
+class TwinSV2D(TwinVS2D):
+    """The SSG_SV step (src/Elastic2D_CPML.py:202-275) with the moment-tensor
+    source injected before each velocity phase; receivers record vx."""
+
+    def traces(self, rho, lam, mu, nt):
+        nx, nz, N = self.nx, self.nz, self.N
+        dx, dz, dt = self.dx, self.dz, self.dt
+        X, Z = self.X, self.Z
+        z = lambda: torch.zeros((nx, nz), dtype=torch.float64)
+        vx, vz, sxx, szz, sxz = z(), z(), z(), z(), z()
+        m = {k: z() for k in ("sxx_dx", "sxz_dz", "sxz_dx", "szz_dz", "dvx_dx", "dvz_dz", "dvz_dx", "dvx_dz")}
+        out = []
+        src = torch.zeros((nx, nz), dtype=torch.float64)
+        src[self.isx, self.isz] = 1.0
+        for it in range(nt):
+            w = self.wav[it]
+            sxx = sxx + src * (w * self.mneg[0])
+            szz = szz + src * (w * self.mneg[1])
+            sxz = sxz + src * (w * self.mneg[2])
+            # vx at (i+1/2, j) :218-229
+            i0, i1, j0, j1 = N, nx - N - 1, N + 1, nz - N
+            P = self.pxh[i0:i1, None] | self.pz[None, j0:j1]
+            r2 = (rho[i0:i1, j0:j1] + rho[i0 + 1:i1 + 1, j0:j1]) / 2
+            a1 = self._dx(sxx, i0, i1, j0, j1, True) / dx
+            b1 = self._dz(sxz, i0, i1, j0, j1, False) / dz
+            a1, m["sxx_dx"] = self._cpml(a1, m["sxx_dx"], P, X["b_half"], X["a_half"], X["k_half"], i0, i1, j0, j1, 0)
+            b1, m["sxz_dz"] = self._cpml(b1, m["sxz_dz"], P, Z["b"], Z["a"], Z["k"], i0, i1, j0, j1, 1)
+            dvx = (a1 + b1) * dt / r2
+            # vz at (i, j+1/2) :231-242
+            k0, k1, l0, l1 = N + 1, nx - N, N, nz - N - 1
+            P = self.px[k0:k1, None] | self.pzh[None, l0:l1]
+            rz = 0.5 * (rho[k0:k1, l0:l1] + rho[k0:k1, l0 + 1:l1 + 1])
+            a2 = self._dx(sxz, k0, k1, l0, l1, False) / dx
+            b2 = self._dz(szz, k0, k1, l0, l1, True) / dz
+            a2, m["sxz_dx"] = self._cpml(a2, m["sxz_dx"], P, X["b"], X["a"], X["k"], k0, k1, l0, l1, 0)
+            b2, m["szz_dz"] = self._cpml(b2, m["szz_dz"], P, Z["b_half"], Z["a_half"], Z["k_half"], k0, k1, l0, l1, 1)
+            dvz = (b2 + a2) * dt / rz
+            vx = vx + _pad(dvx, i0, i1, j0, j1, nx, nz)
+            vz = vz + _pad(dvz, k0, k1, l0, l1, nx, nz)
+            # sxx szz at (i, j) :247-260
+            i0, i1, j0, j1 = N + 1, nx - N, N + 1, nz - N
+            P = self.px[i0:i1, None] | self.pz[None, j0:j1]
+            lm = lam[i0:i1, j0:j1]
+            lpm = lam[i0:i1, j0:j1] + 2 * mu[i0:i1, j0:j1]
+            p = self._dx(vx, i0, i1, j0, j1, False) / dx
+            q = self._dz(vz, i0, i1, j0, j1, False) / dz
+            p, m["dvx_dx"] = self._cpml(p, m["dvx_dx"], P, X["b"], X["a"], X["k"], i0, i1, j0, j1, 0)
+            q, m["dvz_dz"] = self._cpml(q, m["dvz_dz"], P, Z["b"], Z["a"], Z["k"], i0, i1, j0, j1, 1)
+            dsxx = (lpm * p + lm * q) * dt
+            dszz = (lpm * q + lm * p) * dt
+            # sxz at (i+1/2, j+1/2) :262-273, same cells
+            P = self.pxh[i0:i1, None] | self.pzh[None, j0:j1]
+            m4 = 0.25 * (mu[i0:i1, j0 + 1:j1 + 1] + mu[i0:i1, j0:j1] + mu[i0 + 1:i1 + 1, j0 + 1:j1 + 1]
+                         + mu[i0 + 1:i1 + 1, j0:j1])
+            r = self._dx(vz, i0, i1, j0, j1, True) / dx
+            u = self._dz(vx, i0, i1, j0, j1, True) / dz
+            r, m["dvz_dx"] = self._cpml(r, m["dvz_dx"], P, X["b_half"], X["a_half"], X["k_half"], i0, i1, j0, j1, 0)
+            u, m["dvx_dz"] = self._cpml(u, m["dvx_dz"], P, Z["b_half"], Z["a_half"], Z["k_half"], i0, i1, j0, j1, 1)
+            dsxz = m4 * (u + r) * dt
+            sxx = sxx + _pad(dsxx, i0, i1, j0, j1, nx, nz)
+            szz = szz + _pad(dszz, i0, i1, j0, j1, nx, nz)
+            sxz = sxz + _pad(dsxz, i0, i1, j0, j1, nx, nz)
+            out.append(vx.reshape(-1)[self.rec])
         self.final = (vx, vz, sxx, szz, sxz)
         return torch.stack(out)

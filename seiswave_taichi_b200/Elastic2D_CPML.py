@@ -305,12 +305,13 @@ class ElasticWAVE:
         self._plan(s).run(int(it0), nt, use_graph, self._stream())
         return self
 
-    def forward_op(self, vp, vs, rho, checkpoint_every: int = 100):
-        """Differentiable seismogram: the VS scheme's (nt, nrec) traces as a
-        function of the vp, vs, rho tensors (device, the solver's dtype),
-        with the hand-written adjoint as backward (no reference counterpart)."""
+    def forward_op(self, vp, vs, rho, checkpoint_every: int = 100, scheme: str = "VS"):
+        """Differentiable seismogram: the (nt, nrec) traces of the VS scheme
+        (vz) or the SV scheme (vx) as a function of the vp, vs, rho tensors
+        (device, the solver's dtype), with the hand-written adjoint as
+        backward (no reference counterpart)."""
         from .adjoint import ForwardOp2D
-        return ForwardOp2D.apply(vp, vs, rho, self, int(checkpoint_every))
+        return ForwardOp2D.apply(vp, vs, rho, self, int(checkpoint_every), scheme)
 
     def check_finite(self) -> int:
         return self._plan(N.SW2D_SSG_VS).check_finite(self._stream())

@@ -26,16 +26,22 @@ from . import _native as N
 
 
 class Adjoint2D:
-    """Checkpointed forward + adjoint driver for one 2D VS solver."""
+    """Checkpointed forward + adjoint driver for one 2D solver, scheme "VS"
+    (update_SSG_VS, vz traces) or "SV" (update_SSG_SV, vx traces)."""
 
-    def __init__(self, wave, checkpoint_every: int = 100):
+    SCHEMES = {"VS": N.SW2D_SSG_VS, "SV": N.SW2D_SSG_SV}
+
+    def __init__(self, wave, checkpoint_every: int = 100, scheme: str = "VS"):
         if wave.MT is None:
             raise ValueError("the 2D adjoint needs the moment-tensor source (MT=...)")
+        if scheme not in self.SCHEMES:
+            raise ValueError(f"scheme must be 'VS' or 'SV', not {scheme!r}")
         self.w = wave
+        self.scheme = scheme
         self.K = int(checkpoint_every)
         if self.K < 1:
             raise ValueError("checkpoint_every must be >= 1")
-        self.plan = wave._plan(N.SW2D_SSG_VS)
+        self.plan = wave._plan(self.SCHEMES[scheme])
         n = C.c_int64(0)
         N.check(N.load().sw2d_snapshot_elems(self.plan.handle, C.byref(n)))
         self.snap_elems = int(n.value)
@@ -92,7 +98,36 @@ class Adjoint2D:
             N.check(lib.sw2d_record(self.plan.handle, it0, n, C.c_void_p(snap.data_ptr()), C.c_void_p(st)))
             N.check(lib.sw2d_adjoint_run(self.plan.handle, C.byref(d), it0, n, C.c_void_p(snap.data_ptr()),
                                          C.c_void_p(st)))
-        return coefficient_chain(w.rho, grad)
+        return (coefficient_chain_sv if self.scheme == "SV" else coefficient_chain)(w.rho, grad)
+
+
+def coefficient_chain_sv(rho, grad):
+    """The SV scheme's per-cell sums to (g_rho, g_lam, g_mu).
+
+    grad[0]: vx += dt/rho2 * s, rho2 = (rho[i,j] + rho[i+1,j])/2
+    grad[1]: vz += dt/rhoz * s, rhoz = (rho[i,j] + rho[i,j+1])/2
+    grad[2]: lpm = lam + 2 mu at sxx (i, j);  grad[3]: lam at sxx
+    grad[4]: m4 = mean of mu over (i,j) (i,j+1) (i+1,j+1) (i+1,j) at sxz
+    (Elastic2D_CPML.py:225,238,252-253,266).
+    """
+    g0, g1, g2, g3, g4 = grad
+    g_rho = torch.zeros_like(rho)
+    r2 = (rho[:-1] + rho[1:]) / 2
+    q = 0.5 * (-g0[:-1] / (r2 * r2))
+    g_rho[:-1] += q
+    g_rho[1:] += q
+    rz = 0.5 * (rho[:, :-1] + rho[:, 1:])
+    q = 0.5 * (-g1[:, :-1] / (rz * rz))
+    g_rho[:, :-1] += q
+    g_rho[:, 1:] += q
+    g_lam = g2 + g3
+    g_mu = 2 * g2
+    q = 0.25 * g4[:-1, :-1]
+    g_mu[:-1, :-1] += q
+    g_mu[:-1, 1:] += q
+    g_mu[1:, 1:] += q
+    g_mu[1:, :-1] += q
+    return g_rho, g_lam, g_mu
 
 
 def coefficient_chain(rho, grad):
@@ -133,9 +168,9 @@ class ForwardOp2D(torch.autograd.Function):
     its backward."""
 
     @staticmethod
-    def forward(ctx, vp, vs, rho, wave, checkpoint_every):
+    def forward(ctx, vp, vs, rho, wave, checkpoint_every, scheme="VS"):
         wave.set_model(vp.detach(), vs.detach(), rho.detach())
-        drv = Adjoint2D(wave, checkpoint_every)
+        drv = Adjoint2D(wave, checkpoint_every, scheme)
         out = drv.forward()
         ctx.drv = drv
         ctx.save_for_backward(vp.detach(), vs.detach(), rho.detach())
@@ -148,7 +183,7 @@ class ForwardOp2D(torch.autograd.Function):
         g_vp = g_lam * 2 * rho * vp
         g_vs = g_mu * 2 * rho * vs - g_lam * 4 * rho * vs
         g_rh = g_rho + g_mu * vs * vs + g_lam * (vp * vp - 2 * vs * vs)
-        return g_vp.to(vp.dtype), g_vs.to(vs.dtype), g_rh.to(rho.dtype), None, None
+        return g_vp.to(vp.dtype), g_vs.to(vs.dtype), g_rh.to(rho.dtype), None, None, None
 
 
 # ---- 3D (CPML moment-tensor scheme) ---------------------------------------------

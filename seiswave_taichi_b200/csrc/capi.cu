@@ -42,7 +42,7 @@ struct A2 {
   const T* snap0;
   const T* snap1;
 };
-template <typename T> cudaError_t sw2_adjoint_step(const P2<T>&, const A2<T>&, int, int, cudaStream_t);
+template <typename T> cudaError_t sw2_adjoint_step(const P2<T>&, const A2<T>&, int, int, int, cudaStream_t);
 template <typename T>
 struct A3 {
   T* f[9];
@@ -890,8 +890,8 @@ namespace {
 
 int adjoint_plan_ok(sw_plan* pl, const char* who) {
   if (!pl) return fail(SW_ERR_ARG, std::string(who) + ": null plan");
-  if (pl->dim != 2 || pl->scheme != SW2D_SSG_VS)
-    return fail(SW_ERR_UNSUPPORTED, std::string(who) + ": the adjoint covers the 2D SSG_VS scheme");
+  if (pl->dim != 2 || (pl->scheme != SW2D_SSG_VS && pl->scheme != SW2D_SSG_SV))
+    return fail(SW_ERR_UNSUPPORTED, std::string(who) + ": the adjoint covers the 2D SSG_VS and SSG_SV schemes");
   if (pl->src_kind != SW_SRC_MOMENT && pl->src_kind != SW_SRC_NONE)
     return fail(SW_ERR_UNSUPPORTED, std::string(who) + ": the adjoint covers moment-tensor sources");
   return SW_OK;
@@ -943,7 +943,7 @@ cudaError_t adjoint2(sw_plan* pl, const sw::P2<T>& p, const sw2d_adjoint_desc* d
   for (int k = n - 1; k >= 0; --k) {
     a.snap0 = snap + k * se;
     a.snap1 = snap + (k + 1) * se;
-    cudaError_t e = sw::sw2_adjoint_step<T>(p, a, pl->order, it0 + k, st);
+    cudaError_t e = sw::sw2_adjoint_step<T>(p, a, pl->scheme, pl->order, it0 + k, st);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;

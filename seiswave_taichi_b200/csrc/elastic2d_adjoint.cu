@@ -1,6 +1,8 @@
-// elastic2d_adjoint.cu -- hand-written discrete adjoint of the 2D SSG_VS time
-// step (src/Elastic2D_CPML.py:128-200) with a moment-tensor source, and the
-// forward recording pass it runs on.  No reference counterpart.
+// elastic2d_adjoint.cu -- hand-written discrete adjoints of the 2D SSG_VS and
+// SSG_SV time steps (src/Elastic2D_CPML.py:128-200, :202-275) with a
+// moment-tensor source, and the forward recording pass they run on.  No
+// reference counterpart.  The VS derivation is written out here; the SV
+// kernels below follow it with that scheme's staggering.
 //
 // Forward step it, as linear maps on the state (v, sigma, psi):
 //   inject   sigma[src] += w(it) * (-M)                         (affine)
@@ -274,35 +276,237 @@ k2a_str_gather(const __grid_constant__ P2<T> p, const __grid_constant__ A2<T> a)
   a.f[4][idx] += gxz;
 }
 
+// ============================================================================
+// SSG_SV (src/Elastic2D_CPML.py:202-275): vx at (i+1/2, j), vz at (i, j+1/2),
+// sxx szz at (i, j), sxz at (i+1/2, j+1/2).
+//   V  vx += dt/rho2 * (Dfx sxx' + Dbz sxz'),  rho2 = (rho[i,j] + rho[i+1,j]) / 2
+//      vz += dt/rhoz * (Dfz szz' + Dbx sxz'),  rhoz = (rho[i,j] + rho[i,j+1]) / 2
+//   S  sxx += dt*(lpm p' + lm q'),  szz += dt*(lpm q' + lm p'),
+//      p = Dbx vx, q = Dbz vz, lm = lam[i,j], lpm = lam + 2 mu
+//      sxz += m4*(u' + r')*dt,  u = Dfz vx, r = Dfx vz, m4 = mean of mu over
+//      (i,j) (i,j+1) (i+1,j+1) (i+1,j)
+//   record data[it] = vx[rec]
+// The gradient slots hold the same kind of per-cell sums as for VS:
+// G_vx (rho2), G_vz (rhoz), G_lpm, G_lm, G_m4.
+// ============================================================================
+template <typename T, int N>
+__global__ void __launch_bounds__(A2Z * A2X)
+k2a_sv_stress_mid(const __grid_constant__ P2<T> p, const __grid_constant__ A2<T> a) {
+  const int j = blockIdx.x * A2Z + threadIdx.x;
+  const int i = blockIdx.y * A2X + threadIdx.y;
+  const int nx = p.nx, nz = p.nz;
+  if (i >= nx || j >= nz) return;
+  const long long idx = (long long)i * nz + j;
+  const T dx = p.dx, dz = p.dz, dt = p.dt;
+  T c[N];
+#pragma unroll
+  for (int m = 0; m < N; ++m) c[m] = p.c[m];
+  const Snap2<T> s0 = snap_of(p, a.snap0), s1 = snap_of(p, a.snap1);
+  const T* vx = s1.f(0);
+  const T* vz = s1.f(1);
+  const T* cfx = p.cf[0];
+  const T* cfz = p.cf[1];
+  const int xi = slab_index(i, nx, p.lo[0], p.hi[0]);
+  const int zj = slab_index(j, nz, p.lo[1], p.hi[1]);
+  const uint8_t fx = p.fl[0][i], fz = p.fl[1][j];
+  T t0 = 0, t1 = 0, t2 = 0, t3 = 0;
+  if (i >= N + 1 && i < nx - N && j >= N + 1 && j < nz - N) {
+    // sxx szz at (i, j)
+    {
+      const T lm = p.lam[idx];
+      const T lpm = p.lam[idx] + (T)2 * p.mu[idx];
+      T pv = dx_bm<T, N>(vx, idx, nz, c) / dx;
+      T qv = dz_bm<T, N>(vz, idx, c) / dz;
+      const bool P = (fx & 1) || (fz & 1);
+      const T bx = cfx[CB * nx + i], ax = cfx[CA * nx + i], kx = cfx[CK * nx + i];
+      const T bz = cfz[CB * nz + j], az = cfz[CA * nz + j], kz = cfz[CK * nz + j];
+      if (P && xi >= 0) pv = pml_fwd(pv, s0.mx(2, xi, j), bx, ax, kx);
+      if (P && zj >= 0) qv = pml_fwd(qv, s0.mz(2, i, zj), bz, az, kz);
+      const T sb = a.f[2][idx], zb = a.f[3][idx];
+      a.grad[2][idx] += dt * (sb * pv + zb * qv);
+      a.grad[3][idx] += dt * (sb * qv + zb * pv);
+      T pb = dt * (lpm * sb + lm * zb);
+      T qb = dt * (lm * sb + lpm * zb);
+      if (P && xi >= 0) pb = pml_adj(pb, amx(p, a, 2, xi, j), bx, ax, kx);
+      if (P && zj >= 0) qb = pml_adj(qb, amz(p, a, 2, i, zj), bz, az, kz);
+      t0 = pb / dx;
+      t1 = qb / dz;
+    }
+    // sxz at (i+1/2, j+1/2)
+    {
+      const T m4 = (T)0.25 * (p.mu[idx + 1] + p.mu[idx] + p.mu[idx + nz + 1] + p.mu[idx + nz]);
+      T rv = dx_fm<T, N>(vz, idx, nz, c) / dx;
+      T uv = dz_fm<T, N>(vx, idx, c) / dz;
+      const bool P = (fx & 2) || (fz & 2);
+      const T bxh = cfx[CBH * nx + i], axh = cfx[CAH * nx + i], kxh = cfx[CKH * nx + i];
+      const T bzh = cfz[CBH * nz + j], azh = cfz[CAH * nz + j], kzh = cfz[CKH * nz + j];
+      if (P && xi >= 0) rv = pml_fwd(rv, s0.mx(3, xi, j), bxh, axh, kxh);
+      if (P && zj >= 0) uv = pml_fwd(uv, s0.mz(3, i, zj), bzh, azh, kzh);
+      const T xb = a.f[4][idx];
+      a.grad[4][idx] += dt * xb * (uv + rv);
+      T sb = m4 * dt * xb;
+      T ub = sb, rb = sb;
+      if (P && xi >= 0) rb = pml_adj(rb, amx(p, a, 3, xi, j), bxh, axh, kxh);
+      if (P && zj >= 0) ub = pml_adj(ub, amz(p, a, 3, i, zj), bzh, azh, kzh);
+      t2 = ub / dz;
+      t3 = rb / dx;
+    }
+  }
+  a.tmp[0][idx] = t0;
+  a.tmp[1][idx] = t1;
+  a.tmp[2][idx] = t2;
+  a.tmp[3][idx] = t3;
+}
+
+// vx_bar += Dbx^T t0 + Dfz^T t2;  vz_bar += Dbz^T t1 + Dfx^T t3
+template <typename T, int N>
+__global__ void __launch_bounds__(A2Z * A2X)
+k2a_sv_vel_gather(const __grid_constant__ P2<T> p, const __grid_constant__ A2<T> a) {
+  const int j = blockIdx.x * A2Z + threadIdx.x;
+  const int i = blockIdx.y * A2X + threadIdx.y;
+  const int nx = p.nx, nz = p.nz;
+  if (i >= nx || j >= nz) return;
+  const long long idx = (long long)i * nz + j;
+  T gx = 0, gz = 0;
+#pragma unroll
+  for (int m = 0; m < N; ++m) {
+    const T c = p.c[m];
+    gx += c * (at(a.tmp[0], i - m, j, nx, nz) - at(a.tmp[0], i + m + 1, j, nx, nz));
+    gx += c * (at(a.tmp[2], i, j - m - 1, nx, nz) - at(a.tmp[2], i, j + m, nx, nz));
+    gz += c * (at(a.tmp[1], i, j - m, nx, nz) - at(a.tmp[1], i, j + m + 1, nx, nz));
+    gz += c * (at(a.tmp[3], i - m - 1, j, nx, nz) - at(a.tmp[3], i + m, j, nx, nz));
+  }
+  a.f[0][idx] += gx;
+  a.f[1][idx] += gz;
+}
+
+template <typename T, int N>
+__global__ void __launch_bounds__(A2Z * A2X)
+k2a_sv_vel_mid(const __grid_constant__ P2<T> p, const __grid_constant__ A2<T> a) {
+  const int j = blockIdx.x * A2Z + threadIdx.x;
+  const int i = blockIdx.y * A2X + threadIdx.y;
+  const int nx = p.nx, nz = p.nz;
+  if (i >= nx || j >= nz) return;
+  const long long idx = (long long)i * nz + j;
+  const T dx = p.dx, dz = p.dz, dt = p.dt;
+  T c[N];
+#pragma unroll
+  for (int m = 0; m < N; ++m) c[m] = p.c[m];
+  const Snap2<T> s0 = snap_of(p, a.snap0);
+  const T* sxx = s0.f(2);
+  const T* szz = s0.f(3);
+  const T* sxz = s0.f(4);
+  const T* cfx = p.cf[0];
+  const T* cfz = p.cf[1];
+  const T* rho = p.rho;
+  const int xi = slab_index(i, nx, p.lo[0], p.hi[0]);
+  const int zj = slab_index(j, nz, p.lo[1], p.hi[1]);
+  const uint8_t fx = p.fl[0][i], fz = p.fl[1][j];
+  T t0 = 0, t1 = 0, t2 = 0, t3 = 0;
+  // vx at (i+1/2, j)
+  if (i >= N && i < nx - N - 1 && j >= N + 1 && j < nz - N) {
+    T av = dx_fm<T, N>(sxx, idx, nz, c) / dx;
+    T bv = dz_bm<T, N>(sxz, idx, c) / dz;
+    const bool P = (fx & 2) || (fz & 1);
+    const T bxh = cfx[CBH * nx + i], axh = cfx[CAH * nx + i], kxh = cfx[CKH * nx + i];
+    const T bz = cfz[CB * nz + j], az = cfz[CA * nz + j], kz = cfz[CK * nz + j];
+    if (P && xi >= 0) av = pml_fwd(av, s0.mx(0, xi, j), bxh, axh, kxh);
+    if (P && zj >= 0) bv = pml_fwd(bv, s0.mz(0, i, zj), bz, az, kz);
+    const T vb = a.f[0][idx];
+    a.grad[0][idx] += vb * (av + bv) * dt;
+    const T rh = (rho[idx] + rho[idx + nz]) / (T)2;
+    T sb = vb * dt / rh;
+    T ab = sb, bb = sb;
+    if (P && xi >= 0) ab = pml_adj(ab, amx(p, a, 0, xi, j), bxh, axh, kxh);
+    if (P && zj >= 0) bb = pml_adj(bb, amz(p, a, 0, i, zj), bz, az, kz);
+    t0 = ab / dx;
+    t1 = bb / dz;
+  }
+  // vz at (i, j+1/2)
+  if (i >= N + 1 && i < nx - N && j >= N && j < nz - N - 1) {
+    T av = dx_bm<T, N>(sxz, idx, nz, c) / dx;
+    T bv = dz_fm<T, N>(szz, idx, c) / dz;
+    const bool P = (fx & 1) || (fz & 2);
+    const T bx = cfx[CB * nx + i], ax = cfx[CA * nx + i], kx = cfx[CK * nx + i];
+    const T bzh = cfz[CBH * nz + j], azh = cfz[CAH * nz + j], kzh = cfz[CKH * nz + j];
+    if (P && xi >= 0) av = pml_fwd(av, s0.mx(1, xi, j), bx, ax, kx);
+    if (P && zj >= 0) bv = pml_fwd(bv, s0.mz(1, i, zj), bzh, azh, kzh);
+    const T vb = a.f[1][idx];
+    a.grad[1][idx] += vb * (av + bv) * dt;
+    const T rh = (T)0.5 * (rho[idx] + rho[idx + 1]);
+    T sb = vb * dt / rh;
+    T ab = sb, bb = sb;
+    if (P && xi >= 0) ab = pml_adj(ab, amx(p, a, 1, xi, j), bx, ax, kx);
+    if (P && zj >= 0) bb = pml_adj(bb, amz(p, a, 1, i, zj), bzh, azh, kzh);
+    t2 = ab / dx;
+    t3 = bb / dz;
+  }
+  a.tmp[0][idx] = t0;
+  a.tmp[1][idx] = t1;
+  a.tmp[2][idx] = t2;
+  a.tmp[3][idx] = t3;
+}
+
+// sxx_bar += Dfx^T t0;  sxz_bar += Dbz^T t1 + Dbx^T t2;  szz_bar += Dfz^T t3
+template <typename T, int N>
+__global__ void __launch_bounds__(A2Z * A2X)
+k2a_sv_str_gather(const __grid_constant__ P2<T> p, const __grid_constant__ A2<T> a) {
+  const int j = blockIdx.x * A2Z + threadIdx.x;
+  const int i = blockIdx.y * A2X + threadIdx.y;
+  const int nx = p.nx, nz = p.nz;
+  if (i >= nx || j >= nz) return;
+  const long long idx = (long long)i * nz + j;
+  T gxx = 0, gxz = 0, gzz = 0;
+#pragma unroll
+  for (int m = 0; m < N; ++m) {
+    const T c = p.c[m];
+    gxx += c * (at(a.tmp[0], i - m - 1, j, nx, nz) - at(a.tmp[0], i + m, j, nx, nz));
+    gxz += c * (at(a.tmp[1], i, j - m, nx, nz) - at(a.tmp[1], i, j + m + 1, nx, nz));
+    gxz += c * (at(a.tmp[2], i - m, j, nx, nz) - at(a.tmp[2], i + m + 1, j, nx, nz));
+    gzz += c * (at(a.tmp[3], i, j - m - 1, nx, nz) - at(a.tmp[3], i, j + m, nx, nz));
+  }
+  a.f[2][idx] += gxx;
+  a.f[3][idx] += gzz;
+  a.f[4][idx] += gxz;
+}
+
 // ---- host side ----------------------------------------------------------------
 template <typename T, int N>
-static cudaError_t adj_step(const P2<T>& p, const A2<T>& a, int it, cudaStream_t st) {
+static cudaError_t adj_step(const P2<T>& p, const A2<T>& a, int scheme, int it, cudaStream_t st) {
   dim3 block(A2Z, A2X);
   dim3 grid((p.nz + A2Z - 1) / A2Z, (p.nx + A2X - 1) / A2X);
   if (p.nrec > 0) k2a_record<T><<<(p.nrec + 255) / 256, 256, 0, st>>>(p, a, it);
-  k2a_stress_mid<T, N><<<grid, block, 0, st>>>(p, a);
-  k2a_vel_gather<T, N><<<grid, block, 0, st>>>(p, a);
-  k2a_vel_mid<T, N><<<grid, block, 0, st>>>(p, a);
-  k2a_str_gather<T, N><<<grid, block, 0, st>>>(p, a);
+  if (scheme == SW2D_SSG_SV) {
+    k2a_sv_stress_mid<T, N><<<grid, block, 0, st>>>(p, a);
+    k2a_sv_vel_gather<T, N><<<grid, block, 0, st>>>(p, a);
+    k2a_sv_vel_mid<T, N><<<grid, block, 0, st>>>(p, a);
+    k2a_sv_str_gather<T, N><<<grid, block, 0, st>>>(p, a);
+  } else {
+    k2a_stress_mid<T, N><<<grid, block, 0, st>>>(p, a);
+    k2a_vel_gather<T, N><<<grid, block, 0, st>>>(p, a);
+    k2a_vel_mid<T, N><<<grid, block, 0, st>>>(p, a);
+    k2a_str_gather<T, N><<<grid, block, 0, st>>>(p, a);
+  }
   return cudaGetLastError();
 }
 
+// one adjoint step of the 2D SSG_VS or SSG_SV scheme
 template <typename T>
-cudaError_t sw2_adjoint_step(const P2<T>& p, const A2<T>& a, int order, int it, cudaStream_t st) {
+cudaError_t sw2_adjoint_step(const P2<T>& p, const A2<T>& a, int scheme, int order, int it, cudaStream_t st) {
   switch (order) {
-    case 1: return adj_step<T, 1>(p, a, it, st);
-    case 2: return adj_step<T, 2>(p, a, it, st);
-    case 3: return adj_step<T, 3>(p, a, it, st);
-    case 4: return adj_step<T, 4>(p, a, it, st);
-    case 5: return adj_step<T, 5>(p, a, it, st);
-    case 6: return adj_step<T, 6>(p, a, it, st);
-    case 7: return adj_step<T, 7>(p, a, it, st);
-    case 8: return adj_step<T, 8>(p, a, it, st);
+    case 1: return adj_step<T, 1>(p, a, scheme, it, st);
+    case 2: return adj_step<T, 2>(p, a, scheme, it, st);
+    case 3: return adj_step<T, 3>(p, a, scheme, it, st);
+    case 4: return adj_step<T, 4>(p, a, scheme, it, st);
+    case 5: return adj_step<T, 5>(p, a, scheme, it, st);
+    case 6: return adj_step<T, 6>(p, a, scheme, it, st);
+    case 7: return adj_step<T, 7>(p, a, scheme, it, st);
+    case 8: return adj_step<T, 8>(p, a, scheme, it, st);
     default: return cudaErrorInvalidValue;
   }
 }
 
-template cudaError_t sw2_adjoint_step<float>(const P2<float>&, const A2<float>&, int, int, cudaStream_t);
-template cudaError_t sw2_adjoint_step<double>(const P2<double>&, const A2<double>&, int, int, cudaStream_t);
+template cudaError_t sw2_adjoint_step<float>(const P2<float>&, const A2<float>&, int, int, int, cudaStream_t);
+template cudaError_t sw2_adjoint_step<double>(const P2<double>&, const A2<double>&, int, int, int, cudaStream_t);
 
 }  // namespace sw
