@@ -10,8 +10,8 @@
 // elected thread issues cp.async.bulk.tensor loads of whole plane tiles (with
 // the halo each array needs) into shared-memory rings, D planes ahead,
 // completing on mbarriers; x taps come from the ring planes, y and z taps from
-// the halo.  Every thread updates four consecutive z cells (float4 shared and
-// global accesses).  A tile plane that lies inside every update range and
+// the halo.  Every thread updates Q consecutive z cells (a "quad", Q = 2 or
+// 4, moved with 8- or 16-byte shared and global accesses).  A tile plane that lies inside every update range and
 // outside every CPML slab takes a branch-free path; the others evaluate the
 // update ranges per cell and the CPML memory variables on their slabs.
 // Arithmetic follows the reference's operation order with -fmad=false, exact
@@ -24,10 +24,20 @@
 
 namespace sw {
 
-template <int N, int TY, int D>
+// z cells per thread: 2 in exact mode, 4 in fast mode.  Two cells keep the
+// exact kernels at 116-128 registers, so two 256-thread CTAs (16 warps) fit
+// per SM instead of three 128-thread ones at 168 (12 warps), which hides more
+// of the exact arithmetic's dependent chains (measured on B200 at 200^3:
+// steps 300-500 887 vs 1210 us, steady 729 vs 744 us); the fast kernels,
+// with shorter chains, are quicker with four (534 vs 594 us).
+constexpr int staged_q(bool exact) { return exact ? 2 : 4; }
+
+template <int N, int TY, int D, int Q>
 struct SG {
   static constexpr int TZ = 32;
-  static constexpr int NT = TY * 8;            // one thread per 4 z cells
+  static constexpr int CQ = TZ / Q;            // threads along z: Q cells each
+  static constexpr int NT = TY * CQ;
+  static constexpr int MINB = Q == 4 ? 3 : 2;  // CTAs per SM the register budget aims at
   static constexpr int H4 = ((N + 3) / 4) * 4; // z halo, rounded to 16 bytes
   static constexpr int WZ = TZ + 2 * H4;       // width of boxes with a z halo
   static constexpr int HY = TY + 2 * N;        // height of boxes with a y halo
@@ -39,7 +49,7 @@ struct SG {
   static constexpr int B_R = TZ * (TY + 1);    // rho (j+1)
   // stress pass boxes
   static constexpr int B_L = TZ * TY;          // lam
-  static constexpr int WM = TZ + 4;            // mu (k+1 .. k+4 of the last quad)
+  static constexpr int WM = TZ + 4;            // mu (k+1 .. k+Q of the last quad)
   static constexpr int B_M = WM * (TY + 1);    // mu (j+1)
   static constexpr int RX = 2 * N + D;         // rings of arrays with x taps
   static constexpr int R1 = 1 + D;             // rings of in-plane arrays
@@ -66,83 +76,101 @@ struct SG {
   static_assert(N <= 4 || H4 >= N, "z window");
 };
 
-__device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
-__device__ __forceinline__ void st4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
-__device__ __forceinline__ float4 ldg4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+// Q consecutive z cells of one thread (Q = 2 or 4): the float2 / float4
+// vector type itself, moved with one 8- or 16-byte access
+template <int Q>
+struct VecOf;
+template <>
+struct VecOf<4> {
+  using type = float4;
+};
+template <>
+struct VecOf<2> {
+  using type = float2;
+};
+template <int Q>
+using Vq = typename VecOf<Q>::type;
+
+template <int Q>
+__device__ __forceinline__ Vq<Q> ldq(const float* p) {
+  return *reinterpret_cast<const Vq<Q>*>(p);
+}
+template <int Q>
+__device__ __forceinline__ void stq(float* p, const Vq<Q>& a) {
+  *reinterpret_cast<Vq<Q>*>(p) = a;
+}
+template <int Q>
+__device__ __forceinline__ Vq<Q> ldgq(const float* p) {
+  return __ldg(reinterpret_cast<const Vq<Q>*>(p));
+}
 __device__ __forceinline__ float g4(const float4& v, int e) { return e == 0 ? v.x : e == 1 ? v.y : e == 2 ? v.z : v.w; }
 __device__ __forceinline__ void s4(float4& v, int e, float x) {
   if (e == 0) v.x = x; else if (e == 1) v.y = x; else if (e == 2) v.z = x; else v.w = x;
+}
+__device__ __forceinline__ float g4(const float2& v, int e) { return e == 0 ? v.x : v.y; }
+__device__ __forceinline__ void s4(float2& v, int e, float x) {
+  if (e == 0) v.x = x; else v.y = x;
 }
 __device__ __forceinline__ int rslot(int plane, int R) {
   int s = plane % R;
   return s < 0 ? s + R : s;
 }
 
-// acc += c * (a - b), lane by lane, in the reference's operation order
-__device__ __forceinline__ void tap4(float4& acc, float c, const float4& a, const float4& b) {
-  acc.x = acc.x + c * (a.x - b.x);
-  acc.y = acc.y + c * (a.y - b.y);
-  acc.z = acc.z + c * (a.z - b.z);
-  acc.w = acc.w + c * (a.w - b.w);
-}
-
-// fast mode: acc = fma(c, a - b, acc), the spacing already folded into c
-__device__ __forceinline__ void tap4f(float4& acc, float c, const float4& a, const float4& b) {
-  acc.x = __fmaf_rn(c, a.x - b.x, acc.x);
-  acc.y = __fmaf_rn(c, a.y - b.y, acc.y);
-  acc.z = __fmaf_rn(c, a.z - b.z, acc.z);
-  acc.w = __fmaf_rn(c, a.w - b.w, acc.w);
-}
-template <bool EX>
-__device__ __forceinline__ void tapq(float4& acc, float c, const float4& a, const float4& b) {
-  if (EX) tap4(acc, c, a, b);
-  else tap4f(acc, c, a, b);
+// acc += c * (a - b) lane by lane in the reference's operation order (exact
+// mode), or acc = fma(c, a - b, acc) with the spacing folded into c (fast mode)
+template <bool EX, int Q>
+__device__ __forceinline__ void tapq(Vq<Q>& acc, float c, const Vq<Q>& a, const Vq<Q>& b) {
+#pragma unroll
+  for (int e = 0; e < Q; ++e)
+    s4(acc, e, EX ? g4(acc, e) + c * (g4(a, e) - g4(b, e)) : __fmaf_rn(c, g4(a, e) - g4(b, e), g4(acc, e)));
 }
 
 // derivative across ring planes: pl[q] is the plane (centre - N + q + FWD)
-template <int N, bool EX = true>
-__device__ __forceinline__ float4 dxq(const float* const* pl, int off, const float* c) {
-  float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+template <int N, bool EX, int Q>
+__device__ __forceinline__ Vq<Q> dxq(const float* const* pl, int off, const float* c) {
+  Vq<Q> v{};
 #pragma unroll
-  for (int m = 0; m < N; ++m) tapq<EX>(v, c[m], ld4(pl[N + m] + off), ld4(pl[N - 1 - m] + off));
+  for (int m = 0; m < N; ++m) tapq<EX, Q>(v, c[m], ldq<Q>(pl[N + m] + off), ldq<Q>(pl[N - 1 - m] + off));
   return v;
 }
 // derivative along a shared-memory stride (y rows): FWD f[+m+1]-f[-m], else f[+m]-f[-m-1]
-template <int N, bool FWD, bool EX = true>
-__device__ __forceinline__ float4 dyq(const float* s, int off, int stride, const float* c) {
-  float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+template <int N, bool FWD, bool EX, int Q>
+__device__ __forceinline__ Vq<Q> dyq(const float* s, int off, int stride, const float* c) {
+  Vq<Q> v{};
 #pragma unroll
   for (int m = 0; m < N; ++m)
-    tapq<EX>(v, c[m], ld4(s + off + (FWD ? m + 1 : m) * stride), ld4(s + off - (FWD ? m : m + 1) * stride));
+    tapq<EX, Q>(v, c[m], ldq<Q>(s + off + (FWD ? m + 1 : m) * stride), ldq<Q>(s + off - (FWD ? m : m + 1) * stride));
   return v;
 }
-// derivative along z from one window of aligned float4s around the quad
-template <int N, bool FWD, bool EX = true>
-__device__ __forceinline__ float4 dzq(const float* s, int off, const float* c) {
+// derivative along z from one window of aligned vectors around the thread's cells
+template <int N, bool FWD, bool EX, int Q>
+__device__ __forceinline__ Vq<Q> dzq(const float* s, int off, const float* c) {
   constexpr int H = ((N + 3) / 4) * 4;
-  constexpr int NW = (2 * H + 4) / 4;
-  float w[4 * NW];
+  constexpr int NW = (2 * H + Q) / Q;
+  float w[Q * NW];
 #pragma unroll
   for (int t = 0; t < NW; ++t) {
-    const float4 q = ld4(s + off - H + 4 * t);
-    w[4 * t] = q.x; w[4 * t + 1] = q.y; w[4 * t + 2] = q.z; w[4 * t + 3] = q.w;
-  }
-  float r[4] = {0.f, 0.f, 0.f, 0.f};
+    const Vq<Q> q = ldq<Q>(s + off - H + Q * t);
 #pragma unroll
-  for (int e = 0; e < 4; ++e)
+    for (int e = 0; e < Q; ++e) w[Q * t + e] = g4(q, e);
+  }
+  float r[Q];
+#pragma unroll
+  for (int e = 0; e < Q; ++e) r[e] = 0.f;
+#pragma unroll
+  for (int e = 0; e < Q; ++e)
 #pragma unroll
     for (int m = 0; m < N; ++m)
     {
       const float df = FWD ? (w[H + e + m + 1] - w[H + e - m]) : (w[H + e + m] - w[H + e - m - 1]);
       r[e] = EX ? r[e] + c[m] * df : __fmaf_rn(c[m], df, r[e]);
     }
-  return make_float4(r[0], r[1], r[2], r[3]);
+  Vq<Q> o;
+#pragma unroll
+  for (int e = 0; e < Q; ++e) s4(o, e, r[e]);
+  return o;
 }
 
-__device__ __forceinline__ float4 divc4(float4 v, float d, float r, int fast) {
-  return make_float4(div_c(v.x, d, r, fast), div_c(v.y, d, r, fast), div_c(v.z, d, r, fast),
-                     div_c(v.w, d, r, fast));
-}
 // Exact division of a group of stencil sums by the constant spacings.  When
 // the spacings' Markstein path is verified (fast != 0) and every lane is zero
 // or of magnitude in [2^-100, 2^100), the whole group runs as one branch-free
@@ -153,40 +181,30 @@ __device__ __forceinline__ float4 divc4(float4 v, float d, float r, int fast) {
 // rounding, 53 >= 2*24+2), the same result div_c gives -- again without a
 // per-lane branch.  Keeping range tests off the per-lane path leaves the
 // group's independent lanes free to interleave.
-template <int K>
-__device__ __forceinline__ void div_group(float4 (&v)[K], const float (&d)[K], const float (&r)[K], int fast) {
+template <int K, int Q>
+__device__ __forceinline__ void div_group(Vq<Q> (&v)[K], const float (&d)[K], const float (&r)[K], int fast) {
   bool ok = fast != 0;
 #pragma unroll
-  for (int k = 0; k < K; ++k) ok = ok & mk_ok(v[k].x) & mk_ok(v[k].y) & mk_ok(v[k].z) & mk_ok(v[k].w);
+  for (int k = 0; k < K; ++k)
+#pragma unroll
+    for (int e = 0; e < Q; ++e) ok = ok & mk_ok(g4(v[k], e));
   if (ok) {
 #pragma unroll
     for (int k = 0; k < K; ++k)
-      v[k] = make_float4(mk_div(v[k].x, d[k], r[k]), mk_div(v[k].y, d[k], r[k]), mk_div(v[k].z, d[k], r[k]),
-                         mk_div(v[k].w, d[k], r[k]));
+#pragma unroll
+      for (int e = 0; e < Q; ++e) s4(v[k], e, mk_div(g4(v[k], e), d[k], r[k]));
   } else {
 #pragma unroll
     for (int k = 0; k < K; ++k)
-      v[k] = make_float4(dd_div(v[k].x, d[k]), dd_div(v[k].y, d[k]), dd_div(v[k].z, d[k]), dd_div(v[k].w, d[k]));
+#pragma unroll
+      for (int e = 0; e < Q; ++e) s4(v[k], e, dd_div(g4(v[k], e), d[k]));
   }
 }
 
-// exact mode divides the stencil sum by the spacing; fast mode folded it into c
-template <bool EX>
-__device__ __forceinline__ float4 dv4(float4 v, float d, float r, int fast) {
-  return EX ? divc4(v, d, r, fast) : v;
-}
 // division by a per-cell positive value: exact, or __fdividef in fast mode
 template <bool EX>
 __device__ __forceinline__ float dvv(float x, float d) {
   return EX ? div_v(x, d) : __fdividef(x, d);
-}
-
-// one CPML memory-variable update of a single cell (psi in place)
-template <bool EX>
-__device__ __forceinline__ float pml1(float* m, float b, float a, float kk, float d) {
-  const float psi = b * (*m) + a * d;
-  *m = psi;
-  return dvv<EX>(d, kk) + psi;
 }
 
 // CPML on a quad: x and y slabs are per plane / per row, z per cell.
@@ -198,14 +216,15 @@ struct QuadPml {
 };
 
 // Memory variables of one quad on the slabs it lies in, components
-// c0 .. c0+2 of each axis: x and y slab rows as float4, z slab per cell.
+// c0 .. c0+2 of each axis: x and y slab rows as vectors, z slab per cell.
 // quad_mem_load issues every load before any update, so the latencies of the
 // up to nine rows overlap instead of forming one load-update-store chain per
 // component and axis; quad_mem_store writes them back after the updates.
+template <int Q>
 struct QuadMem {
-  float4 x[3], y[3];
-  float z[3][4];
-  int zk[4];
+  Vq<Q> x[3], y[3];
+  float z[3][Q];
+  int zk[Q];
 };
 
 __device__ __forceinline__ float* memx_ptr(const P3<float>& p, const QuadPml& q, int comp) {
@@ -218,36 +237,38 @@ __device__ __forceinline__ float* memz_ptr(const P3<float>& p, const QuadPml& q,
   return p.mem[2] + comp * p.mcomp[2] + ((size_t)q.i * p.ny + q.j) * p.sn[2] + zk;
 }
 
-__device__ __forceinline__ void quad_mem_load(const P3<float>& p, const QuadPml& q, int c0, QuadMem& m) {
+template <int Q>
+__device__ __forceinline__ void quad_mem_load(const P3<float>& p, const QuadPml& q, int c0, QuadMem<Q>& m) {
 #pragma unroll
-  for (int e = 0; e < 4; ++e) m.zk[e] = q.k + e < p.nz ? slab_index(q.k + e, p.nz, p.lo[2], p.hi[2]) : -1;
+  for (int e = 0; e < Q; ++e) m.zk[e] = q.k + e < p.nz ? slab_index(q.k + e, p.nz, p.lo[2], p.hi[2]) : -1;
   if (q.xi >= 0) {
 #pragma unroll
-    for (int c = 0; c < 3; ++c) m.x[c] = ld4(memx_ptr(p, q, c0 + c));
+    for (int c = 0; c < 3; ++c) m.x[c] = ldq<Q>(memx_ptr(p, q, c0 + c));
   }
   if (q.yj >= 0) {
 #pragma unroll
-    for (int c = 0; c < 3; ++c) m.y[c] = ld4(memy_ptr(p, q, c0 + c));
+    for (int c = 0; c < 3; ++c) m.y[c] = ldq<Q>(memy_ptr(p, q, c0 + c));
   }
 #pragma unroll
-  for (int e = 0; e < 4; ++e)
+  for (int e = 0; e < Q; ++e)
     if (m.zk[e] >= 0) {
 #pragma unroll
       for (int c = 0; c < 3; ++c) m.z[c][e] = *memz_ptr(p, q, c0 + c, m.zk[e]);
     }
 }
 
-__device__ __forceinline__ void quad_mem_store(const P3<float>& p, const QuadPml& q, int c0, const QuadMem& m) {
+template <int Q>
+__device__ __forceinline__ void quad_mem_store(const P3<float>& p, const QuadPml& q, int c0, const QuadMem<Q>& m) {
   if (q.xi >= 0) {
 #pragma unroll
-    for (int c = 0; c < 3; ++c) st4(memx_ptr(p, q, c0 + c), m.x[c]);
+    for (int c = 0; c < 3; ++c) stq<Q>(memx_ptr(p, q, c0 + c), m.x[c]);
   }
   if (q.yj >= 0) {
 #pragma unroll
-    for (int c = 0; c < 3; ++c) st4(memy_ptr(p, q, c0 + c), m.y[c]);
+    for (int c = 0; c < 3; ++c) stq<Q>(memy_ptr(p, q, c0 + c), m.y[c]);
   }
 #pragma unroll
-  for (int e = 0; e < 4; ++e)
+  for (int e = 0; e < Q; ++e)
     if (m.zk[e] >= 0) {
 #pragma unroll
       for (int c = 0; c < 3; ++c) *memz_ptr(p, q, c0 + c, m.zk[e]) = m.z[c][e];
@@ -256,9 +277,9 @@ __device__ __forceinline__ void quad_mem_store(const P3<float>& p, const QuadPml
 
 // CPML of one derivative quad d on axis AX from the preloaded memory
 // variables (component c of m), updated in place
-template <int AX, bool EX>
+template <int AX, bool EX, int Q>
 __device__ __forceinline__ void pml_quad_m(const P3<float>& p, const QuadPml& q, int c, int half, const int* pm,
-                                           float4& d, QuadMem& m) {
+                                           Vq<Q>& d, QuadMem<Q>& m) {
   const float* cf = p.cf[AX];
   const int n = AX == 0 ? p.nx : AX == 1 ? p.ny : p.nz;
   const int ob = half ? CBH : CB, oa = half ? CAH : CA, ok = half ? CKH : CK;
@@ -267,9 +288,9 @@ __device__ __forceinline__ void pml_quad_m(const P3<float>& p, const QuadPml& q,
     if (si < 0) return;
     const int idx = AX == 0 ? q.i : q.j;
     const float b = __ldg(cf + ob * n + idx), a = __ldg(cf + oa * n + idx), kk = __ldg(cf + ok * n + idx);
-    float4& o = AX == 0 ? m.x[c] : m.y[c];
+    Vq<Q>& o = AX == 0 ? m.x[c] : m.y[c];
 #pragma unroll
-    for (int e = 0; e < 4; ++e) {
+    for (int e = 0; e < Q; ++e) {
       if (!pm[e]) continue;
       const float de = g4(d, e);
       const float psi = b * g4(o, e) + a * de;
@@ -278,7 +299,7 @@ __device__ __forceinline__ void pml_quad_m(const P3<float>& p, const QuadPml& q,
     }
   } else {
 #pragma unroll
-    for (int e = 0; e < 4; ++e) {
+    for (int e = 0; e < Q; ++e) {
       if (!pm[e] || m.zk[e] < 0) continue;
       const int kk_ = q.k + e;
       const float b = __ldg(cf + ob * n + kk_), a = __ldg(cf + oa * n + kk_), kk = __ldg(cf + ok * n + kk_);
@@ -290,49 +311,14 @@ __device__ __forceinline__ void pml_quad_m(const P3<float>& p, const QuadPml& q,
   }
 }
 
-template <int AX, bool EX>
-__device__ __forceinline__ void pml_quad(const P3<float>& p, const QuadPml& q, int comp, int half, const int* pm,
-                                         float4& d) {
-  const float* cf = p.cf[AX];
-  const int n = AX == 0 ? p.nx : AX == 1 ? p.ny : p.nz;
-  const int ob = half ? CBH : CB, oa = half ? CAH : CA, ok = half ? CKH : CK;
-  if (AX == 0 || AX == 1) {
-    const int idx = AX == 0 ? q.i : q.j;
-    const int si = AX == 0 ? q.xi : q.yj;
-    if (si < 0) return;
-    const float b = cf[ob * n + idx], a = cf[oa * n + idx], kk = cf[ok * n + idx];
-    float* m = AX == 0 ? p.mem[0] + comp * p.mcomp[0] + ((size_t)si * p.ny + q.j) * p.nz + q.k
-                       : p.mem[1] + comp * p.mcomp[1] + ((size_t)q.i * p.sn[1] + si) * p.nz + q.k;
-    float4 o = ld4(m);
-#pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      if (!pm[e]) continue;
-      const float de = g4(d, e);
-      const float psi = b * g4(o, e) + a * de;
-      s4(o, e, psi);
-      s4(d, e, dvv<EX>(de, kk) + psi);
-    }
-    st4(m, o);
-  } else {
-#pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      const int kk_ = q.k + e;
-      const int zk = slab_index(kk_, p.nz, p.lo[2], p.hi[2]);
-      if (!pm[e] || zk < 0) continue;
-      float* m = p.mem[2] + comp * p.mcomp[2] + ((size_t)q.i * p.ny + q.j) * p.sn[2] + zk;
-      s4(d, e, pml1<EX>(m, cf[ob * n + kk_], cf[oa * n + kk_], cf[ok * n + kk_], g4(d, e)));
-    }
-  }
-}
-
 // ---------------------------------------------------------------------------
 // velocity pass
 // ---------------------------------------------------------------------------
-template <int N, int TY, int D, bool TENSOR, bool EX>
-__global__ void __launch_bounds__(TY * 8, 3)
+template <int N, int TY, int D, bool TENSOR, bool EX, int Q>
+__global__ void __launch_bounds__(SG<N, TY, D, Q>::NT, SG<N, TY, D, Q>::MINB)
 k3s_velocity(const __grid_constant__ P3<float> p, const __grid_constant__ StagedMaps maps,
              const __grid_constant__ StagedArgs a, int it, int force_here) {
-  using G = SG<N, TY, D>;
+  using G = SG<N, TY, D, Q>;
   extern __shared__ __align__(128) float sm[];
   uint64_t* bars = reinterpret_cast<uint64_t*>(sm + G::V_FLOATS);
   const int tid = threadIdx.x;
@@ -356,7 +342,7 @@ k3s_velocity(const __grid_constant__ P3<float> p, const __grid_constant__ Staged
   const int fast = p.fast_div;
   const float rdx = p.rd[0], rdy = p.rd[1], rdz = p.rd[2];
   const float wf = force_here ? p.wav[it] : 0.f;
-  const int r = tid >> 3, cq = tid & 7;
+  const int r = tid / G::CQ, cq = tid % G::CQ;
   constexpr int PXX = G::pad(G::B_XX), PY = G::pad(G::B_Y), PZ = G::pad(G::B_Z), PYZ = G::pad(G::B_YZ),
                 PR = G::pad(G::B_R);
   auto sxx_p = [&](int pl) { return sm + G::V_XX + rslot(pl, G::RX) * PXX; };
@@ -366,10 +352,10 @@ k3s_velocity(const __grid_constant__ P3<float> p, const __grid_constant__ Staged
   auto syz_p = [&](int pl) { return sm + G::V_YZ + rslot(pl, G::R1) * PYZ; };
   auto szz_p = [&](int pl) { return sm + G::V_ZZ + rslot(pl, G::R1) * PZ; };
   auto rho_p = [&](int pl) { return sm + G::V_R + rslot(pl, G::R2) * PR; };
-  const int o_xx = r * G::TZ + 4 * cq;                 // sxx, rho boxes
-  const int o_y = (r + N) * G::TZ + 4 * cq;            // sxy, syy boxes
-  const int o_z = r * G::WZ + G::H4 + 4 * cq;          // sxz, szz boxes
-  const int o_yz = (r + N) * G::WZ + G::H4 + 4 * cq;   // syz box
+  const int o_xx = r * G::TZ + Q * cq;                 // sxx, rho boxes
+  const int o_y = (r + N) * G::TZ + Q * cq;            // sxy, syy boxes
+  const int o_z = r * G::WZ + G::H4 + Q * cq;          // sxz, szz boxes
+  const int o_yz = (r + N) * G::WZ + G::H4 + Q * cq;   // syz box
 
   const int units = a.tiles_y * a.tiles_z * a.chunks;
   uint32_t g = 0;
@@ -381,7 +367,7 @@ k3s_velocity(const __grid_constant__ P3<float> p, const __grid_constant__ Staged
     const int j0 = tyi * TY, k0 = tzi * G::TZ;
     const int x0 = max(ch * a.chunk_len, N), x1 = min(min((ch + 1) * a.chunk_len, nx - N), nx);
     if (x0 >= x1) continue;
-    const int j = j0 + r, k = k0 + 4 * cq;
+    const int j = j0 + r, k = k0 + Q * cq;
     const bool jin = j < ny, kin = k < nz;
     // tile-level interior test (y and z): every cell inside every update
     // range and outside the CPML slabs
@@ -390,9 +376,9 @@ k3s_velocity(const __grid_constant__ P3<float> p, const __grid_constant__ Staged
     const int yj = jin ? slab_index(j, ny, p.lo[1], p.hi[1]) : -1;
     const uint8_t fy = jin ? p.fl[1][j] : 0;
     bool zslab = false;
-    uint8_t fz[4];
+    uint8_t fz[Q];
 #pragma unroll
-    for (int e = 0; e < 4; ++e) {
+    for (int e = 0; e < Q; ++e) {
       const int kk = k + e;
       fz[e] = kk < nz ? p.fl[2][kk] : 0;
       zslab = zslab || (kk < nz && slab_index(kk, nz, p.lo[2], p.hi[2]) >= 0);
@@ -448,82 +434,82 @@ k3s_velocity(const __grid_constant__ P3<float> p, const __grid_constant__ Staged
         const float* r0 = rho_p(i);
         const float* r1 = rho_p(i + 1);
         const size_t gi = (size_t)i * nyz + (size_t)j * nz + k;
-        const float4 rc = ld4(r0 + o_xx), rn = ld4(r0 + o_xx + G::TZ);
+        const Vq<Q> rc = ldq<Q>(r0 + o_xx), rn = ldq<Q>(r0 + o_xx + G::TZ);
         // derivatives of the three components (Dx3fm/Dy3bm/Dz3bm etc.)
-        float4 dv[9] = {dxq<N, EX>(pxx, o_xx, cx),
-                        dyq<N, false, EX>(sxy_p(i), o_y, G::TZ, cy),
-                        dzq<N, false, EX>(sxz_p(i), o_z, cz),
-                        dxq<N, EX>(pxy, o_y, cx),
-                        dyq<N, true, EX>(syy_p(i), o_y, G::TZ, cy),
-                        dzq<N, false, EX>(syz_p(i), o_yz, cz),
-                        dxq<N, EX>(pxz, o_z, cx),
-                        dyq<N, false, EX>(syz_p(i), o_yz, G::WZ, cy),
-                        dzq<N, true, EX>(szz_p(i), o_z, cz)};
+        Vq<Q> dv[9] = {dxq<N, EX, Q>(pxx, o_xx, cx),
+                        dyq<N, false, EX, Q>(sxy_p(i), o_y, G::TZ, cy),
+                        dzq<N, false, EX, Q>(sxz_p(i), o_z, cz),
+                        dxq<N, EX, Q>(pxy, o_y, cx),
+                        dyq<N, true, EX, Q>(syy_p(i), o_y, G::TZ, cy),
+                        dzq<N, false, EX, Q>(syz_p(i), o_yz, cz),
+                        dxq<N, EX, Q>(pxz, o_z, cx),
+                        dyq<N, false, EX, Q>(syz_p(i), o_yz, G::WZ, cy),
+                        dzq<N, true, EX, Q>(szz_p(i), o_z, cz)};
         if (EX) {
           const float hd[9] = {dx, dy, dz, dx, dy, dz, dx, dy, dz};
           const float hr[9] = {rdx, rdy, rdz, rdx, rdy, rdz, rdx, rdy, rdz};
-          div_group<9>(dv, hd, hr, fast);
+          div_group<9, Q>(dv, hd, hr, fast);
         }
-        float4 a1 = dv[0], a2 = dv[1], a3 = dv[2], b1 = dv[3], b2 = dv[4], b3 = dv[5], c1 = dv[6], c2 = dv[7],
+        Vq<Q> a1 = dv[0], a2 = dv[1], a3 = dv[2], b1 = dv[3], b2 = dv[4], b3 = dv[5], c1 = dv[6], c2 = dv[7],
                c3 = dv[8];
-        float4 vx = ldg4(p.f[0] + gi), vy = ldg4(p.f[1] + gi), vz = ldg4(p.f[2] + gi);
+        Vq<Q> vx = ldgq<Q>(p.f[0] + gi), vy = ldgq<Q>(p.f[1] + gi), vz = ldgq<Q>(p.f[2] + gi);
         if (interior) {
-          const float4 r1c = ld4(r1 + o_xx), r1n = ld4(r1 + o_xx + G::TZ);
+          const Vq<Q> r1c = ldq<Q>(r1 + o_xx), r1n = ldq<Q>(r1 + o_xx + G::TZ);
           // numerators and densities of the 12 updates, then their quotients
           // as one group (see div_group: no per-lane range branch)
-          float tn[12], td[12];
+          float tn[3 * Q], td[3 * Q];
 #pragma unroll
-          for (int e = 0; e < 4; ++e) {
+          for (int e = 0; e < Q; ++e) {
             const float rce = g4(rc, e), rne = g4(rn, e);
             tn[e] = (g4(a1, e) + g4(a3, e) + g4(a2, e)) * dt;
             td[e] = rce;
-            tn[4 + e] = (g4(b1, e) + g4(b2, e) + g4(b3, e)) * dt;
-            td[4 + e] = 0.5f * (rce + rne);
+            tn[Q + e] = (g4(b1, e) + g4(b2, e) + g4(b3, e)) * dt;
+            td[Q + e] = 0.5f * (rce + rne);
             const float sum = TENSOR ? (g4(c1, e) + g4(c2, e) + g4(c3, e)) : (g4(c3, e) + g4(c1, e) + g4(c2, e));
-            tn[8 + e] = sum * dt;
-            td[8 + e] = 0.25f * (rce + rne + g4(r1n, e) + g4(r1c, e));
+            tn[2 * Q + e] = sum * dt;
+            td[2 * Q + e] = 0.25f * (rce + rne + g4(r1n, e) + g4(r1c, e));
           }
           if (EX) {
             bool okq = true;
 #pragma unroll
-            for (int q = 0; q < 12; ++q) okq = okq & mk_ok(tn[q]);
+            for (int q = 0; q < 3 * Q; ++q) okq = okq & mk_ok(tn[q]);
             if (okq) {
 #pragma unroll
-              for (int q = 0; q < 12; ++q) tn[q] = tn[q] == 0.f ? tn[q] : __fdiv_rn(tn[q], td[q]);
+              for (int q = 0; q < 3 * Q; ++q) tn[q] = tn[q] == 0.f ? tn[q] : __fdiv_rn(tn[q], td[q]);
             } else {
 #pragma unroll
-              for (int q = 0; q < 12; ++q) tn[q] = dd_div(tn[q], td[q]);
+              for (int q = 0; q < 3 * Q; ++q) tn[q] = dd_div(tn[q], td[q]);
             }
           } else {
 #pragma unroll
-            for (int q = 0; q < 12; ++q) tn[q] = __fdividef(tn[q], td[q]);
+            for (int q = 0; q < 3 * Q; ++q) tn[q] = __fdividef(tn[q], td[q]);
           }
 #pragma unroll
-          for (int e = 0; e < 4; ++e) {
+          for (int e = 0; e < Q; ++e) {
             s4(vx, e, g4(vx, e) + tn[e]);
-            s4(vy, e, g4(vy, e) + tn[4 + e]);
-            s4(vz, e, g4(vz, e) + tn[8 + e]);
+            s4(vy, e, g4(vy, e) + tn[Q + e]);
+            s4(vz, e, g4(vz, e) + tn[2 * Q + e]);
           }
         } else {
           QuadPml q{xi, yj, i, j, k, p.fl[0][i], fy};
           const bool anyslab = xi >= 0 || yj >= 0 || zslab;
-          QuadMem mm;
+          QuadMem<Q> mm;
           if (anyslab) quad_mem_load(p, q, 0, mm);
           // vx (x half, y int, z int): i in [N, nx-N-1), j in [N+1, ny-N), k in [N+1, nz-N)
           if (i < nx - N - 1 && j >= N + 1 && j < ny - N) {
-            int pm[4], upd[4];
+            int pm[Q], upd[Q];
 #pragma unroll
-            for (int e = 0; e < 4; ++e) {
+            for (int e = 0; e < Q; ++e) {
               upd[e] = k + e >= N + 1 && k + e < nz - N;
               pm[e] = upd[e] && ((q.fx & 2) || (fy & 1) || (fz[e] & 1));
             }
             if (anyslab) {
-              pml_quad_m<0, EX>(p, q, 0, 1, pm, a1, mm);
-              pml_quad_m<1, EX>(p, q, 0, 0, pm, a2, mm);
-              pml_quad_m<2, EX>(p, q, 0, 0, pm, a3, mm);
+              pml_quad_m<0, EX, Q>(p, q, 0, 1, pm, a1, mm);
+              pml_quad_m<1, EX, Q>(p, q, 0, 0, pm, a2, mm);
+              pml_quad_m<2, EX, Q>(p, q, 0, 0, pm, a3, mm);
             }
 #pragma unroll
-            for (int e = 0; e < 4; ++e)
+            for (int e = 0; e < Q; ++e)
               if (upd[e]) {
                 const float t = (g4(a1, e) + g4(a3, e) + g4(a2, e)) * dt;
                 s4(vx, e, g4(vx, e) + dvv<EX>(t, g4(rc, e)));
@@ -531,19 +517,19 @@ k3s_velocity(const __grid_constant__ P3<float> p, const __grid_constant__ Staged
           }
           // vy (x int, y half, z int): i in [N+1, nx-N), j in [N, ny-N-1), k in [N+1, nz-N)
           if (i >= N + 1 && j < ny - N - 1 && j >= N) {
-            int pm[4], upd[4];
+            int pm[Q], upd[Q];
 #pragma unroll
-            for (int e = 0; e < 4; ++e) {
+            for (int e = 0; e < Q; ++e) {
               upd[e] = k + e >= N + 1 && k + e < nz - N;
               pm[e] = upd[e] && ((q.fx & 1) || (fy & 2) || (fz[e] & 1));
             }
             if (anyslab) {
-              pml_quad_m<0, EX>(p, q, 1, 0, pm, b1, mm);
-              pml_quad_m<1, EX>(p, q, 1, 1, pm, b2, mm);
-              pml_quad_m<2, EX>(p, q, 1, 0, pm, b3, mm);
+              pml_quad_m<0, EX, Q>(p, q, 1, 0, pm, b1, mm);
+              pml_quad_m<1, EX, Q>(p, q, 1, 1, pm, b2, mm);
+              pml_quad_m<2, EX, Q>(p, q, 1, 0, pm, b3, mm);
             }
 #pragma unroll
-            for (int e = 0; e < 4; ++e)
+            for (int e = 0; e < Q; ++e)
               if (upd[e]) {
                 const float rhy = 0.5f * (g4(rc, e) + g4(rn, e));
                 const float t = (g4(b1, e) + g4(b2, e) + g4(b3, e)) * dt;
@@ -552,20 +538,20 @@ k3s_velocity(const __grid_constant__ P3<float> p, const __grid_constant__ Staged
           }
           // vz (x int, y int, z half): i in [N+1, nx-N), j in [N+1, ny-N), k in [N, nz-N-1)
           if (i >= N + 1 && j >= N + 1 && j < ny - N) {
-            const float4 r1c = ld4(r1 + o_xx), r1n = ld4(r1 + o_xx + G::TZ);
-            int pm[4], upd[4];
+            const Vq<Q> r1c = ldq<Q>(r1 + o_xx), r1n = ldq<Q>(r1 + o_xx + G::TZ);
+            int pm[Q], upd[Q];
 #pragma unroll
-            for (int e = 0; e < 4; ++e) {
+            for (int e = 0; e < Q; ++e) {
               upd[e] = k + e >= N && k + e < nz - N - 1;
               pm[e] = upd[e] && ((q.fx & 1) || (fy & 1) || (fz[e] & 2));
             }
             if (anyslab) {
-              pml_quad_m<0, EX>(p, q, 2, 0, pm, c1, mm);
-              pml_quad_m<1, EX>(p, q, 2, 0, pm, c2, mm);
-              pml_quad_m<2, EX>(p, q, 2, 1, pm, c3, mm);
+              pml_quad_m<0, EX, Q>(p, q, 2, 0, pm, c1, mm);
+              pml_quad_m<1, EX, Q>(p, q, 2, 0, pm, c2, mm);
+              pml_quad_m<2, EX, Q>(p, q, 2, 1, pm, c3, mm);
             }
 #pragma unroll
-            for (int e = 0; e < 4; ++e)
+            for (int e = 0; e < Q; ++e)
               if (upd[e]) {
                 const float r4 = 0.25f * (g4(rc, e) + g4(rn, e) + g4(r1n, e) + g4(r1c, e));
                 const float sum =
@@ -576,15 +562,15 @@ k3s_velocity(const __grid_constant__ P3<float> p, const __grid_constant__ Staged
           }
           if (anyslab) quad_mem_store(p, q, 0, mm);
           // point force (Elastic3D_SSG_CPML.py:245), after the update
-          if (force_here && i == p.si && j == p.sj && p.sk >= k && p.sk < k + 4) {
+          if (force_here && i == p.si && j == p.sj && p.sk >= k && p.sk < k + Q) {
             const int e = p.sk - k;
             const float t = dt * wf;
             s4(vz, e, g4(vz, e) + dvv<EX>(t, g4(rc, e)));
           }
         }
-        st4(p.f[0] + gi, vx);
-        st4(p.f[1] + gi, vy);
-        st4(p.f[2] + gi, vz);
+        stq<Q>(p.f[0] + gi, vx);
+        stq<Q>(p.f[1] + gi, vy);
+        stq<Q>(p.f[2] + gi, vz);
       }
       __syncthreads();
       if (tid == 0 && i + D + 1 < x1) issue(i + D + 1, false, g % (D + 1));
@@ -597,11 +583,11 @@ k3s_velocity(const __grid_constant__ P3<float> p, const __grid_constant__ Staged
 // ---------------------------------------------------------------------------
 // stress pass
 // ---------------------------------------------------------------------------
-template <int N, int TY, int D, bool EX>
-__global__ void __launch_bounds__(TY * 8, 3)
+template <int N, int TY, int D, bool EX, int Q>
+__global__ void __launch_bounds__(SG<N, TY, D, Q>::NT, SG<N, TY, D, Q>::MINB)
 k3s_stress(const __grid_constant__ P3<float> p, const __grid_constant__ StagedMaps maps,
            const __grid_constant__ StagedArgs a, int it, int inject_next, int gather) {
-  using G = SG<N, TY, D>;
+  using G = SG<N, TY, D, Q>;
   extern __shared__ __align__(128) float sm[];
   uint64_t* bars = reinterpret_cast<uint64_t*>(sm + G::S_FLOATS);
   const int tid = threadIdx.x;
@@ -629,16 +615,16 @@ k3s_stress(const __grid_constant__ P3<float> p, const __grid_constant__ StagedMa
   const int fast = p.fast_div;
   const float rdx = p.rd[0], rdy = p.rd[1], rdz = p.rd[2];
   const float wn = inject_next ? p.wav[it + 1] : 0.f;
-  const int r = tid >> 3, cq = tid & 7;
+  const int r = tid / G::CQ, cq = tid % G::CQ;
   constexpr int PYZ = G::pad(G::B_YZ), PL = G::pad(G::B_L), PM = G::pad(G::B_M);
   auto vx_p = [&](int pl) { return sm + G::S_VX + rslot(pl, G::RX) * PYZ; };
   auto vy_p = [&](int pl) { return sm + G::S_VY + rslot(pl, G::RX) * PYZ; };
   auto vz_p = [&](int pl) { return sm + G::S_VZ + rslot(pl, G::RX) * PYZ; };
   auto lam_p = [&](int pl) { return sm + G::S_L + rslot(pl, G::R2) * PL; };
   auto mu_p = [&](int pl) { return sm + G::S_M + rslot(pl, G::R2) * PM; };
-  const int o_v = (r + N) * G::WZ + G::H4 + 4 * cq;
-  const int o_l = r * G::TZ + 4 * cq;
-  const int o_m = r * G::WM + 4 * cq;
+  const int o_v = (r + N) * G::WZ + G::H4 + Q * cq;
+  const int o_l = r * G::TZ + Q * cq;
+  const int o_m = r * G::WM + Q * cq;
 
   const int units = a.tiles_y * a.tiles_z * a.chunks;
   uint32_t g = 0;
@@ -650,16 +636,16 @@ k3s_stress(const __grid_constant__ P3<float> p, const __grid_constant__ StagedMa
     const int j0 = tyi * TY, k0 = tzi * G::TZ;
     const int x0 = max(ch * a.chunk_len, N), x1 = min((ch + 1) * a.chunk_len, nx - N);
     if (x0 >= x1) continue;
-    const int j = j0 + r, k = k0 + 4 * cq;
+    const int j = j0 + r, k = k0 + Q * cq;
     const bool jin = j < ny, kin = k < nz;
     const bool tile_in = j0 >= N + 1 && j0 + TY <= ny - N - 1 && k0 >= N + 1 && k0 + G::TZ <= nz - N - 1 &&
                          j0 >= p.lo[1] && j0 + TY <= ny - p.hi[1] && k0 >= p.lo[2] && k0 + G::TZ <= nz - p.hi[2];
     const int yj = jin ? slab_index(j, ny, p.lo[1], p.hi[1]) : -1;
     const uint8_t fy = jin ? p.fl[1][j] : 0;
     bool zslab = false;
-    uint8_t fz[4];
+    uint8_t fz[Q];
 #pragma unroll
-    for (int e = 0; e < 4; ++e) {
+    for (int e = 0; e < Q; ++e) {
       const int kk = k + e;
       fz[e] = kk < nz ? p.fl[2][kk] : 0;
       zslab = zslab || (kk < nz && slab_index(kk, nz, p.lo[2], p.hi[2]) >= 0);
@@ -698,7 +684,7 @@ k3s_stress(const __grid_constant__ P3<float> p, const __grid_constant__ StagedMa
         break;
       }
       const int xi = slab_index(i, nx, p.lo[0], p.hi[0]);
-      const bool src = inject_next && i == p.si && p.sj == j && p.sk >= k && p.sk < k + 4;
+      const bool src = inject_next && i == p.si && p.sj == j && p.sk >= k && p.sk < k + Q;
       const bool interior = tile_in && i >= N + 1 && i < nx - N - 1 && xi < 0 &&
                             !(inject_next && i == p.si && p.sj >= j0 && p.sj < j0 + TY && p.sk >= k0 &&
                               p.sk < k0 + G::TZ);
@@ -716,33 +702,35 @@ k3s_stress(const __grid_constant__ P3<float> p, const __grid_constant__ StagedMa
         const float* vyi = vy_p(i);
         const float* vzi = vz_p(i);
         const size_t gi = (size_t)i * nyz + (size_t)j * nz + k;
-        float4 sxx = ldg4(p.f[3] + gi), syy = ldg4(p.f[4] + gi), szz = ldg4(p.f[5] + gi);
-        float4 sxy = ldg4(p.f[6] + gi), sxz = ldg4(p.f[7] + gi), syz = ldg4(p.f[8] + gi);
-        const float4 l0 = ld4(lam_p(i) + o_l), l1 = ld4(lam_p(i + 1) + o_l);
+        Vq<Q> sxx = ldgq<Q>(p.f[3] + gi), syy = ldgq<Q>(p.f[4] + gi), szz = ldgq<Q>(p.f[5] + gi);
+        Vq<Q> sxy = ldgq<Q>(p.f[6] + gi), sxz = ldgq<Q>(p.f[7] + gi), syz = ldgq<Q>(p.f[8] + gi);
+        const Vq<Q> l0 = ldq<Q>(lam_p(i) + o_l), l1 = ldq<Q>(lam_p(i + 1) + o_l);
         const float* m0p = mu_p(i);
-        const float4 u0 = ld4(m0p + o_m), u1 = ld4(mu_p(i + 1) + o_m), unj = ld4(m0p + o_m + G::WM);
-        const float4 u0s = ld4(m0p + o_m + 4);  // mu[k+4 .. k+7] for the k+1 neighbour
-        const float unk[4] = {u0.y, u0.z, u0.w, u0s.x};
+        const Vq<Q> u0 = ldq<Q>(m0p + o_m), u1 = ldq<Q>(mu_p(i + 1) + o_m), unj = ldq<Q>(m0p + o_m + G::WM);
+        float unk[Q];  // mu[k+1 .. k+Q] for the k+1 neighbours
+#pragma unroll
+        for (int e = 0; e + 1 < Q; ++e) unk[e] = g4(u0, e + 1);
+        unk[Q - 1] = m0p[o_m + Q];
         // derivatives: dvx/dx dvy/dy dvz/dz dvy/dx dvx/dy dvz/dx dvx/dz dvz/dy dvy/dz
-        float4 dv[9] = {dxq<N, EX>(pvx, o_v, cx),
-                        dyq<N, false, EX>(vyi, o_v, G::WZ, cy),
-                        dzq<N, false, EX>(vzi, o_v, cz),
-                        dxq<N, EX>(pvy, o_v, cx),
-                        dyq<N, true, EX>(vxi, o_v, G::WZ, cy),
-                        dxq<N, EX>(pvz, o_v, cx),
-                        dzq<N, true, EX>(vxi, o_v, cz),
-                        dyq<N, true, EX>(vzi, o_v, G::WZ, cy),
-                        dzq<N, true, EX>(vyi, o_v, cz)};
+        Vq<Q> dv[9] = {dxq<N, EX, Q>(pvx, o_v, cx),
+                        dyq<N, false, EX, Q>(vyi, o_v, G::WZ, cy),
+                        dzq<N, false, EX, Q>(vzi, o_v, cz),
+                        dxq<N, EX, Q>(pvy, o_v, cx),
+                        dyq<N, true, EX, Q>(vxi, o_v, G::WZ, cy),
+                        dxq<N, EX, Q>(pvz, o_v, cx),
+                        dzq<N, true, EX, Q>(vxi, o_v, cz),
+                        dyq<N, true, EX, Q>(vzi, o_v, G::WZ, cy),
+                        dzq<N, true, EX, Q>(vyi, o_v, cz)};
         if (EX) {
           const float hd[9] = {dx, dy, dz, dx, dy, dx, dz, dy, dz};
           const float hr[9] = {rdx, rdy, rdz, rdx, rdy, rdx, rdz, rdy, rdz};
-          div_group<9>(dv, hd, hr, fast);
+          div_group<9, Q>(dv, hd, hr, fast);
         }
-        float4 e1 = dv[0], e2 = dv[1], e3 = dv[2], f1 = dv[3], f2 = dv[4], h1 = dv[5], h2 = dv[6], q1 = dv[7],
+        Vq<Q> e1 = dv[0], e2 = dv[1], e3 = dv[2], f1 = dv[3], f2 = dv[4], h1 = dv[5], h2 = dv[6], q1 = dv[7],
                q2 = dv[8];
         if (interior) {
 #pragma unroll
-          for (int e = 0; e < 4; ++e) {
+          for (int e = 0; e < Q; ++e) {
             const float lhx = 0.5f * (g4(l0, e) + g4(l1, e));
             const float mhx = 0.5f * (g4(u0, e) + g4(u1, e));
             const float lpm = lhx + 2.0f * mhx;
@@ -761,23 +749,23 @@ k3s_stress(const __grid_constant__ P3<float> p, const __grid_constant__ StagedMa
         } else {
           QuadPml q{xi, yj, i, j, k, p.fl[0][i], fy};
           const bool anyslab = xi >= 0 || yj >= 0 || zslab;
-          QuadMem mm;
+          QuadMem<Q> mm;
           if (anyslab) quad_mem_load(p, q, 3, mm);
           // normal stresses: i, j, k in [N+1, n-N)
           if (i >= N + 1 && j >= N + 1 && j < ny - N) {
-            int pm[4], upd[4];
+            int pm[Q], upd[Q];
 #pragma unroll
-            for (int e = 0; e < 4; ++e) {
+            for (int e = 0; e < Q; ++e) {
               upd[e] = k + e >= N + 1 && k + e < nz - N;
               pm[e] = upd[e] && ((q.fx | fy | fz[e]) & 1);
             }
             if (anyslab) {
-              pml_quad_m<0, EX>(p, q, 0, 0, pm, e1, mm);
-              pml_quad_m<1, EX>(p, q, 0, 0, pm, e2, mm);
-              pml_quad_m<2, EX>(p, q, 0, 0, pm, e3, mm);
+              pml_quad_m<0, EX, Q>(p, q, 0, 0, pm, e1, mm);
+              pml_quad_m<1, EX, Q>(p, q, 0, 0, pm, e2, mm);
+              pml_quad_m<2, EX, Q>(p, q, 0, 0, pm, e3, mm);
             }
 #pragma unroll
-            for (int e = 0; e < 4; ++e)
+            for (int e = 0; e < Q; ++e)
               if (upd[e]) {
                 const float lhx = 0.5f * (g4(l0, e) + g4(l1, e));
                 const float mhx = 0.5f * (g4(u0, e) + g4(u1, e));
@@ -790,18 +778,18 @@ k3s_stress(const __grid_constant__ P3<float> p, const __grid_constant__ StagedMa
           }
           // sxy (x half, y half, z int): i, j in [N+1, n-N), k in [N, nz-N)
           if (i >= N + 1 && j >= N + 1 && j < ny - N) {
-            int pm[4], upd[4];
+            int pm[Q], upd[Q];
 #pragma unroll
-            for (int e = 0; e < 4; ++e) {
+            for (int e = 0; e < Q; ++e) {
               upd[e] = k + e >= N && k + e < nz - N;
               pm[e] = upd[e] && ((q.fx & 2) || (fy & 2) || (fz[e] & 1));
             }
             if (anyslab) {
-              pml_quad_m<0, EX>(p, q, 1, 1, pm, f1, mm);
-              pml_quad_m<1, EX>(p, q, 1, 1, pm, f2, mm);
+              pml_quad_m<0, EX, Q>(p, q, 1, 1, pm, f1, mm);
+              pml_quad_m<1, EX, Q>(p, q, 1, 1, pm, f2, mm);
             }
 #pragma unroll
-            for (int e = 0; e < 4; ++e)
+            for (int e = 0; e < Q; ++e)
               if (upd[e]) {
                 const float u = g4(u0, e);
                 const float m4 = 0.25f * (g4(unj, e) + u + u + g4(u1, e));
@@ -810,18 +798,18 @@ k3s_stress(const __grid_constant__ P3<float> p, const __grid_constant__ StagedMa
           }
           // sxz (x half, y int, z half): i in [N, nx-N-1), j in [N, ny-N), k in [N, nz-N-1)
           if (i < nx - N - 1 && j >= N && j < ny - N) {
-            int pm[4], upd[4];
+            int pm[Q], upd[Q];
 #pragma unroll
-            for (int e = 0; e < 4; ++e) {
+            for (int e = 0; e < Q; ++e) {
               upd[e] = k + e >= N && k + e < nz - N - 1;
               pm[e] = upd[e] && ((q.fx & 2) || (fy & 1) || (fz[e] & 2));
             }
             if (anyslab) {
-              pml_quad_m<0, EX>(p, q, 2, 1, pm, h1, mm);
-              pml_quad_m<2, EX>(p, q, 1, 1, pm, h2, mm);
+              pml_quad_m<0, EX, Q>(p, q, 2, 1, pm, h1, mm);
+              pml_quad_m<2, EX, Q>(p, q, 1, 1, pm, h2, mm);
             }
 #pragma unroll
-            for (int e = 0; e < 4; ++e)
+            for (int e = 0; e < Q; ++e)
               if (upd[e]) {
                 const float u = g4(u0, e);
                 const float m4 = 0.25f * (u + g4(u1, e) + u + g4(unj, e));
@@ -830,18 +818,18 @@ k3s_stress(const __grid_constant__ P3<float> p, const __grid_constant__ StagedMa
           }
           // syz (x int, y half, z half): i in [N, nx-N), j in [N, ny-N-1), k in [N, nz-N-1)
           if (j >= N && j < ny - N - 1) {
-            int pm[4], upd[4];
+            int pm[Q], upd[Q];
 #pragma unroll
-            for (int e = 0; e < 4; ++e) {
+            for (int e = 0; e < Q; ++e) {
               upd[e] = k + e >= N && k + e < nz - N - 1;
               pm[e] = upd[e] && ((q.fx & 1) || (fy & 2) || (fz[e] & 2));
             }
             if (anyslab) {
-              pml_quad_m<1, EX>(p, q, 2, 1, pm, q1, mm);
-              pml_quad_m<2, EX>(p, q, 2, 1, pm, q2, mm);
+              pml_quad_m<1, EX, Q>(p, q, 2, 1, pm, q1, mm);
+              pml_quad_m<2, EX, Q>(p, q, 2, 1, pm, q2, mm);
             }
 #pragma unroll
-            for (int e = 0; e < 4; ++e)
+            for (int e = 0; e < Q; ++e)
               if (upd[e]) {
                 const float u = g4(u0, e);
                 const float m4 = 0.25f * (g4(unj, e) + u + unk[e] + u);
@@ -860,12 +848,12 @@ k3s_stress(const __grid_constant__ P3<float> p, const __grid_constant__ StagedMa
             s4(syz, e, g4(syz, e) + wn * p.mneg[5]);
           }
         }
-        st4(p.f[3] + gi, sxx);
-        st4(p.f[4] + gi, syy);
-        st4(p.f[5] + gi, szz);
-        st4(p.f[6] + gi, sxy);
-        st4(p.f[7] + gi, sxz);
-        st4(p.f[8] + gi, syz);
+        stq<Q>(p.f[3] + gi, sxx);
+        stq<Q>(p.f[4] + gi, syy);
+        stq<Q>(p.f[5] + gi, szz);
+        stq<Q>(p.f[6] + gi, sxy);
+        stq<Q>(p.f[7] + gi, sxz);
+        stq<Q>(p.f[8] + gi, syz);
       }
       __syncthreads();
       if (tid == 0 && i + D + 1 < x1) issue(i + D + 1, false, g % (D + 1));
@@ -904,7 +892,7 @@ static bool map3(CUtensorMap* m, const void* base, int nx, int ny, int nz, int b
 
 template <int N, int TY, int D>
 static bool staged_maps_t(const P3<float>& p, StagedMaps* vm, StagedMaps* sm_) {
-  using G = SG<N, TY, D>;
+  using G = SG<N, TY, D, 4>;  // box shapes do not depend on the cells per thread
   const int nx = p.nx, ny = p.ny, nz = p.nz;
   bool ok = true;
   // velocity pass: sxx sxy sxz syy syz szz rho
@@ -926,7 +914,7 @@ static bool staged_maps_t(const P3<float>& p, StagedMaps* vm, StagedMaps* sm_) {
 
 template <int N, int TY, int D>
 static StagedConfig staged_cfg_t() {
-  using G = SG<N, TY, D>;
+  using G = SG<N, TY, D, staged_q(true)>;
   return StagedConfig{N, TY, D, G::NT, G::V_BYTES, G::S_BYTES};
 }
 
@@ -954,23 +942,24 @@ template <int N, int TY, int D, bool EX>
 static cudaError_t staged_launch(bool tensor, const P3<float>& p, const StagedMaps& vm, const StagedMaps& smp,
                                  const StagedArgs& a, int grid, int it, bool force_here, bool inject_next,
                                  bool gather, cudaStream_t st) {
-  using G = SG<N, TY, D>;
+  constexpr int Q = staged_q(EX);
+  using G = SG<N, TY, D, Q>;
   static bool init = false;
   if (!init) {
-    cudaError_t e = cudaFuncSetAttribute(k3s_velocity<N, TY, D, true, EX>,
+    cudaError_t e = cudaFuncSetAttribute(k3s_velocity<N, TY, D, true, EX, Q>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::V_BYTES);
     if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(k3s_velocity<N, TY, D, false, EX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      e = cudaFuncSetAttribute(k3s_velocity<N, TY, D, false, EX, Q>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)G::V_BYTES);
     if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(k3s_stress<N, TY, D, EX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      e = cudaFuncSetAttribute(k3s_stress<N, TY, D, EX, Q>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)G::S_BYTES);
     if (e != cudaSuccess) return e;
     init = true;
   }
-  if (tensor) k3s_velocity<N, TY, D, true, EX><<<grid, G::NT, G::V_BYTES, st>>>(p, vm, a, it, 0);
-  else k3s_velocity<N, TY, D, false, EX><<<grid, G::NT, G::V_BYTES, st>>>(p, vm, a, it, force_here ? 1 : 0);
-  k3s_stress<N, TY, D, EX><<<grid, G::NT, G::S_BYTES, st>>>(p, smp, a, it, inject_next ? 1 : 0, gather ? 1 : 0);
+  if (tensor) k3s_velocity<N, TY, D, true, EX, Q><<<grid, G::NT, G::V_BYTES, st>>>(p, vm, a, it, 0);
+  else k3s_velocity<N, TY, D, false, EX, Q><<<grid, G::NT, G::V_BYTES, st>>>(p, vm, a, it, force_here ? 1 : 0);
+  k3s_stress<N, TY, D, EX, Q><<<grid, G::NT, G::S_BYTES, st>>>(p, smp, a, it, inject_next ? 1 : 0, gather ? 1 : 0);
   return cudaGetLastError();
 }
 
