@@ -24,12 +24,14 @@
 
 namespace sw {
 
-// z cells per thread: 2 in exact mode, 4 in fast mode.  Two cells keep the
-// exact kernels at 116-128 registers, so two 256-thread CTAs (16 warps) fit
-// per SM instead of three 128-thread ones at 168 (12 warps), which hides more
-// of the exact arithmetic's dependent chains (measured on B200 at 200^3:
-// steps 300-500 887 vs 1210 us, steady 729 vs 744 us); the fast kernels,
-// with shorter chains, are quicker with four (534 vs 594 us).
+// z cells per thread: 2 in exact mode, 4 in fast mode.  Two cells per thread
+// bound to three 256-thread CTAs per SM (80 registers, a few spills) give 24
+// resident warps instead of 12 (three 128-thread CTAs at 160-168 registers),
+// which hides more of the exact arithmetic's dependent chains; measured on
+// B200 at 200^3 (exact, steps 300-500 / 600-800): 829 / 626 us per step
+// against 1215 / 746 with four cells, and 823 / 664 at two CTAs per SM
+// without spills.  The fast kernels, with shorter chains, keep four cells
+// (482 us; 594 with two).
 constexpr int staged_q(bool exact) { return exact ? 2 : 4; }
 
 template <int N, int TY, int D, int Q>
@@ -37,7 +39,7 @@ struct SG {
   static constexpr int TZ = 32;
   static constexpr int CQ = TZ / Q;            // threads along z: Q cells each
   static constexpr int NT = TY * CQ;
-  static constexpr int MINB = Q == 4 ? 3 : 2;  // CTAs per SM the register budget aims at
+  static constexpr int MINB = 3;              // CTAs per SM the register budget aims at
   static constexpr int H4 = ((N + 3) / 4) * 4; // z halo, rounded to 16 bytes
   static constexpr int WZ = TZ + 2 * H4;       // width of boxes with a z halo
   static constexpr int HY = TY + 2 * N;        // height of boxes with a y halo
