@@ -24,14 +24,16 @@
 
 namespace sw {
 
-// z cells per thread: 2 in exact mode, 4 in fast mode.  Two cells per thread
-// bound to three 256-thread CTAs per SM (80 registers, a few spills) give 24
-// resident warps instead of 12 (three 128-thread CTAs at 160-168 registers),
-// which hides more of the exact arithmetic's dependent chains; measured on
-// B200 at 200^3 (exact, steps 300-500 / 600-800): 829 / 626 us per step
-// against 1215 / 746 with four cells, and 823 / 664 at two CTAs per SM
-// without spills.  The fast kernels, with shorter chains, keep four cells
-// (482 us; 594 with two).
+// z cells per thread: 2 in exact mode, 4 in fast mode.  With two cells per
+// thread the exact velocity pass is bound to three 256-thread CTAs per SM
+// (80 registers, 16/32 bytes of spills: 24 resident warps) and the stress
+// pass to two (128 registers, no spills: 16 warps), against 12 warps for
+// four cells (three 128-thread CTAs at 160-168 registers); the extra warps
+// hide more of the exact arithmetic's dependent chains.  Measured on B200 at
+// 200^3 (exact, steps 300-500 / 600-800 us per step): 793 / 601, against
+// 835 / 626 with both passes at three CTAs, 823 / 664 with both at two,
+// 774 / 691 with one cell per thread and 1215 / 746 with four.  The fast
+// kernels, with shorter chains, keep four cells (482 us; 594 with two).
 constexpr int staged_q(bool exact) { return exact ? 2 : 4; }
 
 template <int N, int TY, int D, int Q>
@@ -40,6 +42,7 @@ struct SG {
   static constexpr int CQ = TZ / Q;            // threads along z: Q cells each
   static constexpr int NT = TY * CQ;
   static constexpr int MINB = 3;              // CTAs per SM the register budget aims at
+  static constexpr int MINB_S = Q == 4 ? 3 : 2;  // same for the stress pass
   static constexpr int H4 = ((N + 3) / 4) * 4; // z halo, rounded to 16 bytes
   static constexpr int WZ = TZ + 2 * H4;       // width of boxes with a z halo
   static constexpr int HY = TY + 2 * N;        // height of boxes with a y halo
@@ -586,7 +589,7 @@ k3s_velocity(const __grid_constant__ P3<float> p, const __grid_constant__ Staged
 // stress pass
 // ---------------------------------------------------------------------------
 template <int N, int TY, int D, bool EX, int Q>
-__global__ void __launch_bounds__(SG<N, TY, D, Q>::NT, SG<N, TY, D, Q>::MINB)
+__global__ void __launch_bounds__(SG<N, TY, D, Q>::NT, SG<N, TY, D, Q>::MINB_S)
 k3s_stress(const __grid_constant__ P3<float> p, const __grid_constant__ StagedMaps maps,
            const __grid_constant__ StagedArgs a, int it, int inject_next, int gather) {
   using G = SG<N, TY, D, Q>;
