@@ -43,7 +43,7 @@ FALLBACK_HBM_GBS = 6650.0
 
 # DRAM bytes per time step (velocity + stress launch pair, default path and
 # numerics) from one ncu capture of the full workload (profiles/).
-NCU_TRAFFIC_PER_STEP = {"3d-ssg-cpml-tensor-200^3-nt1000": (477.977600 + 134.305536 + 521.134848 + 216.787200) * 1e6}
+NCU_TRAFFIC_PER_STEP = {"3d-ssg-cpml-tensor-200^3-nt1000": (460.576768 + 130.507520 + 508.705024 + 218.024704) * 1e6}
 
 
 def peaks():
