@@ -97,28 +97,35 @@ __device__ void tnet_load(float* T, const float* __restrict__ params, int nface)
   }
 }
 
-// bias block b[K] into s
-template <int K>
-__device__ __forceinline__ void tload(const float* __restrict__ b, float (&s)[K]) {
+// The correction kernels keep each layer's pre-activations as pairs and use
+// the packed two-lane FMA (__ffma2_rn, sm_100): each lane is one fmaf with
+// the same operands and order as the generic form above, so the bits are the
+// same, with half the FMA instructions.
+
+// bias block b[2P] into s
+template <int P>
+__device__ __forceinline__ void tload(const float* __restrict__ b, float2 (&s)[P]) {
 #pragma unroll
-  for (int o = 0; o < K; o += 4) {
-    const float4 v = *reinterpret_cast<const float4*>(b + o);
-    s[o] = v.x; s[o + 1] = v.y; s[o + 2] = v.z; s[o + 3] = v.w;
+  for (int o = 0; o < P; o += 2) {
+    const float4 v = *reinterpret_cast<const float4*>(b + 2 * o);
+    s[o] = make_float2(v.x, v.y);
+    s[o + 1] = make_float2(v.z, v.w);
   }
 }
 
-// s += W^T col for a transposed W[nin][K]; col holds this thread's inputs at
+// s += W^T col for a transposed W[nin][2P]; col holds this thread's inputs at
 // stride CT (its own column of the block's buffer)
-template <int K, int NIN, int U, int CT>
-__device__ __forceinline__ void tdense(const float* __restrict__ W, const float* col, float (&s)[K]) {
+template <int P, int NIN, int U, int CT>
+__device__ __forceinline__ void tdense(const float* __restrict__ W, const float* col, float2 (&s)[P]) {
 #pragma unroll U
   for (int k = 0; k < NIN; ++k) {
     const float xk = col[k * CT];
+    const float2 x2 = make_float2(xk, xk);
 #pragma unroll
-    for (int o = 0; o < K; o += 4) {
-      const float4 v = *reinterpret_cast<const float4*>(W + k * K + o);
-      s[o] = fmaf(v.x, xk, s[o]); s[o + 1] = fmaf(v.y, xk, s[o + 1]);
-      s[o + 2] = fmaf(v.z, xk, s[o + 2]); s[o + 3] = fmaf(v.w, xk, s[o + 3]);
+    for (int o = 0; o < P; o += 2) {
+      const float4 v = *reinterpret_cast<const float4*>(W + k * 2 * P + 2 * o);
+      s[o] = __ffma2_rn(make_float2(v.x, v.y), x2, s[o]);
+      s[o + 1] = __ffma2_rn(make_float2(v.z, v.w), x2, s[o + 1]);
     }
   }
 }
@@ -128,20 +135,26 @@ __device__ __forceinline__ void tdense(const float* __restrict__ W, const float*
 template <class NT, int CT>
 __device__ __forceinline__ void mlp_forward_t(const float* __restrict__ T, float* col, float* y) {
   using TN = TNet<NT>;
-  float s[TN::NH];
+  float2 s[TN::NH / 2];
   tload(T + TN::B1, s);
-  tdense<TN::NH, TN::NI, 3, CT>(T + TN::W1, col, s);
+  tdense<TN::NH / 2, TN::NI, 3, CT>(T + TN::W1, col, s);
 #pragma unroll
-  for (int o = 0; o < TN::NH; ++o) col[o * CT] = act(s[o]);
+  for (int o = 0; o < TN::NH / 2; ++o) {
+    col[(2 * o) * CT] = act(s[o].x);
+    col[(2 * o + 1) * CT] = act(s[o].y);
+  }
   tload(T + TN::B2, s);
-  tdense<TN::NH, TN::NH, 4, CT>(T + TN::W2, col, s);
+  tdense<TN::NH / 2, TN::NH, 4, CT>(T + TN::W2, col, s);
 #pragma unroll
-  for (int o = 0; o < TN::NH; ++o) col[o * CT] = act(s[o]);
-  float t[TN::NOP];
+  for (int o = 0; o < TN::NH / 2; ++o) {
+    col[(2 * o) * CT] = act(s[o].x);
+    col[(2 * o + 1) * CT] = act(s[o].y);
+  }
+  float2 t[TN::NOP / 2];
   tload(T + TN::B3, t);
-  tdense<TN::NOP, TN::NH, 4, CT>(T + TN::W3, col, t);
+  tdense<TN::NOP / 2, TN::NH, 4, CT>(T + TN::W3, col, t);
 #pragma unroll
-  for (int o = 0; o < TN::NO; ++o) y[o] = t[o];
+  for (int o = 0; o < TN::NO; ++o) y[o] = (o & 1) ? t[o / 2].y : t[o / 2].x;
 }
 
 // correction-kernel blocks: the faces' transposed blocks, then one column of
