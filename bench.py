@@ -444,6 +444,8 @@ def main(argv=None):
     cfg = get_config(args.config)
     three_d = len(cfg["shape"]) == 3
     w = build_solver(cfg, torch) if three_d else build_solver2d(cfg, torch)
+    if three_d:
+        w.autotune()  # x planes per work unit, outside the timed region
     nt = cfg["nt"]
     ncell = int(np.prod(cfg["shape"]))
     stream = torch.cuda.current_stream()

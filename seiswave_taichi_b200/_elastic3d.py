@@ -295,6 +295,77 @@ class Elastic3DBase:
     def set_tile(self, x_chunk: int):
         (self._plan or self._build_plan()).set_tile(int(x_chunk))
 
+    # -- autotuner (no reference counterpart) ------------------------------------
+    AUTOTUNE_CHUNKS = (6, 8, 12, 16, 25, 50)
+
+    def autotune(self, steps: int = 6, force: bool = False) -> int:
+        """Choose the x planes per work unit of the plan's current path (the
+        staged or fused chunk, or the two-pass kernels' x_chunk) by timing
+        `steps` steps of each candidate on this solver's own grid, with its
+        state replaced by random values for the trials and restored
+        afterwards (results do not depend on the choice).  The winner is
+        cached per (GPU, solver class, order, dtype, numeric mode, path, log2
+        shape bucket) in the batch autotuner's JSON file
+        (SEISWAVE_AUTOTUNE_CACHE).  Returns the chosen chunk length."""
+        import json
+        import math
+        from .batch import _cache_path
+        plan = self._plan or self._build_plan()
+        info = plan.info()
+        path_name = info["path"]
+        nx, ny, nz = self.gridsize
+        dev = torch.cuda.get_device_name(self._dev).replace(" ", "_")
+        bucket = "-".join(str(round(math.log2(max(n, 1)))) for n in (nx, ny, nz))
+        key = (f"3d|{dev}|{type(self).__module__}|{self.star}|{self._dt_torch}|{int(info['exact'])}|"
+               f"{path_name}|{bucket}")
+
+        def apply(chunk):
+            if path_name in ("staged", "fused"):
+                plan.set_path(path_name, int(chunk))
+            else:
+                plan.set_tile(int(chunk))
+
+        cache_file = _cache_path()
+        cache = {}
+        if cache_file.exists():
+            try:
+                cache = json.loads(cache_file.read_text())
+            except (OSError, ValueError):
+                cache = {}
+        if key in cache and not force:
+            apply(int(cache[key]))
+            return int(cache[key])
+        state = [getattr(self, f) for f in FIELDS3] + [m for m in self._mem if m is not None] + [self.data]
+        saved = [t.clone() for t in state]
+        gen = torch.Generator(device=state[0].device).manual_seed(0)
+        for t in state:
+            t.copy_(torch.randn(t.shape, generator=gen, device=t.device, dtype=t.dtype) * 1e-3)
+        st = torch.cuda.current_stream(self._dev)
+        steps = max(1, min(int(steps), self.nt - 1))
+        best, best_ms = None, float("inf")
+        for chunk in [c for c in self.AUTOTUNE_CHUNKS if c <= nx]:
+            apply(chunk)
+            self.run(1, 0, use_graph=False)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            self.run(steps, 1, use_graph=False)
+            e1.record(st)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            if ms < best_ms:
+                best, best_ms = chunk, ms
+        for t, v in zip(state, saved):
+            t.copy_(v)
+        apply(best)
+        cache[key] = best
+        try:
+            cache_file.parent.mkdir(parents=True, exist_ok=True)
+            cache_file.write_text(json.dumps(cache, indent=1, sort_keys=True))
+        except OSError:
+            pass
+        return best
+
     def check_finite(self) -> int:
         """Number of non-finite wavefield values (0 when the state is finite)."""
         return (self._plan or self._build_plan()).check_finite(self._stream())
