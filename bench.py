@@ -509,6 +509,7 @@ def main(argv=None):
     fast = None
     if three_d:
         wf = build_solver(cfg, torch, exact=False)
+        wf.autotune()
         for _ in range(2):
             wf.reset()
             wf.run(nt)
