@@ -345,8 +345,9 @@ SW_API int sw2d_adjoint_run(sw_plan* plan, const sw2d_adjoint_desc* adj, int32_t
                             const void* snap, void* stream);
 
 /* ---- 3D adjoint (no reference counterpart) --------------------------------
- * The same for the SW3D_CPML_TENSOR scheme (Elastic3D_SSG_Tensor.py:166-345),
- * orders 1..4: sw3d_record runs forward steps it0..it0+nsteps-1 with the
+ * The same for the SW3D_CPML_TENSOR scheme (Elastic3D_SSG_Tensor.py:166-345)
+ * and the SW3D_CPML_FORCE scheme (Elastic3D_SSG_CPML.py:144-309, whose point
+ * force adds its rho term to grad[0] at the source cell), orders 1..4: sw3d_record runs forward steps it0..it0+nsteps-1 with the
  * exact register-queue kernels and stores nsteps+1 snapshots of
  * sw3d_snapshot_elems() elements; sw3d_adjoint_run steps the adjoint state
  * back over them. */

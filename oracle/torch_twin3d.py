@@ -1,7 +1,8 @@
 """Test infrastructure, not product code: a differentiable float64 PyTorch
 restatement of the 3D SSG-CPML moment-tensor step (src/Elastic3D_SSG_Tensor.py:
-166-345, in the oracle's velocity3d / stress3d order) used as an independent
-gradient oracle for the hand-written 3D adjoint kernels.  CPU, tiny grids.
+166-345, in the oracle's velocity3d / stress3d order) and, in TwinForce3D, of
+the point-force step (src/Elastic3D_SSG_CPML.py:144-309), used as an
+independent gradient oracle for the hand-written 3D adjoint kernels.  CPU, tiny grids.
 Profiles, predicate bounds and coefficients come from an oracle.Oracle3D."""
 from __future__ import annotations
 
@@ -20,6 +21,7 @@ class TwinTensor3D:
         self.dt = float(d.dt)
         self.c = [float(d.c[m]) for m in range(self.N)]
         self.src = (int(d.isx), int(d.isy), int(d.isz))
+        self.force = False
         self.mneg = [-float(np.float32(d.mt[q])) for q in range(6)]
         self.wav = np.asarray(wavelet, np.float32).astype(np.float64)
         self.rec = torch.as_tensor(np.asarray(rec_index, np.int64))
@@ -88,12 +90,13 @@ class TwinTensor3D:
         out = []
         for it in range(nt):
             w = self.wav[it]
-            sxx = sxx + src * (w * self.mneg[0])
-            syy = syy + src * (w * self.mneg[1])
-            szz = szz + src * (w * self.mneg[2])
-            sxy = sxy + src * (w * self.mneg[3])
-            sxz = sxz + src * (w * self.mneg[4])
-            syz = syz + src * (w * self.mneg[5])
+            if not self.force:
+                sxx = sxx + src * (w * self.mneg[0])
+                syy = syy + src * (w * self.mneg[1])
+                szz = szz + src * (w * self.mneg[2])
+                sxy = sxy + src * (w * self.mneg[3])
+                sxz = sxz + src * (w * self.mneg[4])
+                syz = syz + src * (w * self.mneg[5])
             # vx
             r = ((N, nx - N - 1), (N + 1, ny - N), (N + 1, nz - N))
             P = self._pred((True, False, False), r)
@@ -126,6 +129,9 @@ class TwinTensor3D:
             vx = vx + self._pad(dvx, rx)
             vy = vy + self._pad(dvy, ry)
             vz = vz + self._pad(dvz, r)
+            if self.force:
+                # point force after the velocity phase (Elastic3D_SSG_CPML.py:245)
+                vz = vz + src * (dt * w / rho[self.src])
             # normal stresses
             r = ((N + 1, nx - N), (N + 1, ny - N), (N + 1, nz - N))
             (i0, i1), (j0, j1), (k0, k1) = r
@@ -178,3 +184,15 @@ class TwinTensor3D:
             out.append(vx.reshape(-1)[self.rec])
         self.final = (vx, vy, vz, sxx, syy, szz, sxy, sxz, syz)
         return torch.stack(out)
+
+
+class TwinForce3D(TwinTensor3D):
+    """The SSG-CPML point-force step (src/Elastic3D_SSG_CPML.py:144-309): the
+    same stencils, no moment tensor, vz[isx+5, isy+5, isz+5] += dt*w/rho
+    after the velocity phase; receivers record vx."""
+
+    def __init__(self, o, wavelet, rec_index):
+        super().__init__(o, wavelet, rec_index)
+        d = o.desc
+        self.src = (int(d.isx) + 5, int(d.isy) + 5, int(d.isz) + 5)
+        self.force = True

@@ -35,6 +35,14 @@ class ElasticWAVE(Elastic3DBase):
     def _receivers(self):
         return 0, self._rec_lin
 
+    def forward_op(self, vp, vs, rho, checkpoint_every: int = 100):
+        """Differentiable seismogram: the (nt, nrec) vx traces as a function of
+        the vp, vs, rho tensors (device, the solver's dtype), with the
+        hand-written 3D adjoint as backward, the point force's dt/rho term
+        included (no reference counterpart; exact numerics, orders 1..4)."""
+        from .adjoint import ForwardOp3D
+        return ForwardOp3D.apply(vp, vs, rho, self, int(checkpoint_every))
+
     def update_SSG(self, nt: int):
         """One time step (Elastic3D_SSG_CPML.py:144-309)."""
         self._step(nt)

@@ -191,8 +191,9 @@ F3 = ("vx", "vy", "vz", "sxx", "syy", "szz", "sxy", "sxz", "syz")
 
 
 class Adjoint3D:
-    """Checkpointed forward + adjoint driver for one 3D moment-tensor
-    solver (Elastic3D_SSG_Tensor, exact numerics, orders 1..4)."""
+    """Checkpointed forward + adjoint driver for one 3D CPML solver, moment
+    tensor (Elastic3D_SSG_Tensor) or point force (Elastic3D_SSG_CPML); exact
+    numerics, orders 1..4."""
 
     def __init__(self, wave, checkpoint_every: int = 100):
         if not getattr(wave, "exact", True):

@@ -951,8 +951,9 @@ cudaError_t adjoint2(sw_plan* pl, const sw::P2<T>& p, const sw2d_adjoint_desc* d
 
 int adjoint3_plan_ok(sw_plan* pl, const char* who) {
   if (!pl) return fail(SW_ERR_ARG, std::string(who) + ": null plan");
-  if (pl->dim != 3 || pl->scheme != SW3D_CPML_TENSOR)
-    return fail(SW_ERR_UNSUPPORTED, std::string(who) + ": the 3D adjoint covers the CPML moment-tensor scheme");
+  if (pl->dim != 3 || (pl->scheme != SW3D_CPML_TENSOR && pl->scheme != SW3D_CPML_FORCE))
+    return fail(SW_ERR_UNSUPPORTED,
+                std::string(who) + ": the 3D adjoint covers the CPML moment-tensor and point-force schemes");
   if (pl->order > 4) return fail(SW_ERR_UNSUPPORTED, std::string(who) + ": the 3D adjoint covers orders 1..4");
   return SW_OK;
 }
@@ -982,11 +983,14 @@ cudaError_t record3(sw_plan* pl, const sw::P3<T>& p, int it0, int n, T* snap, cu
   const long long se = snap3_elems(p);
   sw::P3<T> q = p;
   if (!pl->gather_in_stress) q.nrec = 0;
+  const bool tensor = pl->scheme == SW3D_CPML_TENSOR;
+  const bool moment = pl->src_kind == SW_SRC_MOMENT, force = pl->src_kind == SW_SRC_FORCE;
   for (int k = 0; k < n; ++k) {
     const int it = it0 + k;
-    cudaError_t e = sw::sw3_moment_inject<T>(p, it, st);
+    cudaError_t e = moment ? sw::sw3_moment_inject<T>(p, it, st) : cudaSuccess;
     if (e == cudaSuccess) e = snap3_store(p, snap + k * se, st);
-    if (e == cudaSuccess) e = sw::sw3_velocity<T>(q, pl->order, it, true, false, st);
+    if (e == cudaSuccess) e = sw::sw3_velocity<T>(q, pl->order, it, tensor, force && pl->src_in_kernel, st);
+    if (e == cudaSuccess && force && !pl->src_in_kernel) e = sw::sw3_force_inject<T>(p, it, st);
     if (e == cudaSuccess) e = sw::sw3_stress<T>(q, pl->order, it, false, st);
     if (e == cudaSuccess && !pl->gather_in_stress) e = sw::sw3_gather<T>(p, it, st);
     if (e != cudaSuccess) return e;

@@ -1,6 +1,7 @@
 // elastic3d_adjoint.cu -- hand-written discrete adjoint of the 3D SSG-CPML
-// moment-tensor step (src/Elastic3D_SSG_Tensor.py:166-345) for gradients of a
-// seismogram misfit with respect to rho, lambda and mu.  No reference
+// moment-tensor step (src/Elastic3D_SSG_Tensor.py:166-345) and point-force
+// step (src/Elastic3D_SSG_CPML.py:144-309, the same stencils) for gradients of
+// a seismogram misfit with respect to rho, lambda and mu.  No reference
 // counterpart.
 //
 // Forward step it (the oracle's velocity3d / stress3d order):
@@ -349,6 +350,17 @@ k3a_str_gather(const __grid_constant__ P3<T> p, const __grid_constant__ A3<T> a)
 
 #undef CELL3
 
+// The point force (Elastic3D_SSG_CPML.py:245) adds t/rho[src], t = dt*w(it),
+// to vz after the velocity phase; its adjoint leaves vz_bar as it is and adds
+// -t*vz_bar/rho^2 to d misfit / d rho[src], kept as t*vz_bar in grad[0] (the
+// slot whose coefficient is 1/rho of the same cell).  vz_bar here is the
+// adjoint after the stress phase's gather.
+template <typename T>
+__global__ void k3a_force(const __grid_constant__ P3<T> p, const __grid_constant__ A3<T> a, int it) {
+  const long long s = ((long long)p.si * p.ny + p.sj) * p.nz + p.sk;
+  a.grad[0][s] += (p.dt * p.wav[it]) * a.f[2][s];
+}
+
 template <typename T, int N>
 static cudaError_t adj3_step(const P3<T>& p, const A3<T>& a, int it, cudaStream_t st) {
   dim3 block(B3Z, B3Y);
@@ -356,6 +368,7 @@ static cudaError_t adj3_step(const P3<T>& p, const A3<T>& a, int it, cudaStream_
   if (p.nrec > 0) k3a_record<T><<<(p.nrec + 255) / 256, 256, 0, st>>>(p, a, it);
   k3a_stress_mid<T, N><<<grid, block, 0, st>>>(p, a);
   k3a_vel_gather<T, N><<<grid, block, 0, st>>>(p, a);
+  if (p.src_kind == SW_SRC_FORCE) k3a_force<T><<<1, 1, 0, st>>>(p, a, it);
   k3a_vel_mid<T, N><<<grid, block, 0, st>>>(p, a);
   k3a_str_gather<T, N><<<grid, block, 0, st>>>(p, a);
   return cudaGetLastError();

@@ -31,6 +31,61 @@ def _twin(c, wav):
     return o, TwinTensor3D(o, wav, rec)
 
 
+def _force_case(nt=60):
+    return case3d(shape=(20, 18, 22), N=2, scheme="CPML", nt=nt, npml=5, dtype=np.float64, seed=7)
+
+
+def _force_twin(c, wav):
+    from oracle.torch_twin3d import TwinForce3D
+    o = oracle3d(c, wavelet=wav)
+    nx, ny, nz = c["shape"]
+    rec = (np.asarray(c["rsx"]).reshape(-1) * ny + np.asarray(c["rsy"]).reshape(-1)) * nz + \
+        np.asarray(c["rsz"]).reshape(-1)
+    return o, TwinForce3D(o, wav, rec)
+
+
+def test_force_twin3d_forward_matches_oracle():
+    from seiswave_taichi_b200 import BaseFun
+    c = _force_case(nt=40)
+    wav = BaseFun.series("ricker", 40, c["dt"], c["freq"], 1000)
+    o, tw = _force_twin(c, wav)
+    d = tw.traces(torch.as_tensor(o.rho), torch.as_tensor(o.lam), torch.as_tensor(o.mu), 40)
+    o.run(0, 40)
+    assert rel_l2(d.numpy().astype(np.float32), np.asarray(o.data).reshape(d.shape)) <= 1e-6
+    for f, t in zip(("vx", "vy", "vz", "sxx", "syy", "szz", "sxy", "sxz", "syz"), tw.final):
+        assert rel_l2(t.numpy(), getattr(o, f)) <= 1e-13, f
+    assert np.abs(o.data).max() > 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("K", [25, 60])
+def test_force_adjoint3d_matches_twin_autograd(cuda, K):
+    """The point-force (Elastic3D_SSG_CPML) scheme: the same adjoint kernels
+    plus the force's dt/rho term at the source cell."""
+    from seiswave_taichi_b200.adjoint import Adjoint3D
+    c = _force_case()
+    w = product3d(c)
+    drv = Adjoint3D(w, K)
+    d = drv.forward()
+    nrec = d.shape[1] if d.dim() > 1 else 1
+    W = np.random.default_rng(1).standard_normal(tuple(d.shape))
+    g_rho, g_lam, g_mu = drv.backward(torch.as_tensor(W, device="cuda"))
+    wav = to_np(w._wavelet).astype(np.float32)
+    o, tw = _force_twin(c, wav)
+    rho = torch.tensor(o.rho, requires_grad=True)
+    lam = torch.tensor(o.lam, requires_grad=True)
+    mu = torch.tensor(o.mu, requires_grad=True)
+    dt = tw.traces(rho, lam, mu, c["nt"]).reshape(tuple(d.shape))
+    assert rel_l2(to_np(d).astype(np.float64), dt.detach().numpy()) <= 1e-6
+    (dt * torch.as_tensor(W)).sum().backward()
+    for name, mine, ref in (("rho", g_rho, rho.grad), ("lam", g_lam, lam.grad), ("mu", g_mu, mu.grad)):
+        e = rel_l2(to_np(mine), ref.numpy())
+        assert e <= 1e-9, (name, e, nrec)
+    # the source cell's rho gradient carries the force term
+    s = tw.src
+    assert abs(float(g_rho[s])) > 0
+
+
 def test_twin3d_forward_matches_oracle():
     c = _case(nt=40)
     wav = _wavelet(c)

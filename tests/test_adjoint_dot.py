@@ -74,10 +74,11 @@ def test_2d_adjoint_dot_product(cuda, scheme, n):
     assert abs(lhs - rhs) <= TOL * max(abs(lhs), abs(rhs)), (lhs, rhs)
 
 
+@pytest.mark.parametrize("scheme", ["TENSOR", "CPML"])
 @pytest.mark.parametrize("n", [1, 23])
-def test_3d_adjoint_dot_product(cuda, n):
+def test_3d_adjoint_dot_product(cuda, n, scheme):
     import seiswave_taichi_b200._native as N
-    c = case3d(shape=(20, 18, 22), N=2, scheme="TENSOR", nt=40, npml=5, dtype=np.float64, seed=6)
+    c = case3d(shape=(20, 18, 22), N=2, scheme=scheme, nt=40, npml=5, dtype=np.float64, seed=6)
     w = product3d(c)
     plan = w._plan or w._build_plan()
     w._wavelet.zero_()
