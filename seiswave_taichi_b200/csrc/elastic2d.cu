@@ -17,8 +17,10 @@
 
 namespace sw {
 
+// single-shot tile: 32 (z) x 4 (x) cells, one per thread (config 1, 400^2:
+// 13.3 Gcell/s against 12.8 with 32 x 8 on B200)
 constexpr int T2Z = 32;
-constexpr int T2X = 8;
+constexpr int T2X = 4;
 
 // ---------------------------------------------------------------------------
 // velocity update of cell (i, j), 0 <= i < nx, 0 <= j < nz
