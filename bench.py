@@ -43,7 +43,7 @@ FALLBACK_HBM_GBS = 6650.0
 
 # DRAM bytes per time step (velocity + stress launch pair, default path and
 # numerics) from one ncu capture of the full workload (profiles/).
-NCU_TRAFFIC_PER_STEP = {"3d-ssg-cpml-tensor-200^3-nt1000": (460.576768 + 130.507520 + 508.705024 + 218.024704) * 1e6}
+NCU_TRAFFIC_PER_STEP = {"3d-ssg-cpml-tensor-200^3-nt1000": (421.792512 + 127.147008 + 516.385536 + 223.332864) * 1e6}
 
 
 def peaks():
