@@ -1,0 +1,76 @@
+"""Edge cases against the oracle, bit for bit: the smallest grids the plans
+accept, grids smaller than one kernel tile (the tensor-map loads then read
+mostly out-of-range, zero-filled boxes), one-cell CPML layers, a point force
+on a cell the update passes do not cover, and receivers on dead boundary
+cells (never updated, so their traces stay zero) beside receivers on live
+cells."""
+import numpy as np
+import pytest
+
+from cases import case2d, case3d, oracle2d, oracle3d, product2d, product3d, to_np
+
+pytestmark = pytest.mark.gpu
+
+F2 = ("vx", "vz", "sxx", "szz", "sxz")
+F3 = ("vx", "vy", "vz", "sxx", "syy", "szz", "sxy", "sxz", "syz")
+
+
+def _eq(name, got, ref):
+    got, ref = np.asarray(got), np.asarray(ref)
+    assert got.shape == ref.shape, (name, got.shape, ref.shape)
+    assert np.array_equal(got, ref), (name, int((got != ref).sum()))
+
+
+@pytest.mark.parametrize("scheme", ["VS", "SV"])
+@pytest.mark.parametrize("N", [1, 2])
+def test_2d_smallest_grid(cuda, scheme, N):
+    import seiswave_taichi_b200._native as N_
+    n = 2 * N + 3
+    c = case2d(shape=(n, n), N=N, npml=1, nt=40, MT="explosive", src_scale=1e5)
+    c["rsx"] = np.array([[0, n // 2, n - 1]], np.int64)
+    c["rsz"] = np.array([[0, n // 2, n - 1]], np.int64)
+    w = product2d(c)
+    sid = {"VS": N_.SW2D_SSG_VS, "SV": N_.SW2D_SSG_SV}[scheme]
+    w._plan(sid)
+    o = oracle2d(c, wavelet=to_np(w._wavelets[sid]).astype(np.float32))
+    w.run(40, scheme=scheme)
+    o.run(scheme, 0, 40)
+    for f in F2:
+        _eq(f, to_np(getattr(w, f)), getattr(o, f))
+    _eq("data", to_np(w.data), o.data)
+    assert np.all(to_np(w.data)[:, 0] == 0) and np.all(to_np(w.data)[:, 2] == 0)
+
+
+@pytest.mark.parametrize("scheme", ["TENSOR", "CPML"])
+@pytest.mark.parametrize("shape", [(12, 12, 8), (9, 10, 12)])
+def test_3d_grid_smaller_than_a_tile(cuda, scheme, shape):
+    nx, ny, nz = shape
+    c = case3d(shape=shape, N=2, scheme=scheme, npml=2, nt=50, seed=3)
+    if scheme == "TENSOR":
+        c["rsx"] = np.array([[0, nx // 2, nx - 1]], np.int64)
+        c["rsy"] = np.array([[0, ny // 2, ny - 1]], np.int64)
+        c["rsz"] = np.array([[0, nz // 2, nz - 1]], np.int64)
+    else:
+        c["isx"], c["isy"], c["isz"] = 1, 1, 1  # the point force lands at (6, 6, 6)
+        c["rsx"], c["rsy"], c["rsz"] = 3, 4, nz // 2
+    w = product3d(c)
+    plan = w._build_plan()
+    # the staged kernels carry the source when it lies in [N, n-N) on every
+    # axis; otherwise (the point force at z = 6 of 8 here) the plan injects it
+    # with its own kernel on the two-pass path
+    off = 5 if scheme == "CPML" else 0
+    src = (c["isx"] + off, c["isy"] + off, c["isz"] + off)
+    inside = all(2 <= s_ < n - 2 for s_, n in zip(src, shape))
+    assert plan.info()["path"] == ("staged" if nz % 4 == 0 and inside else "two_pass")
+    o = oracle3d(c, wavelet=to_np(w._wavelet).astype(np.float32))
+    w.run(50)
+    o.run(0, 50)
+    for f in F3:
+        _eq(f, to_np(getattr(w, f)), getattr(o, f))
+    _eq("data", to_np(w.data), o.data)
+    for name in o.MEM_CPML:
+        _eq(name, to_np(getattr(w, name)), o.memory(name))
+    assert np.abs(o.vx).max() > 0
+    if scheme == "TENSOR":
+        d = to_np(w.data)
+        assert np.all(d[:, 0] == 0) and np.all(d[:, 2] == 0)
