@@ -6,6 +6,10 @@ coefficients (oracle_diff_coff), PML profiles (oracle_pml_axis), mu/lam
 (numpy, as Compute_mu/Compute_lam), full-grid memory variables and wavefields.
 Nothing here is imported by the product; tests/, __graft_entry__.smoke() and
 bench.py's CPU-baseline leg use it as the checker.
+
+Parity unpinned: the reference has no golden vectors and Taichi cannot run
+here; the restatement is held by closed-form coefficients, the numpy twin and
+the physics checks of tests/test_oracle.py (see sw_oracle.cpp's header).
 """
 from __future__ import annotations
 

@@ -21,6 +21,13 @@
 // reference's per-line operation order with true divisions; the build recipe
 // (oracle/Makefile) disables floating-point contraction so each operation
 // rounds on its own.
+//
+// Parity unpinned: the reference ships no golden vectors or known-answer
+// tests and Taichi cannot run here, so no output of the reference itself
+// checks this restatement.  It is held instead by closed-form coefficient
+// values, an independent numpy twin (oracle/np_twin.py, bit for bit) and
+// physics checks (arrival times, symmetry, reciprocity, convergence, CPML
+// reflection energy) in tests/test_oracle.py.
 #include <cmath>
 #include <cstdint>
 #include <cstring>
