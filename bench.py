@@ -214,6 +214,29 @@ def get_config(name):
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
+    if args.config == "segy":
+        # segyio (the reference's decoder) is absent: the numpy oracle, one core
+        sys.path.insert(0, str(ROOT))
+        from oracle import segy_ref
+        ntr, ns = 512, 16000
+        rec = 240 + 4 * ns
+        body = np.random.default_rng(0).integers(0, 256, ntr * rec, dtype=np.uint8)
+        vals = []
+        for s_ in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            segy_ref.decode(body, ntr, ns, 1)
+            if s_ >= args.warmup:
+                vals.append(ntr * rec / (time.perf_counter() - t0) / 1e9)
+        v = float(np.mean(vals))
+        print(json.dumps({
+            "impl": "reference", "metric": "GB/s", "value": v, "unit": "GB/s (SEG-Y input decoded)",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ntr * rec / v / 1e6,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8->f32",
+            "data": "synthetic", "config": {"workload": f"segy-ibm-{ntr}x{ns} (bounded sample)"},
+            "cpu_baseline": {"value": v, "unit": "GB/s", "cores": 1, "kind": "port",
+                             "sample": f"{ntr} traces of {ns} IBM samples per step, numpy oracle"},
+            "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}), flush=True)
+        return 0
     cfg = get_config(args.config)
     samples = []
     for s in range(args.warmup + args.steps):
@@ -347,6 +370,108 @@ def run_batch(args, rank, world, local):
     return 0
 
 
+def run_segy(args, rank, world, local):
+    """SEG-Y ingestion (`--config segy`): decode 8192 traces of 16000 IBM-float
+    samples (about 0.5 GB of seeded synthetic file bytes: normal amplitudes
+    over several orders of magnitude, SourceX in each trace header) to
+    float32 per step with
+    sw_segy_decode.  value: GB/s of SEG-Y input decoded with the bytes already
+    in HBM; e2e: the same through pinned host memory (host-to-device copy of
+    the bytes, decode, device-to-host read of the float samples)."""
+    import ctypes as C
+    import torch
+    from seiswave_taichi_b200 import _native as N
+    from seiswave_taichi_b200.ReadSegy import decode_traces
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    ntr, ns, fmt = 8192, 16000, 1
+    rec = 240 + 4 * ns
+    rng = np.random.default_rng(rank)
+    body = np.empty((ntr, rec), np.uint8)
+    # recorded amplitudes: normal values of a few orders of magnitude, as IBM
+    # words (fraction truncated) written big-endian
+    amp = rng.standard_normal((ntr, ns)) * np.exp(rng.uniform(-8.0, 8.0, (ntr, 1)))
+    m, p2 = np.frexp(np.abs(amp))
+    q = -((-p2) // 4)
+    f = np.floor(np.ldexp(m, p2 - 4 * q + 24)).astype(np.uint32)
+    w = (np.signbit(amp).astype(np.uint32) << 31) | ((q + 64).astype(np.uint32) << 24) | f
+    w[amp == 0] = 0
+    body[:, 240:] = w.astype(">u4").view(np.uint8).reshape(ntr, 4 * ns)
+    del amp, m, p2, q, f, w
+    body[:, :240] = 0
+    body[:, 72:76] = np.arange(ntr, dtype=">i4").view(np.uint8).reshape(ntr, 4)
+    host = torch.from_numpy(body.reshape(-1)).pin_memory()
+    dev = host.to("cuda")
+    nbytes = host.numel()
+    out_host = torch.empty((ntr, ns), dtype=torch.float32).pin_memory()
+    stream = torch.cuda.current_stream()
+    for _ in range(max(3, args.warmup)):
+        decode_traces(dev, ntr, ns, fmt)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            out, _ = decode_traces(dev, ntr, ns, fmt)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1), dist) / args.steps
+    value = world * nbytes / (ms * 1e-3) / 1e9
+    # end to end: file bytes from pinned host memory in, float samples out
+    e0.record(stream)
+    for _ in range(args.steps):
+        d = host.to("cuda", non_blocking=True)
+        o, _ = decode_traces(d, ntr, ns, fmt)
+        out_host.copy_(o, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = max_over_ranks(e0.elapsed_time(e1), dist) / args.steps
+    peak, peak_kind = peaks()
+    moved = nbytes + 4 * ntr * ns
+    line = None
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu_baseline:
+            sys.path.insert(0, str(ROOT))
+            from oracle import segy_ref
+            k = 512
+            t0 = time.perf_counter()
+            reps = 0
+            while time.perf_counter() - t0 < 10.0:
+                segy_ref.decode(body[:k].reshape(-1), k, ns, fmt)
+                reps += 1
+            sec = time.perf_counter() - t0
+            cpu = {"value": reps * k * rec / sec / 1e9, "unit": "GB/s", "cores": 1, "kind": "port",
+                   "sample": f"{reps} decodes of {k} traces ({k * rec / 1e6:.0f} MB) with the numpy oracle"}
+        line = {
+            "metric": "GB/s", "value": value, "unit": "GB/s (SEG-Y input decoded)", "n_gpus": world,
+            "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8->f32", "data": "synthetic",
+            "config": {"workload": f"segy-ibm-{ntr}x{ns}", "traces": ntr, "samples": ns, "format": "IBM float",
+                       "bytes_per_step": nbytes, "l2": "input larger than L2"},
+            "roofline": {"bound": "hbm", "achieved": moved / (ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": moved / (ms * 1e-3) / 1e9 / peak, "traffic": None,
+                         "kernel": "k_segy_decode<1> (file bytes in, float32 samples out)",
+                         "algorithmic_bytes_per_launch": moved, "ms_per_launch": ms,
+                         "peak_source": f"{peak_kind} {peak:.0f} GB/s"},
+            "e2e": {"value": world * nbytes / (ms_e2e * 1e-3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": nbytes,
+                    "d2h_bytes_per_step": 4 * ntr * ns},
+            "gpu_launches": args.steps, "clocks": clk.summary(), "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def run_thin_layer(args, rank, world, local):
     """Config 5's cost comparison on one GPU: forward runs of a 256^3
     interior (seeded layered vp 2000-5000 m/s, dx = 10 m, dt = 0.8 ms,
@@ -416,7 +541,7 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="config2", choices=["config2", "config1", "config3", "config4", "config5"])
+    ap.add_argument("--config", default="config2", choices=["config2", "config1", "config3", "config4", "config5", "segy"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the float64 error runs")
     args = ap.parse_args(argv)
@@ -432,6 +557,8 @@ def main(argv=None):
         return run_batch(args, rank, world, local)
     if args.config == "config5":
         return run_thin_layer(args, rank, world, local)
+    if args.config == "segy":
+        return run_segy(args, rank, world, local)
 
     import torch
     torch.cuda.set_device(local)

@@ -391,6 +391,19 @@ SW_API int sw_check_finite(sw_plan* plan, void* stream, int64_t* nonfinite);
 SW_API int sw_count_nonfinite_noalloc(const void* const* arrays, const int64_t* lengths, int32_t narrays,
                                       int32_t dtype, void* stream, int64_t* counts);
 
+/* ---- SEG-Y ingestion -------------------------------------------------------
+ * Decode SEG-Y traces on the device, replacing the segyio trace reads of
+ * ReadSegy.py:3-18 (read_segy).  traces: the file's bytes from the first trace
+ * header on (after the 3600-byte header and any extended textual headers),
+ * in device memory, 4-byte aligned: ntraces records of a 240-byte trace
+ * header and nsamples big-endian samples in `format` (1 IBM float, 2 int32,
+ * 3 int16, 5 IEEE float, 8 int8).  out: (ntraces, nsamples) float32; IBM
+ * values are exact in double and rounded once to float.  srcx (optional,
+ * ntraces int32): the SourceX header word (bytes 73-76) of each trace, which
+ * read_segy groups shots by.  Enqueued on stream; nothing is allocated. */
+SW_API int sw_segy_decode(const void* traces, int64_t ntraces, int32_t nsamples, int32_t format, float* out,
+                          int32_t* srcx, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

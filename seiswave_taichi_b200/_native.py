@@ -35,7 +35,7 @@ EXPORTS = (
     "sw_batch_destroy", "sw2d_abc_correct", "sw2d_abc_features", "sw_mlp_grad", "sw_mlp_forward",
     "sw_mlp_backward", "sw2d_abc_adjoint", "sw3d_snapshot_elems", "sw3d_record", "sw3d_adjoint_run",
     "sw3d_abc_correct", "sw3d_abc_features", "sw3d_abc_adjoint", "sw3d_mlp_grad", "sw3d_mlp_forward",
-    "sw3d_mlp_backward",
+    "sw3d_mlp_backward", "sw_segy_decode",
 )
 
 SW_ABC_DEPTH = 6
@@ -156,6 +156,7 @@ def load() -> C.CDLL:
         "sw_count_nonfinite_noalloc": (C.c_int, [C.POINTER(vp), C.POINTER(C.c_int64), C.c_int32, C.c_int32, vp,
                                                  C.POINTER(C.c_int64)]),
         "sw2d_snapshot_elems": (C.c_int, [vp, C.POINTER(C.c_int64)]),
+        "sw_segy_decode": (C.c_int, [vp, C.c_int64, C.c_int32, C.c_int32, vp, vp, vp]),
         "sw2d_record": (C.c_int, [vp, C.c_int32, C.c_int32, vp, vp]),
         "sw2d_adjoint_run": (C.c_int, [vp, C.POINTER(Adjoint2D), C.c_int32, C.c_int32, vp, vp]),
         "sw2d_batch_create": (C.c_int, [C.POINTER(Desc2D), C.c_int32, C.POINTER(vp)]),

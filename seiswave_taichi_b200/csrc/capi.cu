@@ -27,6 +27,7 @@ template <typename T> cudaError_t sw3_gather(const P3<T>&, int, cudaStream_t);
 template <typename T> cudaError_t sw3_spml_step(const P3<T>&, int, int, bool, cudaStream_t);
 template <typename T> cudaError_t sw2_step(const P2<T>&, int, int, int, T, bool, bool, bool, cudaStream_t);
 template <typename T> cudaError_t sw2_moment_inject(const P2<T>&, int, cudaStream_t);
+cudaError_t segy_decode(const void*, long long, int, int, float*, int32_t*, cudaStream_t);
 template <typename T>
 cudaError_t sw2_persistent(const P2<T>&, int, int, int, int, bool, bool, unsigned int*, int*, cudaStream_t);
 template <typename T>
@@ -1502,6 +1503,21 @@ int noalloc_scratch(unsigned long long** out) {
 }  // namespace
 
 extern "C" {
+
+int sw_segy_decode(const void* traces, int64_t ntraces, int32_t nsamples, int32_t format, float* out,
+                   int32_t* srcx, void* stream) {
+  if (ntraces < 0 || nsamples < 0) return fail(SW_ERR_ARG, "sw_segy_decode: negative trace or sample count");
+  if (format != 1 && format != 2 && format != 3 && format != 5 && format != 8)
+    return fail(SW_ERR_UNSUPPORTED, "sw_segy_decode: sample format " + std::to_string(format) +
+                                        " (supported: 1 IBM float, 2 int32, 3 int16, 5 IEEE float, 8 int8)");
+  if (ntraces == 0 || nsamples == 0) return SW_OK;
+  if (!traces || !out) return fail(SW_ERR_ARG, "sw_segy_decode: null traces or output");
+  if (!aligned(traces, 4) || !aligned(out, 4) || (srcx && !aligned(srcx, 4)))
+    return fail(SW_ERR_ARG, "sw_segy_decode: traces, out and srcx must be 4-byte aligned");
+  cudaError_t e = sw::segy_decode(traces, ntraces, nsamples, format, out, srcx, (cudaStream_t)stream);
+  if (e != cudaSuccess) return cuda_fail(e, "sw_segy_decode");
+  return SW_OK;
+}
 
 int sw_count_nonfinite_noalloc(const void* const* arrays, const int64_t* lengths, int32_t narrays, int32_t dtype,
                                void* stream, int64_t* counts) {
