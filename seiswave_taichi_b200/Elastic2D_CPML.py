@@ -106,6 +106,7 @@ class ElasticWAVE:
         self.zmin_pml, self.zmax_pml = self.zmin, self.zmax
         self._prof = None
         self._plans = {}
+        self._free_surface = False
         self._wavelets = {}
         self._mem = [None, None]
         self.MT = None if MT is None else moment_2d(MT)
@@ -273,6 +274,8 @@ class ElasticWAVE:
             d.rec.data = self.data.data_ptr()
             d.rec.dtype = N.SW_F64 if self.data.dtype == torch.float64 else N.SW_F32
         plan = N.Plan(d, keep, three_d=False)
+        if self._free_surface:
+            plan.set_free_surface(True)
         self._plans[scheme] = plan
         return plan
 
@@ -297,9 +300,24 @@ class ElasticWAVE:
         """One step of Elastic2D_CPML.py:277-353 with the caller's source value."""
         self._plan(N.SW2D_RSG).step_amp(int(nt), float(np.float32(source)), self._stream())
 
-    def run(self, nt=None, it0: int = 0, scheme: str = "VS", use_graph: bool = True):
+    def set_free_surface(self, on: bool = True):
+        """Free-surface mode (no reference counterpart as a mode): every
+        update_SSG_VS / update_SSG_SV / update_RSG step and every run() step
+        first applies AEA (sxx = 0 on the x layer `star`), as the reference's
+        driver loop `AEA(); update_SSG_VS(i)` does (Relay_wave.py:55-59); in
+        run() the hooks are folded into the kernels.  Call AEA_init() once
+        for the material part of the condition."""
+        self._free_surface = bool(on)
+        for plan in self._plans.values():
+            plan.set_free_surface(self._free_surface)
+        return self
+
+    def run(self, nt=None, it0: int = 0, scheme: str = "VS", use_graph: bool = True, free_surface=None):
         """Steps it0 .. it0+nt-1 of update_SSG_VS ("VS") or update_SSG_SV ("SV")
-        in one enqueue (CUDA graph)."""
+        in one enqueue (CUDA graph); free_surface=True/False sets the
+        free-surface mode first (set_free_surface)."""
+        if free_surface is not None:
+            self.set_free_surface(free_surface)
         nt = self.nt - it0 if nt is None else int(nt)
         s = {"VS": N.SW2D_SSG_VS, "SV": N.SW2D_SSG_SV}[scheme]
         self._plan(s).run(int(it0), nt, use_graph, self._stream())

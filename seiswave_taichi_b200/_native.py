@@ -35,7 +35,7 @@ EXPORTS = (
     "sw_batch_destroy", "sw2d_abc_correct", "sw2d_abc_features", "sw_mlp_grad", "sw_mlp_forward",
     "sw_mlp_backward", "sw2d_abc_adjoint", "sw3d_snapshot_elems", "sw3d_record", "sw3d_adjoint_run",
     "sw3d_abc_correct", "sw3d_abc_features", "sw3d_abc_adjoint", "sw3d_mlp_grad", "sw3d_mlp_forward",
-    "sw3d_mlp_backward", "sw_segy_decode",
+    "sw3d_mlp_backward", "sw_segy_decode", "sw_plan_set_free_surface",
 )
 
 SW_ABC_DEPTH = 6
@@ -157,6 +157,7 @@ def load() -> C.CDLL:
                                                  C.POINTER(C.c_int64)]),
         "sw2d_snapshot_elems": (C.c_int, [vp, C.POINTER(C.c_int64)]),
         "sw_segy_decode": (C.c_int, [vp, C.c_int64, C.c_int32, C.c_int32, vp, vp, vp]),
+        "sw_plan_set_free_surface": (C.c_int, [vp, C.c_int32]),
         "sw2d_record": (C.c_int, [vp, C.c_int32, C.c_int32, vp, vp]),
         "sw2d_adjoint_run": (C.c_int, [vp, C.POINTER(Adjoint2D), C.c_int32, C.c_int32, vp, vp]),
         "sw2d_batch_create": (C.c_int, [C.POINTER(Desc2D), C.c_int32, C.POINTER(vp)]),
@@ -289,6 +290,10 @@ class Plan:
         return {"path": names[a[0]], "fast_div": bool(a[1]), "staged": bool(a[2]), "staged_grid": a[3],
                 "staged_chunk": a[4], "fused": bool(a[5]), "fused_grid": a[6], "fused_chunk": a[7],
                 "exact": bool(a[8])}
+
+    def set_free_surface(self, on: bool = True) -> None:
+        """2D: apply the free-surface hook AEA before every step (sticky)."""
+        check(load().sw_plan_set_free_surface(self._h, 1 if on else 0))
 
     def set_exact(self, exact: bool) -> None:
         """Numeric mode of the staged path (the other paths are always exact)."""

@@ -25,7 +25,7 @@ template <typename T> cudaError_t sw3_moment_inject(const P3<T>&, int, cudaStrea
 template <typename T> cudaError_t sw3_force_inject(const P3<T>&, int, cudaStream_t);
 template <typename T> cudaError_t sw3_gather(const P3<T>&, int, cudaStream_t);
 template <typename T> cudaError_t sw3_spml_step(const P3<T>&, int, int, bool, cudaStream_t);
-template <typename T> cudaError_t sw2_step(const P2<T>&, int, int, int, T, bool, bool, bool, cudaStream_t);
+template <typename T> cudaError_t sw2_step(const P2<T>&, int, int, int, T, bool, bool, bool, int, cudaStream_t);
 template <typename T> cudaError_t sw2_moment_inject(const P2<T>&, int, cudaStream_t);
 cudaError_t segy_decode(const void*, long long, int, int, float*, int32_t*, cudaStream_t);
 template <typename T>
@@ -151,6 +151,7 @@ struct sw_plan {
   // per run)
   int path = 0;
   unsigned int* d_bar = nullptr;  // 2D persistent path: grid-barrier arrival and generation words
+  bool aea = false;               // 2D free-surface hook before every step (sw_plan_set_free_surface)
 };
 
 namespace {
@@ -379,12 +380,15 @@ cudaError_t enqueue_step(sw_plan* pl, int it, bool first, bool last, bool has_am
   const bool moment = pl->src_kind == SW_SRC_MOMENT;
   const bool fold = moment && pl->gather_in_stress;
   const bool pre = moment && (first || !fold), nxt = fold && !last;
+  // free surface: the hook of the first step runs on its own, those of the
+  // later steps are folded into the previous stress pass
+  const int aea = pl->aea ? ((first ? 1 : 0) | (last ? 0 : 2)) : 0;
   if (pl->dtype == SW_F32) {
     float a = has_amp ? (float)amp : 0.f;
-    return sw::sw2_step<float>(pl->p2f, pl->scheme, pl->order, it, a, pl->gather_in_stress, pre, nxt, st);
+    return sw::sw2_step<float>(pl->p2f, pl->scheme, pl->order, it, a, pl->gather_in_stress, pre, nxt, aea, st);
   }
   double a = has_amp ? (double)(float)amp : 0.0;
-  return sw::sw2_step<double>(pl->p2d, pl->scheme, pl->order, it, a, pl->gather_in_stress, pre, nxt, st);
+  return sw::sw2_step<double>(pl->p2d, pl->scheme, pl->order, it, a, pl->gather_in_stress, pre, nxt, aea, st);
 }
 
 int check_it(sw_plan* pl, int it0, int n) {
@@ -780,6 +784,15 @@ int sw_plan_set_path(sw_plan* pl, int32_t path, int32_t chunk_len) {
   return SW_OK;
 }
 
+int sw_plan_set_free_surface(sw_plan* pl, int32_t on) {
+  if (!pl) return fail(SW_ERR_ARG, "null plan");
+  if (pl->dim != 2) return fail(SW_ERR_UNSUPPORTED, "the free-surface hook is built for 2D plans");
+  const bool v = on != 0;
+  if (v != pl->aea && pl->gexec) { cudaGraphExecDestroy(pl->gexec); pl->gexec = nullptr; pl->g_it0 = pl->g_n = -1; }
+  pl->aea = v;
+  return SW_OK;
+}
+
 int sw_plan_set_exact(sw_plan* pl, int32_t exact) {
   if (!pl) return fail(SW_ERR_ARG, "null plan");
   pl->sa.exact = exact ? 1 : 0;
@@ -824,7 +837,7 @@ int sw_run(sw_plan* pl, int32_t it0, int32_t nsteps, int32_t use_graph, void* st
   if (nsteps == 0) return SW_OK;
   cudaStream_t st = (cudaStream_t)stream;
   cudaError_t e;
-  if (pl->dim == 2 && pl->path == 3) {
+  if (pl->dim == 2 && pl->path == 3 && !pl->aea) {
     // one launch for the whole run: nothing to capture
     e = persistent_run2(pl, it0, nsteps, st);
     if (e != cudaSuccess) return cuda_fail(e, "sw_run: persistent launch");
@@ -925,7 +938,7 @@ cudaError_t record2(sw_plan* pl, const sw::P2<T>& p, int it0, int n, T* snap, cu
     cudaError_t e = cudaSuccess;
     if (pl->src_kind == SW_SRC_MOMENT) e = sw::sw2_moment_inject<T>(p, it, st);
     if (e == cudaSuccess) e = snap_store(p, snap + k * se, st);
-    if (e == cudaSuccess) e = sw::sw2_step<T>(p, pl->scheme, pl->order, it, (T)0, pl->gather_in_stress, false, false, st);
+    if (e == cudaSuccess) e = sw::sw2_step<T>(p, pl->scheme, pl->order, it, (T)0, pl->gather_in_stress, false, false, 0, st);
     if (e != cudaSuccess) return e;
   }
   return snap_store(p, snap + (long long)n * se, st);

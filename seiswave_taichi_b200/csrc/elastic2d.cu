@@ -190,6 +190,9 @@ __device__ __forceinline__ void vel2_cell(const P2<T>& p, int i, int j, int it, 
 
 // stress update of cell (i, j), then the next step's moment-tensor source
 template <typename T, int N, int SCHEME>
+// flags: bit 0 adds step it+1's moment-tensor source after the update, bit 1
+// zeroes sxx on the x layer N first (the free-surface hook AEA of step it+1,
+// Elastic2D_CPML.py:122-125, which precedes the source of that step)
 __device__ __forceinline__ void str2_cell(const P2<T>& p, int i, int j, int it, int inject_next) {
   const int nx = p.nx, nz = p.nz;
   const long long idx = (long long)i * nz + j;
@@ -313,7 +316,8 @@ __device__ __forceinline__ void str2_cell(const P2<T>& p, int i, int j, int it, 
   }
   // moment-tensor source of step it+1, added after this cell's own update
   // (nothing reads the stresses between here and the next velocity pass)
-  if (inject_next && i == p.si && j == p.sk) {
+  if ((inject_next & 2) && i == N) sxx[idx] = (T)0;
+  if ((inject_next & 1) && i == p.si && j == p.sk) {
     const T w = p.wav[it + 1];
     sxx[idx] = sxx[idx] + w * p.mneg[0];
     szz[idx] = szz[idx] + w * p.mneg[1];
@@ -356,51 +360,61 @@ __global__ void k2_moment_inject(const __grid_constant__ P2<T> p, int it) {
   p.f[4][s] = p.f[4][s] + w * p.mneg[2];
 }
 
+// free-surface hook AEA (Elastic2D_CPML.py:122-125): sxx = 0 on the x layer N
+template <typename T>
+__global__ void k2_aea(const __grid_constant__ P2<T> p, int n_layer) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < p.nz) p.f[2][(long long)n_layer * p.nz + j] = (T)0;
+}
+
 template <typename T>
 __global__ void k2_gather(const __grid_constant__ P2<T> p, int it) {
   const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (r < p.nrec) store_rec(p.rec_data, p.rec_f64, (long long)it * p.nrec + r, p.f[p.rec_field][p.rec_idx[r]]);
 }
 
+// aea: bit 0 applies the free-surface hook before this step, bit 1 folds the
+// next step's into this step's stress pass
 template <typename T, int N, int S>
 static cudaError_t launch2(const P2<T>& p, int it, T amp, bool gather_in_stress, bool pre_inject,
-                           bool inject_next, cudaStream_t st) {
+                           bool inject_next, int aea, cudaStream_t st) {
   dim3 block(T2Z, T2X);
   dim3 grid((p.nz + T2Z - 1) / T2Z, (p.nx + T2X - 1) / T2X);
   const bool moment = p.src_kind == SW_SRC_MOMENT;
+  if (aea & 1) k2_aea<T><<<(p.nz + 255) / 256, 256, 0, st>>>(p, N);
   if (moment && pre_inject) k2_moment_inject<T><<<1, 1, 0, st>>>(p, it);
   k2_velocity<T, N, S><<<grid, block, 0, st>>>(p, it, amp, (p.src_kind != SW_SRC_NONE && !moment) ? 1 : 0);
   P2<T> q = p;
   if (!gather_in_stress) q.nrec = 0;
-  k2_stress<T, N, S><<<grid, block, 0, st>>>(q, it, (moment && inject_next) ? 1 : 0);
+  k2_stress<T, N, S><<<grid, block, 0, st>>>(q, it, ((moment && inject_next) ? 1 : 0) | ((aea & 2) ? 2 : 0));
   if (!gather_in_stress && p.nrec > 0) k2_gather<T><<<(p.nrec + 255) / 256, 256, 0, st>>>(p, it);
   return cudaGetLastError();
 }
 
 template <typename T, int S>
-static cudaError_t dispatch2(const P2<T>& p, int order, int it, T amp, bool g, bool pre, bool nxt,
+static cudaError_t dispatch2(const P2<T>& p, int order, int it, T amp, bool g, bool pre, bool nxt, int aea,
                              cudaStream_t st) {
   switch (order) {
-    case 1: return launch2<T, 1, S>(p, it, amp, g, pre, nxt, st);
-    case 2: return launch2<T, 2, S>(p, it, amp, g, pre, nxt, st);
-    case 3: return launch2<T, 3, S>(p, it, amp, g, pre, nxt, st);
-    case 4: return launch2<T, 4, S>(p, it, amp, g, pre, nxt, st);
-    case 5: return launch2<T, 5, S>(p, it, amp, g, pre, nxt, st);
-    case 6: return launch2<T, 6, S>(p, it, amp, g, pre, nxt, st);
-    case 7: return launch2<T, 7, S>(p, it, amp, g, pre, nxt, st);
-    case 8: return launch2<T, 8, S>(p, it, amp, g, pre, nxt, st);
+    case 1: return launch2<T, 1, S>(p, it, amp, g, pre, nxt, aea, st);
+    case 2: return launch2<T, 2, S>(p, it, amp, g, pre, nxt, aea, st);
+    case 3: return launch2<T, 3, S>(p, it, amp, g, pre, nxt, aea, st);
+    case 4: return launch2<T, 4, S>(p, it, amp, g, pre, nxt, aea, st);
+    case 5: return launch2<T, 5, S>(p, it, amp, g, pre, nxt, aea, st);
+    case 6: return launch2<T, 6, S>(p, it, amp, g, pre, nxt, aea, st);
+    case 7: return launch2<T, 7, S>(p, it, amp, g, pre, nxt, aea, st);
+    case 8: return launch2<T, 8, S>(p, it, amp, g, pre, nxt, aea, st);
     default: return cudaErrorInvalidValue;
   }
 }
 
 template <typename T>
 cudaError_t sw2_step(const P2<T>& p, int scheme, int order, int it, T amp, bool gather_in_stress, bool pre_inject,
-                     bool inject_next, cudaStream_t st) {
+                     bool inject_next, int aea, cudaStream_t st) {
   if (scheme == SW2D_SSG_VS)
-    return dispatch2<T, SW2D_SSG_VS>(p, order, it, amp, gather_in_stress, pre_inject, inject_next, st);
+    return dispatch2<T, SW2D_SSG_VS>(p, order, it, amp, gather_in_stress, pre_inject, inject_next, aea, st);
   if (scheme == SW2D_SSG_SV)
-    return dispatch2<T, SW2D_SSG_SV>(p, order, it, amp, gather_in_stress, pre_inject, inject_next, st);
-  return dispatch2<T, SW2D_RSG>(p, order, it, amp, gather_in_stress, pre_inject, inject_next, st);
+    return dispatch2<T, SW2D_SSG_SV>(p, order, it, amp, gather_in_stress, pre_inject, inject_next, aea, st);
+  return dispatch2<T, SW2D_RSG>(p, order, it, amp, gather_in_stress, pre_inject, inject_next, aea, st);
 }
 
 template <typename T>
@@ -682,7 +696,7 @@ cudaError_t sw2b_step(const Batch2<T>& bt, int scheme, int order, int cfg, int t
 template cudaError_t sw2b_step<float>(const Batch2<float>&, int, int, int, int, int, bool, bool, cudaStream_t);
 template cudaError_t sw2b_step<double>(const Batch2<double>&, int, int, int, int, int, bool, bool, cudaStream_t);
 
-template cudaError_t sw2_step<float>(const P2<float>&, int, int, int, float, bool, bool, bool, cudaStream_t);
-template cudaError_t sw2_step<double>(const P2<double>&, int, int, int, double, bool, bool, bool, cudaStream_t);
+template cudaError_t sw2_step<float>(const P2<float>&, int, int, int, float, bool, bool, bool, int, cudaStream_t);
+template cudaError_t sw2_step<double>(const P2<double>&, int, int, int, double, bool, bool, bool, int, cudaStream_t);
 
 }  // namespace sw
