@@ -245,8 +245,7 @@ class ElasticWAVE:
             d.mem[a] = m.data_ptr() if m is not None else None
             keep.append(m)
         if scheme == N.SW2D_SSG_VS:
-            t0 = np.float32(1.5) / np.float32(self.f0)
-            wav = BaseFun.series("ricker2", self.nt, self.dt, self.f0, self.src_scale, t0=t0)
+            wav = self._vs_wavelet()
             d.src.kind = N.SW_SRC_FORCE
             rec_field = 1  # vz (Elastic2D_CPML.py:200)
         elif scheme == N.SW2D_SSG_SV:
@@ -278,6 +277,11 @@ class ElasticWAVE:
             plan.set_free_surface(True)
         self._plans[scheme] = plan
         return plan
+
+    def _vs_wavelet(self):
+        """update_SSG_VS's source series: Ricker2 with t0 = 1.5/f0 (:142, :170)."""
+        t0 = np.float32(1.5) / np.float32(self.f0)
+        return BaseFun.series("ricker2", self.nt, self.dt, self.f0, self.src_scale, t0=t0)
 
     def _stream(self) -> int:
         return torch.cuda.current_stream(self._dev).cuda_stream
