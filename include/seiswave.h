@@ -77,7 +77,8 @@ extern "C" {
 typedef struct sw_pml_axis {
   int32_t lo;          /* memory-variable slab: indices [0, lo) ...            */
   int32_t hi;          /* ... and [n-hi, n) of this axis; elsewhere the CPML
-                          correction is the identity and is not stored        */
+                          correction is the identity and is not stored (split
+                          PML: the slabs of the split-field shell)            */
   const void* coef;    /* 6*n values (field type): b, a, k at integer points,
                           then b_half, a_half, k_half                          */
   const void* damp;    /* 2*n values: d, d_half (split PML only, else NULL)    */
@@ -125,7 +126,15 @@ typedef struct sw2d_desc {
  *   sxx_dx sxy_dx sxz_dx dvx_dx dvy_dx dvz_dx;
  * mem[1] = y, (6, nx, lo+hi, nz): sxy_dy syy_dy syz_dy dvy_dy dvx_dy dvz_dy;
  * mem[2] = z, (6, nx, ny, lo+hi): sxz_dz syz_dz szz_dz dvz_dz dvx_dz dvy_dz.
- * Split PML: split = (24, nx, ny, nz) split fields. */
+ * Split PML: the 24 split fields (vx_x vx_y vx_z vy_x vy_y vy_z vz_x vz_y vz_z
+ * sxx_x sxx_y sxx_z syy_x syy_y syy_z sxy_x sxy_y sxz_x sxz_z syz_y syz_z szz_x
+ * szz_y szz_z) are stored only on the PML shell: split = (24, S), where the
+ * shell is the union of the axes' slabs [0, lo) and [n-hi, n) and its S cells
+ * are ordered as the x slabs (sx, ny, nz), then the y slabs of the x interior
+ * (nx-sx, sy, nz), then the z slabs of the x-y interior (nx-sx, ny-sy, sz),
+ * with s_d = lo_d + hi_d and S = sx*ny*nz + (nx-sx)*sy*nz + (nx-sx)*(ny-sy)*sz.
+ * For the split PML, lo and hi of each axis must cover every index whose
+ * predicate flag is set (sw_plan_create checks it). */
 typedef struct sw3d_desc {
   int32_t scheme, dtype, nx, ny, nz, order;
   int32_t nt_max;

@@ -6,10 +6,17 @@ dense field):
   rho lam mu                          (nx, ny, nz) each
   CPML memory variables               slab-compact, 6 per direction:
       _mem[0] (6, Lx+Rx, ny, nz), _mem[1] (6, nx, Ly+Ry, nz), _mem[2] (6, nx, ny, Lz+Rz)
-  split-PML fields                    (24, nx, ny, nz)
+  split-PML fields                    (24, S) on the PML shell (shell_size)
   data                                (nt, nrec) float32 receiver traces
-The reference's full-grid memory arrays (memory_sxx_dx, ...) are still readable
-as attributes; they are expanded from the slabs on access.
+The reference's full-grid memory arrays (memory_sxx_dx, ...) and split fields
+(vx_x, ...) are still readable as attributes; they are expanded from the slabs
+or the shell on access.
+
+The split-PML shell is the union of the axes' slabs [0, lo) and [n-hi, n)
+(pml.flag_extent of the predicate flags): the x slabs (sx, ny, nz) first, then
+the y slabs of the x interior (nx-sx, sy, nz), then the z slabs of the x-y
+interior (nx-sx, ny-sy, sz), s_d = lo_d + hi_d.  The split kernels index it the
+same way (shell_index in csrc/sw_device.cuh).
 """
 from __future__ import annotations
 
@@ -39,6 +46,35 @@ SPLIT3 = ("vx_x", "vx_y", "vx_z", "vy_x", "vy_y", "vy_z", "vz_x", "vz_y", "vz_z"
           "szz_x", "szz_y", "szz_z")
 
 AXES = ("x", "y", "z")
+
+
+def shell_size(grid, lohi) -> int:
+    """Cells in the split-PML shell of a grid whose axes have slabs lohi[d] = (lo, hi)."""
+    (nx, ny, nz), s = grid, [lo + hi for lo, hi in lohi]
+    return s[0] * ny * nz + (nx - s[0]) * s[1] * nz + (nx - s[0]) * (ny - s[1]) * s[2]
+
+
+def _slab_indices(n, lo, hi, dev):
+    return torch.cat([torch.arange(lo, device=dev), torch.arange(n - hi, n, device=dev)])
+
+
+def shell_to_full(src: torch.Tensor, grid, lohi) -> torch.Tensor:
+    """One split component (S,) on the shell as a full (nx, ny, nz) grid, zero
+    outside the shell."""
+    nx, ny, nz = grid
+    (l0, h0), (l1, h1), (l2, h2) = lohi
+    s0, s1, s2 = l0 + h0, l1 + h1, l2 + h2
+    dev = src.device
+    out = torch.zeros(grid, dtype=src.dtype, device=dev)
+    a = s0 * ny * nz
+    b = (nx - s0) * s1 * nz
+    out[_slab_indices(nx, l0, h0, dev)] = src[:a].view(s0, ny, nz)
+    xi = torch.arange(l0, nx - h0, device=dev)
+    yi = torch.arange(l1, ny - h1, device=dev)
+    out[xi[:, None], _slab_indices(ny, l1, h1, dev)[None, :]] = src[a:a + b].view(nx - s0, s1, nz)
+    out[xi[:, None, None], yi[None, :, None], _slab_indices(nz, l2, h2, dev)[None, None, :]] = \
+        src[a + b:].view(nx - s0, ny - s1, s2)
+    return out
 
 
 class Elastic3DBase:
@@ -148,13 +184,15 @@ class Elastic3DBase:
         self._tables = []
         for a in range(3):
             pr = profs[a]
-            lo, hi = P.slab_extent(pr)
+            flag = P.axis_flags(self.gridsize[a], self.star, h[a], pr.pml_min, pr.pml_max, self._np_dtype)
+            # CPML: slabs where the correction departs from the identity;
+            # split PML: slabs that hold every flagged index (the shell)
+            lo, hi = P.flag_extent(flag) if self._scheme == N.SW3D_SPML else P.slab_extent(pr)
             self._tables.append(dict(
                 lo=lo, hi=hi,
                 coef=torch.as_tensor(P.coef_table(pr, self._np_dtype), device=self._dev),
                 damp=torch.as_tensor(P.damp_table(pr, self._np_dtype), device=self._dev),
-                flag=torch.as_tensor(P.axis_flags(self.gridsize[a], self.star, h[a], pr.pml_min, pr.pml_max,
-                                                  self._np_dtype), device=self._dev),
+                flag=torch.as_tensor(flag, device=self._dev),
             ))
         self._alloc_boundary_state()
         self._plan = None
@@ -162,12 +200,16 @@ class Elastic3DBase:
     def _alloc_boundary_state(self):
         nx, ny, nz = self.gridsize
         if self._scheme == N.SW3D_SPML:
-            self._split = torch.zeros((24, nx, ny, nz), dtype=self._dt_torch, device=self._dev)
+            self._split = torch.zeros((24, shell_size(self.gridsize, self._lohi())), dtype=self._dt_torch,
+                                      device=self._dev)
             return
         s = [t["lo"] + t["hi"] for t in self._tables]
         shapes = [(6, s[0], ny, nz), (6, nx, s[1], nz), (6, nx, ny, s[2])]
         self._mem = [torch.zeros(sh, dtype=self._dt_torch, device=self._dev) if min(sh) > 0 else None
                      for sh in shapes]
+
+    def _lohi(self):
+        return [(t["lo"], t["hi"]) for t in self._tables]
 
     # ---- reference attribute access to the boundary state ------------------
     def _mem_full(self, name):
@@ -198,7 +240,7 @@ class Elastic3DBase:
         if name in SPLIT3 and self._scheme == N.SW3D_SPML:
             if self.__dict__.get("_split") is None:
                 return torch.zeros(self.gridsize, dtype=self._dt_torch, device=self._dev)
-            return self._split[SPLIT3.index(name)]
+            return shell_to_full(self._split[SPLIT3.index(name)], self.gridsize, self._lohi())
         raise AttributeError(name)
 
     # ---- free surface hooks (Elastic3D_SSG_Tensor.py:151-163) ---------------

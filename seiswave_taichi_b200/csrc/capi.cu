@@ -181,6 +181,22 @@ int check_axis(const sw_pml_axis& a, int n, const char* name, bool need_damp, in
   return SW_OK;
 }
 
+// split PML: the split fields exist only on the shell of the axes' slabs, so
+// every index whose predicate flag is set must lie in [0, lo) or [n-hi, n)
+int check_shell(const sw_pml_axis& a, int n, const char* name) {
+  std::vector<uint8_t> h(n);
+  cudaError_t e = cudaMemcpy(h.data(), a.flag, n, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(e, "split PML: reading the predicate flags");
+  for (int i = a.lo; i < n - a.hi; ++i)
+    if (h[i]) {
+      char buf[200];
+      snprintf(buf, sizeof buf, "pml axis %s: index %d is inside the split-PML predicate but outside the "
+               "slabs lo=%d hi=%d that hold the split fields", name, i, a.lo, a.hi);
+      return fail(SW_ERR_ARG, buf);
+    }
+  return SW_OK;
+}
+
 int check_receivers(const sw_receivers& r, int nfield, long long ncell, int nt_max) {
   if (r.nrec < 0) return fail(SW_ERR_ARG, "receivers: nrec < 0");
   if (r.nrec == 0) return SW_OK;
@@ -270,6 +286,8 @@ int make_p3(sw_plan* pl, const sw3d_desc* d, sw::P3<T>& p) {
   p.mcomp[1] = (long long)d->nx * p.sn[1] * d->nz;
   p.mcomp[2] = (long long)d->nx * d->ny * p.sn[2];
   p.split = (T*)d->split;
+  p.scomp = (long long)p.sn[0] * d->ny * d->nz + (long long)(d->nx - p.sn[0]) * p.sn[1] * d->nz +
+            (long long)(d->nx - p.sn[0]) * (d->ny - p.sn[1]) * p.sn[2];
   p.src_kind = d->src.kind; p.si = d->src.i; p.sj = d->src.j; p.sk = d->src.k;
   p.wav = (const T*)d->src.wavelet;
   for (int q = 0; q < 6; ++q) p.mneg[q] = -(T)(float)d->src.mt[q];
@@ -682,6 +700,7 @@ int sw3d_plan_create(const sw3d_desc* d, sw_plan** out) {
   const int ns[3] = {d->nx, d->ny, d->nz};
   for (int a = 0; a < 3; ++a) {
     if ((rc = check_axis(d->pml[a], ns[a], names[a], spml, esz)) != SW_OK) return rc;
+    if (spml && (rc = check_shell(d->pml[a], ns[a], names[a])) != SW_OK) return rc;
     if (!spml && d->pml[a].lo + d->pml[a].hi > 0 && !d->mem[a])
       return fail(SW_ERR_ARG, std::string(names[a]) + " memory variables missing");
   }

@@ -4,9 +4,10 @@
 // Inside the PML predicate each component is advanced as split parts
 //   psi_d <- ((1 - dt/2 d) psi_d + dt * term_d) / (1 + dt/2 d)
 // and the field is set to their sum; outside it the plain update is used.
-// The 24 split fields are full-grid arrays (split[24][nx][ny][nz]) that are
-// only touched inside the PML region.  One thread per cell, block 32 (z) x 8
-// (y), one x plane per blockIdx.z.
+// The 24 split fields live only on the PML shell (split[24][scomp], cells
+// ordered by shell_index); a cell whose axis predicates are all clear never
+// touches them.  One thread per cell, block 32 (z) x 8 (y), one x plane per
+// blockIdx.z.
 #include "sw_device.cuh"
 
 namespace sw {
@@ -47,7 +48,7 @@ ks_velocity(const __grid_constant__ P3<T> p, int it, int src_here) {
   if (j >= ny || k >= nz) return;
   const long long sx = (long long)ny * nz, sy = nz;
   const long long idx = (long long)i * sx + (long long)j * nz + k;
-  const long long G = (long long)nx * sx;
+  const long long G = p.scomp;
   const T dx = p.dx, dy = p.dy, dz = p.dz, dt = p.dt;
   const T hdt = (T)0.5 * dt;
   T c[N];
@@ -58,6 +59,8 @@ ks_velocity(const __grid_constant__ P3<T> p, int it, int src_here) {
   T* sp = p.split;
   const T *rho = p.rho, *dpx = p.dmp[0], *dpy = p.dmp[1], *dpz = p.dmp[2];
   const uint8_t fx = p.fl[0][i], fy = p.fl[1][j], fz = p.fl[2][k];
+  // every flagged index lies in its axis's slabs (checked when the plan is made)
+  const long long sh = (fx | fy | fz) ? shell_index(p, i, j, k) : 0;
 
   // vx :182-205
   if (i >= N && i < nx - N - 1 && j >= N + 1 && j < ny - N && k >= N + 1 && k < nz - N) {
@@ -69,12 +72,12 @@ ks_velocity(const __grid_constant__ P3<T> p, int it, int src_here) {
     if ((fx & 2) || (fy & 1) || (fz & 1)) {
       const T xn = (T)1 - hdt * dpx[nx + i], yn = (T)1 - hdt * dpy[j], zn = (T)1 - hdt * dpz[k];
       const T xd = (T)1 + hdt * dpx[nx + i], yd = (T)1 + hdt * dpy[j], zd = (T)1 + hdt * dpz[k];
-      T a = div_v((xn * sp[PVX_X * G + idx] + dsxxdx * dt * ro), xd);
-      T b = div_v((yn * sp[PVX_Y * G + idx] + dsxydy * dt * ro), yd);
-      T cc = div_v((zn * sp[PVX_Z * G + idx] + dsxzdz * dt * ro), zd);
-      sp[PVX_X * G + idx] = a;
-      sp[PVX_Y * G + idx] = b;
-      sp[PVX_Z * G + idx] = cc;
+      T a = div_v((xn * sp[PVX_X * G + sh] + dsxxdx * dt * ro), xd);
+      T b = div_v((yn * sp[PVX_Y * G + sh] + dsxydy * dt * ro), yd);
+      T cc = div_v((zn * sp[PVX_Z * G + sh] + dsxzdz * dt * ro), zd);
+      sp[PVX_X * G + sh] = a;
+      sp[PVX_Y * G + sh] = b;
+      sp[PVX_Z * G + sh] = cc;
       vx[idx] = a + b + cc;
     } else {
       vx[idx] = vx[idx] + (dsxxdx + dsxydy + dsxzdz) * dt * ro;
@@ -90,12 +93,12 @@ ks_velocity(const __grid_constant__ P3<T> p, int it, int src_here) {
     if ((fx & 1) || (fy & 2) || (fz & 1)) {
       const T xn = (T)1 - hdt * dpx[i], yn = (T)1 - hdt * dpy[ny + j], zn = (T)1 - hdt * dpz[k];
       const T xd = (T)1 + hdt * dpx[i], yd = (T)1 + hdt * dpy[ny + j], zd = (T)1 + hdt * dpz[k];
-      T a = div_v((xn * sp[PVY_X * G + idx] + dt * dsxydx * ro), xd);
-      T b = div_v((yn * sp[PVY_Y * G + idx] + dt * dsyydy * ro), yd);
-      T cc = div_v((zn * sp[PVY_Z * G + idx] + dt * dsyzdz * ro), zd);
-      sp[PVY_X * G + idx] = a;
-      sp[PVY_Y * G + idx] = b;
-      sp[PVY_Z * G + idx] = cc;
+      T a = div_v((xn * sp[PVY_X * G + sh] + dt * dsxydx * ro), xd);
+      T b = div_v((yn * sp[PVY_Y * G + sh] + dt * dsyydy * ro), yd);
+      T cc = div_v((zn * sp[PVY_Z * G + sh] + dt * dsyzdz * ro), zd);
+      sp[PVY_X * G + sh] = a;
+      sp[PVY_Y * G + sh] = b;
+      sp[PVY_Z * G + sh] = cc;
       vy[idx] = a + b + cc;
     } else {
       vy[idx] = vy[idx] + (dsxydx + dsyydy + dsyzdz) * dt * ro;
@@ -115,12 +118,12 @@ ks_velocity(const __grid_constant__ P3<T> p, int it, int src_here) {
       if ((fx & 1) || (fy & 1) || (fz & 2)) {
         const T xn = (T)1 - hdt * dpx[i], yn = (T)1 - hdt * dpy[j], zn = (T)1 - hdt * dpz[nz + k];
         const T xd = (T)1 + hdt * dpx[i], yd = (T)1 + hdt * dpy[j], zd = (T)1 + hdt * dpz[nz + k];
-        T a = div_v((xn * sp[PVZ_X * G + idx] + dt * dsxzdx * ro), xd);
-        T b = div_v((yn * sp[PVZ_Y * G + idx] + dt * dsyzdy * ro), yd);
-        T cc = div_v((zn * sp[PVZ_Z * G + idx] + dt * dszzdz * ro), zd);
-        sp[PVZ_X * G + idx] = a;
-        sp[PVZ_Y * G + idx] = b;
-        sp[PVZ_Z * G + idx] = cc;
+        T a = div_v((xn * sp[PVZ_X * G + sh] + dt * dsxzdx * ro), xd);
+        T b = div_v((yn * sp[PVZ_Y * G + sh] + dt * dsyzdy * ro), yd);
+        T cc = div_v((zn * sp[PVZ_Z * G + sh] + dt * dszzdz * ro), zd);
+        sp[PVZ_X * G + sh] = a;
+        sp[PVZ_Y * G + sh] = b;
+        sp[PVZ_Z * G + sh] = cc;
         v = a + b + cc;
       } else {
         v = v + (dsxzdx + dsyzdy + dszzdz) * dt * ro;
@@ -150,7 +153,7 @@ ks_stress(const __grid_constant__ P3<T> p, int it) {
   if (j >= ny || k >= nz) return;
   const long long sx = (long long)ny * nz, sy = nz;
   const long long idx = (long long)i * sx + (long long)j * nz + k;
-  const long long G = (long long)nx * sx;
+  const long long G = p.scomp;
   const T dx = p.dx, dy = p.dy, dz = p.dz, dt = p.dt;
   const T hdt = (T)0.5 * dt;
   T c[N];
@@ -161,6 +164,8 @@ ks_stress(const __grid_constant__ P3<T> p, int it) {
   T* sp = p.split;
   const T *lam = p.lam, *mu = p.mu, *dpx = p.dmp[0], *dpy = p.dmp[1], *dpz = p.dmp[2];
   const uint8_t fx = p.fl[0][i], fy = p.fl[1][j], fz = p.fl[2][k];
+  // every flagged index lies in its axis's slabs (checked when the plan is made)
+  const long long sh = (fx | fy | fz) ? shell_index(p, i, j, k) : 0;
 
   // normal stresses :296-333
   if (i >= N + 1 && i < nx - N && j >= N + 1 && j < ny - N && k >= N + 1 && k < nz - N) {
@@ -172,18 +177,18 @@ ks_stress(const __grid_constant__ P3<T> p, int it) {
     if ((fx | fy | fz) & 1) {
       const T xn = (T)1 - hdt * dpx[i], yn = (T)1 - hdt * dpy[j], zn = (T)1 - hdt * dpz[k];
       const T xd = (T)1 + hdt * dpx[i], yd = (T)1 + hdt * dpy[j], zd = (T)1 + hdt * dpz[k];
-      T xx = div_v((xn * sp[PSXX_X * G + idx] + dt * l2m * dvxdx), xd);
-      T xy = div_v((yn * sp[PSXX_Y * G + idx] + dt * lm * dvydy), yd);
-      T xz = div_v((zn * sp[PSXX_Z * G + idx] + dt * lm * dvzdz), zd);
-      T yx = div_v((xn * sp[PSYY_X * G + idx] + dt * lm * dvxdx), xd);
-      T yy = div_v((yn * sp[PSYY_Y * G + idx] + dt * l2m * dvydy), yd);
-      T yz = div_v((zn * sp[PSYY_Z * G + idx] + dt * lm * dvzdz), zd);
-      T zx = div_v((xn * sp[PSZZ_X * G + idx] + dt * lm * dvxdx), xd);
-      T zy = div_v((yn * sp[PSZZ_Y * G + idx] + dt * lm * dvydy), yd);
-      T zz = div_v((zn * sp[PSZZ_Z * G + idx] + dt * l2m * dvzdz), zd);
-      sp[PSXX_X * G + idx] = xx; sp[PSXX_Y * G + idx] = xy; sp[PSXX_Z * G + idx] = xz;
-      sp[PSYY_X * G + idx] = yx; sp[PSYY_Y * G + idx] = yy; sp[PSYY_Z * G + idx] = yz;
-      sp[PSZZ_X * G + idx] = zx; sp[PSZZ_Y * G + idx] = zy; sp[PSZZ_Z * G + idx] = zz;
+      T xx = div_v((xn * sp[PSXX_X * G + sh] + dt * l2m * dvxdx), xd);
+      T xy = div_v((yn * sp[PSXX_Y * G + sh] + dt * lm * dvydy), yd);
+      T xz = div_v((zn * sp[PSXX_Z * G + sh] + dt * lm * dvzdz), zd);
+      T yx = div_v((xn * sp[PSYY_X * G + sh] + dt * lm * dvxdx), xd);
+      T yy = div_v((yn * sp[PSYY_Y * G + sh] + dt * l2m * dvydy), yd);
+      T yz = div_v((zn * sp[PSYY_Z * G + sh] + dt * lm * dvzdz), zd);
+      T zx = div_v((xn * sp[PSZZ_X * G + sh] + dt * lm * dvxdx), xd);
+      T zy = div_v((yn * sp[PSZZ_Y * G + sh] + dt * lm * dvydy), yd);
+      T zz = div_v((zn * sp[PSZZ_Z * G + sh] + dt * l2m * dvzdz), zd);
+      sp[PSXX_X * G + sh] = xx; sp[PSXX_Y * G + sh] = xy; sp[PSXX_Z * G + sh] = xz;
+      sp[PSYY_X * G + sh] = yx; sp[PSYY_Y * G + sh] = yy; sp[PSYY_Z * G + sh] = yz;
+      sp[PSZZ_X * G + sh] = zx; sp[PSZZ_Y * G + sh] = zy; sp[PSZZ_Z * G + sh] = zz;
       sxx[idx] = xx + xy + xz;
       syy[idx] = yx + yy + yz;
       szz[idx] = zx + zy + zz;
@@ -201,10 +206,10 @@ ks_stress(const __grid_constant__ P3<T> p, int it) {
     if ((fx & 2) || (fy & 2) || (fz & 1)) {
       const T xn = (T)1 - hdt * dpx[nx + i], yn = (T)1 - hdt * dpy[ny + j];
       const T xd = (T)1 + hdt * dpx[nx + i], yd = (T)1 + hdt * dpy[ny + j];
-      T a = div_v((xn * sp[PSXY_X * G + idx] + dt * m4 * dvydx), xd);
-      T b = div_v((yn * sp[PSXY_Y * G + idx] + dt * m4 * dvxdy), yd);
-      sp[PSXY_X * G + idx] = a;
-      sp[PSXY_Y * G + idx] = b;
+      T a = div_v((xn * sp[PSXY_X * G + sh] + dt * m4 * dvydx), xd);
+      T b = div_v((yn * sp[PSXY_Y * G + sh] + dt * m4 * dvxdy), yd);
+      sp[PSXY_X * G + sh] = a;
+      sp[PSXY_Y * G + sh] = b;
       sxy[idx] = a + b;
     } else {
       sxy[idx] = sxy[idx] + m4 * (dvxdy + dvydx) * dt;
@@ -218,10 +223,10 @@ ks_stress(const __grid_constant__ P3<T> p, int it) {
     if ((fx & 2) || (fy & 1) || (fz & 2)) {
       const T xn = (T)1 - hdt * dpx[nx + i], zn = (T)1 - hdt * dpz[nz + k];
       const T xd = (T)1 + hdt * dpx[nx + i], zd = (T)1 + hdt * dpz[nz + k];
-      T a = div_v((xn * sp[PSXZ_X * G + idx] + dt * m4 * dvzdx), xd);
-      T b = div_v((zn * sp[PSXZ_Z * G + idx] + dt * m4 * dvxdz), zd);
-      sp[PSXZ_X * G + idx] = a;
-      sp[PSXZ_Z * G + idx] = b;
+      T a = div_v((xn * sp[PSXZ_X * G + sh] + dt * m4 * dvzdx), xd);
+      T b = div_v((zn * sp[PSXZ_Z * G + sh] + dt * m4 * dvxdz), zd);
+      sp[PSXZ_X * G + sh] = a;
+      sp[PSXZ_Z * G + sh] = b;
       sxz[idx] = a + b;
     } else {
       sxz[idx] = sxz[idx] + m4 * (dvxdz + dvzdx) * dt;
@@ -235,10 +240,10 @@ ks_stress(const __grid_constant__ P3<T> p, int it) {
     if ((fx & 1) || (fy & 2) || (fz & 2)) {
       const T yn = (T)1 - hdt * dpy[ny + j], zn = (T)1 - hdt * dpz[nz + k];
       const T yd = (T)1 + hdt * dpy[ny + j], zd = (T)1 + hdt * dpz[nz + k];
-      T a = div_v((yn * sp[PSYZ_Y * G + idx] + dt * m4 * dvzdy), yd);
-      T b = div_v((zn * sp[PSYZ_Z * G + idx] + dt * m4 * dvydz), zd);
-      sp[PSYZ_Y * G + idx] = a;
-      sp[PSYZ_Z * G + idx] = b;
+      T a = div_v((yn * sp[PSYZ_Y * G + sh] + dt * m4 * dvzdy), yd);
+      T b = div_v((zn * sp[PSYZ_Z * G + sh] + dt * m4 * dvydz), zd);
+      sp[PSYZ_Y * G + sh] = a;
+      sp[PSYZ_Z * G + sh] = b;
       syz[idx] = a + b;
     } else {
       syz[idx] = syz[idx] + m4 * (dvydz + dvzdy) * dt;

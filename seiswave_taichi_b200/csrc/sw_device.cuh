@@ -42,7 +42,8 @@ struct P3 {
   int lo[3], hi[3], sn[3];  // slab widths and sn = lo+hi
   T* mem[3];
   long long mcomp[3];       // elements between two components of mem[d]
-  T* split;                 // SPML: 24 full-grid arrays
+  T* split;                 // SPML: 24 components over the PML shell (shell_index)
+  long long scomp;          // SPML: cells in the shell = elements per component
   // source
   int src_kind, si, sj, sk;
   const T* wav;
@@ -97,6 +98,23 @@ struct Batch2 {
 
 template <typename T>
 __device__ __forceinline__ T ldg(const T* p) { return __ldg(p); }
+
+// Position of cell (i, j, k) in the split-PML shell, the union of the three
+// axes' slabs [0, lo) and [n-hi, n): first the x slabs over the whole (y, z)
+// plane, then the y slabs of the x interior, then the z slabs of the x-y
+// interior, z fastest in each part.  Valid for cells inside some slab.
+template <typename T>
+__device__ __forceinline__ long long shell_index(const P3<T>& p, int i, int j, int k) {
+  const int ix = slab_index(i, p.nx, p.lo[0], p.hi[0]);
+  if (ix >= 0) return ((long long)ix * p.ny + j) * p.nz + k;
+  const long long a = (long long)p.sn[0] * p.ny * p.nz;
+  const long long i2 = i - p.lo[0];
+  const int iy = slab_index(j, p.ny, p.lo[1], p.hi[1]);
+  if (iy >= 0) return a + (i2 * p.sn[1] + iy) * p.nz + k;
+  const long long b = (long long)(p.nx - p.sn[0]) * p.sn[1] * p.nz;
+  const int iz = slab_index(k, p.nz, p.lo[2], p.hi[2]);
+  return a + b + (i2 * (p.ny - p.sn[1]) + (j - p.lo[1])) * p.sn[2] + iz;
+}
 
 // x / d for a positive divisor that varies per cell (density, kappa, split-PML
 // denominators).  A zero numerator -- most of the grid ahead of the wavefront

@@ -163,6 +163,26 @@ def slab_extent(prof: AxisProfile) -> tuple[int, int]:
     return lo, hi
 
 
+def flag_extent(flags: np.ndarray) -> tuple[int, int]:
+    """(lo, hi): leading and trailing index ranges that hold every index whose
+    PML predicate flag (axis_flags, either bit) is set -- the slabs of the
+    split-field PML's shell."""
+    f = np.asarray(flags) != 0
+    n = f.size
+    if not f.any():
+        return 0, 0
+    lo = 0
+    while lo < n and f[lo]:
+        lo += 1
+    hi = 0
+    while hi < n - lo and f[n - 1 - hi]:
+        hi += 1
+    inner = np.nonzero(f[lo:n - hi])[0]
+    if inner.size:
+        lo = lo + int(inner.max()) + 1
+    return lo, hi
+
+
 def coef_table(prof: AxisProfile, dtype=np.float32) -> np.ndarray:
     """Rows b, a, k, b_half, a_half, k_half, concatenated (6*n values)."""
     a = prof.arrays
