@@ -196,14 +196,16 @@ SW_API int sw_plan_info(sw_plan* plan, int32_t* info);
  * Every path gives the same result bit for bit. */
 SW_API int sw_plan_set_path(sw_plan* plan, int32_t path, int32_t chunk_len);
 
-/* Free-surface mode of a 2D plan: when on != 0 every step first applies the
- * reference's free-surface hook AEA (sxx = 0 on the x layer N,
- * Elastic2D_CPML.py:122-125), as a driver loop `AEA(); update_SSG_VS(i)` does
- * (Relay_wave.py:55-59); inside sw_run the hooks of all but the first step
- * are folded into the previous stress pass.  Pair it with AEA_init (lambda =
- * 0 and rho halved on the first N x layers), which the Python class applies
- * to the material arrays.  3D plans: SW_ERR_UNSUPPORTED (the reference's 3D
- * hook is never called). */
+/* Free-surface mode: when on != 0 every step first applies the reference's
+ * free-surface hook AEA, as a driver loop `AEA(); update_SSG_VS(i)` does
+ * (Relay_wave.py:55-59).  2D: sxx = 0 on the x layer N (Elastic2D_CPML.py:
+ * 122-125); inside sw_run the hooks of all but the first step are folded into
+ * the previous stress pass.  3D: szz = 0 on the z layer N
+ * (Elastic3D_SSG_Tensor.py:160-163), one small kernel at the start of each
+ * step (the two-step fused path is not used in this mode).  Pair it with
+ * AEA_init (lambda = 0 and rho halved on the first N layers), which the
+ * Python classes apply to the material arrays.  The adjoint entry points
+ * refuse plans in this mode (SW_ERR_UNSUPPORTED). */
 SW_API int sw_plan_set_free_surface(sw_plan* plan, int32_t on);
 
 /* Numeric mode of the staged path.  exact != 0: every operation rounds in

@@ -130,6 +130,7 @@ class Elastic3DBase:
         self.zmin_pml, self.zmax_pml = self.zmin, self.zmax
         self._prof = None
         self._plan = None
+        self._free_surface = False
         self._mem = [None, None, None]
         self._split = None
 
@@ -315,6 +316,8 @@ class Elastic3DBase:
         keep += [self._rec_index, self.data]
         self._plan = N.Plan(d, keep, three_d=True)
         self._plan.set_exact(self.exact)
+        if self._free_surface:
+            self._plan.set_free_surface(True)
         return self._plan
 
     def _stream(self) -> int:
@@ -326,9 +329,24 @@ class Elastic3DBase:
         plan = self._plan or self._build_plan()
         plan.step(int(nt), self._stream())
 
-    def run(self, nt=None, it0: int = 0, use_graph: bool = True):
+    def set_free_surface(self, on: bool = True):
+        """Free-surface mode (no reference counterpart as a mode): every
+        update_SSG / update_SSG_SPML step and every run() step first applies
+        AEA (szz = 0 on the z layer `star`), as a driver loop
+        `AEA(); update_SSG(i)` would; in run() the hook is one kernel of the
+        captured step.  Call AEA_init() once for the material part of the
+        condition.  The adjoint (forward_op) does not cover this mode."""
+        self._free_surface = bool(on)
+        if self._plan is not None:
+            self._plan.set_free_surface(self._free_surface)
+        return self
+
+    def run(self, nt=None, it0: int = 0, use_graph: bool = True, free_surface=None):
         """Steps it0 .. it0+nt-1 in one enqueue (CUDA graph), the drivers'
-        `for i in range(nt): test.update_SSG(i)` loop."""
+        `for i in range(nt): test.update_SSG(i)` loop; free_surface=True/False
+        sets the free-surface mode first (set_free_surface)."""
+        if free_surface is not None:
+            self.set_free_surface(free_surface)
         nt = self.nt - it0 if nt is None else int(nt)
         plan = self._plan or self._build_plan()
         plan.run(int(it0), nt, use_graph, self._stream())

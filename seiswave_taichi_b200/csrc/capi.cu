@@ -23,6 +23,7 @@ template <typename T> cudaError_t sw3_velocity(const P3<T>&, int, int, bool, boo
 template <typename T> cudaError_t sw3_stress(const P3<T>&, int, int, bool, cudaStream_t);
 template <typename T> cudaError_t sw3_moment_inject(const P3<T>&, int, cudaStream_t);
 template <typename T> cudaError_t sw3_force_inject(const P3<T>&, int, cudaStream_t);
+template <typename T> cudaError_t sw3_aea(const P3<T>&, int, cudaStream_t);
 template <typename T> cudaError_t sw3_gather(const P3<T>&, int, cudaStream_t);
 template <typename T> cudaError_t sw3_spml_step(const P3<T>&, int, int, bool, cudaStream_t);
 template <typename T> cudaError_t sw2_step(const P2<T>&, int, int, int, T, bool, bool, bool, int, cudaStream_t);
@@ -151,7 +152,7 @@ struct sw_plan {
   // per run)
   int path = 0;
   unsigned int* d_bar = nullptr;  // 2D persistent path: grid-barrier arrival and generation words
-  bool aea = false;               // 2D free-surface hook before every step (sw_plan_set_free_surface)
+  bool aea = false;               // free-surface hook before every step (sw_plan_set_free_surface)
 };
 
 namespace {
@@ -351,6 +352,12 @@ cudaError_t enqueue3(sw_plan* pl, const sw::P3<T>& p, int it, bool first, bool l
   cudaError_t e = cudaSuccess;
   sw::P3<T> q = p;
   if (!pl->gather_in_stress) q.nrec = 0;
+  // free surface: szz = 0 on the layer k = N before the step, as a driver
+  // loop `AEA(); update_SSG(i)` does
+  if (pl->aea) {
+    e = sw::sw3_aea<T>(p, pl->order, st);
+    if (e != cudaSuccess) return e;
+  }
   if (pl->scheme == SW3D_SPML) {
     e = sw::sw3_spml_step<T>(q, pl->order, it, pl->gather_in_stress, st);
     if (e == cudaSuccess && !pl->gather_in_stress) e = sw::sw3_gather<T>(p, it, st);
@@ -358,16 +365,19 @@ cudaError_t enqueue3(sw_plan* pl, const sw::P3<T>& p, int it, bool first, bool l
   }
   const bool tensor = pl->scheme == SW3D_CPML_TENSOR;
   const bool moment = pl->src_kind == SW_SRC_MOMENT;
+  // a moment source on the free-surface layer must follow that layer's
+  // zeroing, so it is not folded into the previous stress pass
+  const bool unfold = pl->aea && p.sk == pl->order;
   // moment tensor: the stress pass of step it-1 already added step it's
   // source unless this is the first step of the sequence
-  if (moment && (first || !pl->src_in_kernel)) {
+  if (moment && (first || !pl->src_in_kernel || unfold)) {
     e = sw::sw3_moment_inject<T>(p, it, st);
     if (e != cudaSuccess) return e;
   }
   const bool force = pl->src_kind == SW_SRC_FORCE;
   if constexpr (std::is_same<T, float>::value) {
     if (pl->path >= 1 && pl->staged) {
-      const bool inject_next = moment && !last;
+      const bool inject_next = moment && !last && !unfold;
       e = sw::sw3_staged_step(pl->staged_N, tensor, p, pl->svm, pl->ssm, pl->sa, pl->staged_grid, it, force,
                               inject_next, pl->gather_in_stress, st);
       if (e != cudaSuccess) return e;
@@ -381,7 +391,7 @@ cudaError_t enqueue3(sw_plan* pl, const sw::P3<T>& p, int it, bool first, bool l
     e = sw::sw3_force_inject<T>(p, it, st);
     if (e != cudaSuccess) return e;
   }
-  const bool inject_next = moment && pl->src_in_kernel && !last;
+  const bool inject_next = moment && pl->src_in_kernel && !last && !unfold;
   e = sw::sw3_stress<T>(q, pl->order, it, inject_next, st);
   if (e != cudaSuccess) return e;
   if (!pl->gather_in_stress) e = sw::sw3_gather<T>(p, it, st);
@@ -605,7 +615,7 @@ cudaError_t persistent_run2(sw_plan* pl, int it0, int nsteps, cudaStream_t st) {
 }
 
 cudaError_t enqueue_sequence(sw_plan* pl, int it0, int nsteps, cudaStream_t st) {
-  if (pl->fused && pl->path == 2 && nsteps >= 2) return enqueue_fused_run(pl, it0, nsteps, st);
+  if (pl->fused && pl->path == 2 && nsteps >= 2 && !pl->aea) return enqueue_fused_run(pl, it0, nsteps, st);
   for (int s = 0; s < nsteps; ++s) {
     cudaError_t e = enqueue_step(pl, it0 + s, s == 0, s == nsteps - 1, false, 0.0, st);
     if (e != cudaSuccess) return e;
@@ -805,7 +815,6 @@ int sw_plan_set_path(sw_plan* pl, int32_t path, int32_t chunk_len) {
 
 int sw_plan_set_free_surface(sw_plan* pl, int32_t on) {
   if (!pl) return fail(SW_ERR_ARG, "null plan");
-  if (pl->dim != 2) return fail(SW_ERR_UNSUPPORTED, "the free-surface hook is built for 2D plans");
   const bool v = on != 0;
   if (v != pl->aea && pl->gexec) { cudaGraphExecDestroy(pl->gexec); pl->gexec = nullptr; pl->g_it0 = pl->g_n = -1; }
   pl->aea = v;
@@ -927,6 +936,7 @@ int adjoint_plan_ok(sw_plan* pl, const char* who) {
     return fail(SW_ERR_UNSUPPORTED, std::string(who) + ": the adjoint covers the 2D SSG_VS and SSG_SV schemes");
   if (pl->src_kind != SW_SRC_MOMENT && pl->src_kind != SW_SRC_NONE)
     return fail(SW_ERR_UNSUPPORTED, std::string(who) + ": the adjoint covers moment-tensor sources");
+  if (pl->aea) return fail(SW_ERR_UNSUPPORTED, std::string(who) + ": the adjoint does not cover the free-surface mode");
   return SW_OK;
 }
 
@@ -988,6 +998,7 @@ int adjoint3_plan_ok(sw_plan* pl, const char* who) {
     return fail(SW_ERR_UNSUPPORTED,
                 std::string(who) + ": the 3D adjoint covers the CPML moment-tensor and point-force schemes");
   if (pl->order > 4) return fail(SW_ERR_UNSUPPORTED, std::string(who) + ": the 3D adjoint covers orders 1..4");
+  if (pl->aea) return fail(SW_ERR_UNSUPPORTED, std::string(who) + ": the adjoint does not cover the free-surface mode");
   return SW_OK;
 }
 

@@ -539,6 +539,18 @@ cudaError_t sw3_force_inject(const P3<T>& p, int it, cudaStream_t st) {
   k3_force_inject<T><<<1, 1, 0, st>>>(p, it);
   return cudaGetLastError();
 }
+// free-surface hook (Elastic3D_SSG_Tensor.py:160-163): szz = 0 on the z layer kz
+template <typename T>
+__global__ void k3_aea(T* szz, long long nxy, int nz, int kz) {
+  const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (c < nxy) szz[c * nz + kz] = (T)0;
+}
+template <typename T>
+cudaError_t sw3_aea(const P3<T>& p, int kz, cudaStream_t st) {
+  const long long nxy = (long long)p.nx * p.ny;
+  k3_aea<T><<<(unsigned)((nxy + 255) / 256), 256, 0, st>>>(p.f[5], nxy, p.nz, kz);
+  return cudaGetLastError();
+}
 template <typename T>
 cudaError_t sw3_gather(const P3<T>& p, int it, cudaStream_t st) {
   if (p.nrec <= 0) return cudaSuccess;
@@ -554,6 +566,8 @@ template cudaError_t sw3_moment_inject<float>(const P3<float>&, int, cudaStream_
 template cudaError_t sw3_moment_inject<double>(const P3<double>&, int, cudaStream_t);
 template cudaError_t sw3_force_inject<float>(const P3<float>&, int, cudaStream_t);
 template cudaError_t sw3_force_inject<double>(const P3<double>&, int, cudaStream_t);
+template cudaError_t sw3_aea<float>(const P3<float>&, int, cudaStream_t);
+template cudaError_t sw3_aea<double>(const P3<double>&, int, cudaStream_t);
 template cudaError_t sw3_gather<float>(const P3<float>&, int, cudaStream_t);
 template cudaError_t sw3_gather<double>(const P3<double>&, int, cudaStream_t);
 

@@ -74,3 +74,61 @@ def test_free_surface_mode_off_again(cuda):
     b.run(60)
     for f in F2:
         _eq(f, to_np(getattr(a, f)), to_np(getattr(b, f)))
+
+
+F3 = ("vx", "vy", "vz", "sxx", "syy", "szz", "sxy", "sxz", "syz")
+
+
+@pytest.mark.parametrize("kw", [dict(scheme="TENSOR"), dict(scheme="TENSOR", src_on_surface=True),
+                                dict(scheme="CPML"), dict(scheme="SPML"), dict(scheme="TENSOR", path="fused"),
+                                dict(scheme="TENSOR", dtype=np.float64)],
+                         ids=["tensor", "tensor-src-k=N", "cpml", "spml", "tensor-fused", "tensor-f64"])
+def test_free_surface_3d_equals_hooked_loop_and_oracle(cuda, kw):
+    """3D: szz = 0 on the z layer N before every step (Elastic3D_SSG_Tensor.py:
+    160-163) as one kernel of the captured step; a moment source on that layer
+    is injected after the zeroing, and the fused path steps aside."""
+    from cases import case3d, oracle3d, product3d
+    kw = dict(kw)
+    on_surface = kw.pop("src_on_surface", False)
+    path = kw.pop("path", None)
+    nt = 70
+    c = case3d(nt=nt, N=2, **kw)
+    if on_surface:
+        c["isz"] = c["N"]
+    N = c["N"]
+    a = product3d(c)
+    a.AEA_init()
+    if path:
+        a._build_plan().set_path(path)
+    a.set_free_surface(True)
+    a.run(30)
+    a.run(nt - 30, it0=30)
+    b = product3d(c)
+    b.AEA_init()
+    for it in range(nt):
+        b.AEA()
+        b._step(it)
+    for f in F3:
+        _eq(f, to_np(getattr(a, f)), to_np(getattr(b, f)))
+    _eq("data", to_np(a.data), to_np(b.data))
+    o = oracle3d(c, wavelet=to_np(a._wavelet).astype(np.float32))
+    o.lam[:, :, :N] = 0
+    o.rho[:, :, :N] *= 0.5
+    for it in range(nt):
+        o.szz[:, :, N] = 0
+        o.run(it, 1)
+    for f in F3:
+        _eq(f, to_np(getattr(a, f)), getattr(o, f))
+    _eq("data", to_np(a.data), o.data)
+    assert np.abs(o.vx).max() > 0
+
+
+def test_free_surface_3d_refused_by_the_adjoint(cuda):
+    import torch
+    from cases import case3d, product3d
+    c = case3d(scheme="TENSOR", nt=20, N=2)
+    w = product3d(c)
+    w.set_free_surface(True)
+    vp, vs, rho = (torch.as_tensor(c[k], device="cuda") for k in ("vp", "vs", "rho"))
+    with pytest.raises(RuntimeError, match="free-surface"):
+        w.forward_op(vp, vs, rho, checkpoint_every=10)
