@@ -3,6 +3,9 @@
 * sw3d_mlp_grad / sw3d_mlp_forward equal the float64 numpy reference
   (oracle/mlp_ref.py, 33 inputs, 9 outputs) within 2e-4 / 1e-5 relative.
 * Layer tables: every cell within 6 of a face, once, with its nearest face.
+* The correction kernel (sw3d_abc_correct) gives every layer
+  cell's nine corrections within 1e-5 relative of the float64 numpy network
+  on that cell's inputs (sw3d_abc_features), for cells of all six faces.
 * An untrained network leaves the thin CPML run unchanged bit for bit.
 * The through-the-loop gradient (correction adjoints + 3D step adjoints +
   sw3d_mlp_backward) equals central finite differences of the float32
@@ -57,6 +60,48 @@ def test_mlp3_kernels_match_reference(cuda, n):
     assert np.linalg.norm(g - g_ref) <= 2e-4 * np.linalg.norm(g_ref)
     y_ref = mlp_ref.forward(p, X, NI, NH, NO)[0]
     assert np.abs(out.cpu().numpy() - y_ref).max() <= 1e-5 * max(1.0, np.abs(y_ref).max())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape", [(20, 18, 22), (17, 16, 19)])
+def test_correction_equals_reference_network(cuda, shape):
+    from seiswave_taichi_b200.learned_abc3d import FIELDS, LearnedABC3D, solver3d
+    vp, vs, rho = _model(max(shape), 3)
+    vp, vs, rho = (m[: shape[0], : shape[1], : shape[2]].copy() for m in (vp, vs, rho))
+    rng = np.random.default_rng(sum(shape))
+    p = (rng.standard_normal((6, mlp_ref_params())) * 0.3).astype(np.float32)
+    scale = (1e-3,) * 3 + (1e3,) * 6
+    oscale = tuple(float(v) for v in rng.uniform(0.5, 2.0, 9))
+    abc = LearnedABC3D(p, scale=scale, oscale=oscale)
+    w = solver3d(vp, vs, rho, 10.0, 1e-3, shape[0] // 2, shape[1] // 2, shape[2] // 2, 10)
+    w._build_plan()
+    for f, s_ in zip(FIELDS, scale):
+        getattr(w, f).copy_(torch.as_tensor(rng.standard_normal(shape).astype(np.float32) * s_, device="cuda"))
+    X = abc.features(w).cpu().numpy().astype(np.float64)
+    before = [getattr(w, f).clone() for f in FIELDS]
+    abc.correct(w)
+    torch.cuda.synchronize()
+    _, delta = abc._cache[w.gridsize]
+    got = delta.cpu().numpy().astype(np.float64)
+    from seiswave_taichi_b200.learned_abc3d import layer_cells3
+    cell, face, _ = layer_cells3(*shape)
+    want = np.zeros_like(got)
+    for f in range(6):
+        m = face == f
+        want[m] = mlp_ref.forward(p[f].astype(np.float64), X[m], NI, NH, NO)[0] * np.asarray(oscale)
+    assert set(face.tolist()) == set(range(6))
+    err = np.abs(got - want).max() / np.abs(want).max()
+    assert err <= 1e-5, err
+    # the correction is added to the fields of the layer cells
+    for q, f in enumerate(FIELDS):
+        d = (getattr(w, f) - before[q]).reshape(-1).cpu().numpy().astype(np.float64)
+        tol = 1e-6 * float(before[q].abs().max()) + 1e-5 * np.abs(want[:, q]).max()
+        assert np.abs(d[cell] - want[:, q]).max() <= tol, f
+
+
+def mlp_ref_params():
+    from seiswave_taichi_b200 import _native as N
+    return N.SW_ABC3_PARAMS
 
 
 def _model(n, seed):
