@@ -338,6 +338,47 @@ class ElasticWAVE:
     def check_finite(self) -> int:
         return self._plan(N.SW2D_SSG_VS).check_finite(self._stream())
 
+    # ---- stability, checked runs, checkpoint/resume (no reference counterpart)
+    def courant(self) -> float:
+        """Stability number vp_max*dt*sqrt(1/dx^2 + 1/dz^2)*sum|c| of the
+        staggered scheme; the run is stable when it is <= 1."""
+        return P.courant_check(float(self.vp.max()), self.dt, (self.dx, self.dz), as_numpy(self.c))
+
+    def run_checked(self, nt=None, it0: int = 0, every: int = 100, **run_kw):
+        """run() in segments of `every` steps with a NaN/Inf scan of the
+        wavefields after each; raises state.NonFiniteError (with the step)
+        instead of running on with a blown-up state."""
+        from . import state
+        state.run_checked(self, self.nt - it0 if nt is None else int(nt), it0, every, **run_kw)
+        return self
+
+    def _state_arrays(self):
+        d = {f: getattr(self, f) for f in FIELDS2}
+        d.update({f"mem{a}": m for a, m in enumerate(self._mem)})
+        d["data"] = self.data
+        return d
+
+    def _fingerprint(self):
+        if self._prof is None:
+            raise RuntimeError("call SetADEPML2D(pml_surface, parameter) before saving or loading a state")
+        return {"class": "Elastic2D_CPML", "grid": list(self.gridsize), "dtype": str(self._dt_torch),
+                "order": self.star, "h": [float(self.dx), float(self.dz)], "dt": float(self.dt), "nt": self.nt,
+                "slabs": [[t["lo"], t["hi"]] for t in self._tables], "data": list(self.data.shape)}
+
+    def save_state(self, path, it: int):
+        """Write the state after steps 0..it-1 (it = the next step) to an
+        .npz file (state.write)."""
+        from . import state
+        torch.cuda.current_stream(self._dev).synchronize()
+        state.write(path, self._state_arrays(), {"config": self._fingerprint(), "it": int(it)})
+
+    def load_state(self, path) -> int:
+        """Load a state written by save_state for this configuration; returns
+        the next step index (resume with run(nt - it, it0=it))."""
+        from . import state
+        torch.cuda.current_stream(self._dev).synchronize()
+        return int(state.read(path, self._state_arrays(), self._fingerprint())["it"])
+
     def set_model(self, vp, vs, rho, non_blocking: bool = True):
         """Load a new model of the same shape into the solver's own arrays
         (host->device copy for host inputs) and recompute mu and lam."""
