@@ -5,7 +5,7 @@ The solver grid ends in a thin CPML of SW_ABC_DEPTH (6) cells built by the
 reference's SetADEPML2D (Elastic2D_CPML.py:392-528); after every time step a
 small network per face corrects the five fields of the outer 6 cells from
 their 3x3 stencils (sw2d_abc_correct).  Plain thin CPML is the fallback (run
-without the network) and a 20-cell CPML is the judge of reflected energy.
+without the network) and a 20-cell CPML is the yardstick for reflected energy.
 
 Training runs through the time loop with this library's own kernels: the
 thin solver with the network runs forward with per-step snapshots
@@ -196,12 +196,12 @@ def evaluate(abc: LearnedABC2D, vp, vs, rho, isx, isz, nt, h=10.0, dt=1e-3, N_=2
     from the grid edge, of the final (vx, vz) and of the vz traces of a
     receiver line at z = margin: the thin 6-cell CPML with the network
     ("net") and without it ("plain"), and the same interior with a 20-cell
-    CPML ("cpml20", the judge)."""
+    CPML ("cpml20", the yardstick)."""
     nx, nz = vp.shape
     rx = np.arange(margin, nx - margin, 2, dtype=np.int64)
     rz = np.full(rx.size, margin, np.int64)
     truth, d_true = truth_run(vp, vs, rho, h, dt, isx, isz, nt, N_, freq, pad, rec=(rx, rz))
-    judge, d_judge = truth_run(vp, vs, rho, h, dt, isx, isz, nt, N_, freq, 20 - L, rec=(rx, rz))
+    thick, d_thick = truth_run(vp, vs, rho, h, dt, isx, isz, nt, N_, freq, 20 - L, rec=(rx, rz))
     sl = (slice(margin, nx - margin), slice(margin, nz - margin))
     ref = truth[nt][:2][(slice(None),) + sl]
 
@@ -214,7 +214,7 @@ def evaluate(abc: LearnedABC2D, vp, vs, rho, isx, isz, nt, h=10.0, dt=1e-3, N_=2
         w = _solver(vp, vs, rho, h, dt, isx, isz, nt, N_, freq, L, "explosive", 1e5, rec=(rx, rz))
         abc.run(w, nt, net=tag == "net")
         out[tag], out[tag + "_traces"] = err(torch.stack([w.vx[sl], w.vz[sl]]), w.data)
-    out["cpml20"], out["cpml20_traces"] = err(judge[nt][:2][(slice(None),) + sl], d_judge)
+    out["cpml20"], out["cpml20_traces"] = err(thick[nt][:2][(slice(None),) + sl], d_thick)
     return out
 
 

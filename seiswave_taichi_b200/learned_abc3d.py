@@ -6,7 +6,7 @@ The solver grid ends in a 6-cell CPML built by the reference's SetADEPML3D
 face (six faces) corrects the nine fields of the outer 6 cells from the
 fields at the cell and its two neighbours along the face's inward normal
 (sw3d_abc_correct).  Plain thin CPML is the fallback (run without the
-network); a 20-cell CPML is the judge.
+network); a 20-cell CPML is the yardstick.
 
 Training runs through the time loop with this library's kernels: forward
 steps with snapshots (sw3d_record) and stored network inputs, a vx-trace
