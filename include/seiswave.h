@@ -337,7 +337,8 @@ SW_API int sw3d_mlp_backward(const float* params, const float* x, const float* d
 /* ---- 2D adjoint (no reference counterpart) --------------------------------
  * Hand-written discrete adjoint of the SW2D_SSG_VS or SW2D_SSG_SV time loop
  * (the plan's scheme) with a SW_SRC_MOMENT (or no) source and the scheme's
- * receivers (vz for VS, vx for SV), for gradients of a seismogram
+ * receivers (vz for VS, vx for SV; plans recording another field are
+ * refused with SW_ERR_UNSUPPORTED), for gradients of a seismogram
  * misfit with respect to the material.  sw2d_record runs forward steps
  * it0..it0+nsteps-1 from the plan's current state and stores nsteps+1
  * snapshots of sw2d_snapshot_elems() elements each; sw2d_adjoint_run then

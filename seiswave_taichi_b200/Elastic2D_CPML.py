@@ -62,7 +62,7 @@ def moment_2d(MT) -> np.ndarray:
 
 class ElasticWAVE:
     def __init__(self, vs, vp, rho, dx, dz, dt, isx, isz, rsx, rsz, nt, accuracy=3, freq=100.,
-                 fieldtype=torch.float32, *, coef64=False, MT=None, src_scale=1.0):
+                 fieldtype=torch.float32, *, coef64=False, MT=None, src_scale=1.0, rec_component=None):
         self._dt_torch = torch_dtype(fieldtype)
         self._np_dtype = np.float64 if self._dt_torch == torch.float64 else np.float32
         self._dev = device()
@@ -111,6 +111,11 @@ class ElasticWAVE:
         self._mem = [None, None]
         self.MT = None if MT is None else moment_2d(MT)
         self.src_scale = float(src_scale)
+        # receivers of update_SSG_VS / update_SSG_SV: the scheme's component
+        # (vz, vx) unless a field is named
+        if rec_component is not None and rec_component not in FIELDS2:
+            raise ValueError(f"rec_component must be one of {FIELDS2}")
+        self._rec_component = rec_component
 
     # ---- reference helpers ------------------------------------------------
     def Compute_mu(self, fieldtype=None):
@@ -256,6 +261,8 @@ class ElasticWAVE:
             wav = np.zeros(self.nt, dtype=np.float32)
             d.src.kind = N.SW_SRC_RSG4
             rec_field = -1  # update_RSG records nothing
+        if rec_field >= 0 and self._rec_component is not None:
+            rec_field = FIELDS2.index(self._rec_component)
         wt = torch.as_tensor(wav, device=self._dev).to(self._dt_torch).contiguous()
         keep.append(wt)
         self._wavelets[scheme] = wt

@@ -937,6 +937,11 @@ int adjoint_plan_ok(sw_plan* pl, const char* who) {
   if (pl->src_kind != SW_SRC_MOMENT && pl->src_kind != SW_SRC_NONE)
     return fail(SW_ERR_UNSUPPORTED, std::string(who) + ": the adjoint covers moment-tensor sources");
   if (pl->aea) return fail(SW_ERR_UNSUPPORTED, std::string(who) + ": the adjoint does not cover the free-surface mode");
+  const int nrec = pl->dtype == SW_F32 ? pl->p2f.nrec : pl->p2d.nrec;
+  const int rf = pl->dtype == SW_F32 ? pl->p2f.rec_field : pl->p2d.rec_field;
+  if (nrec > 0 && rf != (pl->scheme == SW2D_SSG_VS ? 1 : 0))
+    return fail(SW_ERR_UNSUPPORTED,
+                std::string(who) + ": the adjoint covers receivers of the scheme's own component (VS: vz, SV: vx)");
   return SW_OK;
 }
 
