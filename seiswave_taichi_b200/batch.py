@@ -45,6 +45,9 @@ class ShotBatch2D:
     def __init__(self, waves, scheme: str = "VS", autotune: bool = True):
         if not waves:
             raise ValueError("empty batch")
+        if any(getattr(w, "_free_surface", False) for w in waves):
+            raise ValueError("the batch runner does not apply the free-surface hook: run shots in free-surface "
+                             "mode one by one (ElasticWAVE.run)")
         self.waves = list(waves)
         self.scheme = {"VS": N.SW2D_SSG_VS, "SV": N.SW2D_SSG_SV}[scheme]
         plans = [w._plan(self.scheme) for w in self.waves]
