@@ -246,6 +246,8 @@ int choose_x_chunk(int nx, int ny, int nz) {
 // ---------------------------------------------------------------------------
 bool verified_divisor(float d, float r, cudaStream_t st) {
   static std::vector<std::pair<uint32_t, bool>> cache;
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lock(mu);
   uint32_t bits;
   memcpy(&bits, &d, 4);
   for (auto& e : cache)

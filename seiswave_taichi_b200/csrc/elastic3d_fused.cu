@@ -722,13 +722,13 @@ template <int N, int TY, int D, bool TENSOR>
 static cudaError_t launch_fused(const P3<float>& p, const FusedMaps& m, const FusedExtra& x, int grid, int it,
                                 int src, bool inject_next, int gather_it, cudaStream_t st) {
   using G = FG<N, TY, D>;
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(k3_fused<N, TY, D, TENSOR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)G::BYTES);
-    if (e != cudaSuccess) return e;
-    attr_set = true;
-  }
+  static std::atomic<unsigned long long> done{0};
+  static std::mutex mu;
+  cudaError_t e = once_per_device(done, mu, [] {
+    return cudaFuncSetAttribute(k3_fused<N, TY, D, TENSOR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)G::BYTES);
+  });
+  if (e != cudaSuccess) return e;
   k3_fused<N, TY, D, TENSOR><<<grid, G::NT, G::BYTES, st>>>(p, m, x, it, src, inject_next ? 1 : 0, gather_it);
   return cudaGetLastError();
 }

@@ -949,8 +949,9 @@ static cudaError_t staged_launch(bool tensor, const P3<float>& p, const StagedMa
                                  bool gather, cudaStream_t st) {
   constexpr int Q = staged_q(EX);
   using G = SG<N, TY, D, Q>;
-  static bool init = false;
-  if (!init) {
+  static std::atomic<unsigned long long> done{0};
+  static std::mutex mu;
+  cudaError_t e0 = once_per_device(done, mu, [] {
     cudaError_t e = cudaFuncSetAttribute(k3s_velocity<N, TY, D, true, EX, Q>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::V_BYTES);
     if (e == cudaSuccess)
@@ -959,9 +960,9 @@ static cudaError_t staged_launch(bool tensor, const P3<float>& p, const StagedMa
     if (e == cudaSuccess)
       e = cudaFuncSetAttribute(k3s_stress<N, TY, D, EX, Q>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)G::S_BYTES);
-    if (e != cudaSuccess) return e;
-    init = true;
-  }
+    return e;
+  });
+  if (e0 != cudaSuccess) return e0;
   if (tensor) k3s_velocity<N, TY, D, true, EX, Q><<<grid, G::NT, G::V_BYTES, st>>>(p, vm, a, it, 0);
   else k3s_velocity<N, TY, D, false, EX, Q><<<grid, G::NT, G::V_BYTES, st>>>(p, vm, a, it, force_here ? 1 : 0);
   k3s_stress<N, TY, D, EX, Q><<<grid, G::NT, G::S_BYTES, st>>>(p, smp, a, it, inject_next ? 1 : 0, gather ? 1 : 0);

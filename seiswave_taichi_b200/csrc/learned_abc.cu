@@ -332,13 +332,13 @@ cudaError_t abc_adjoint(const AbcArgs& a, float* const* lam_host, float* ybar, c
 
 cudaError_t abc_correct(const AbcArgs& a, cudaStream_t st) {
   if (a.ncell == 0) return cudaSuccess;
-  static bool init = false;
+  static std::atomic<unsigned long long> done{0};
+  static std::mutex mu;
   const int sm = (int)corr_smem<Net2>(4, CT2);
-  if (!init) {
-    cudaError_t e = cudaFuncSetAttribute(k_abc_delta, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    if (e != cudaSuccess) return e;
-    init = true;
-  }
+  cudaError_t e = once_per_device(done, mu, [sm] {
+    return cudaFuncSetAttribute(k_abc_delta, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  });
+  if (e != cudaSuccess) return e;
   k_abc_delta<<<corr_grid(a.ncell, CT2), CT2, sm, st>>>(a);
   k_abc_apply<<<(a.ncell + 127) / 128, 128, 0, st>>>(a);
   return cudaGetLastError();
@@ -469,13 +469,15 @@ static size_t abc3_smem() { return sizeof(float) * 6 * SW_ABC3_PARAMS; }
 static size_t abc3_tsmem() { return corr_smem<Net3>(6, CT3); }
 
 static cudaError_t abc3_init() {
-  static bool init = false;
-  if (init) return cudaSuccess;
-  cudaError_t e = cudaFuncSetAttribute(k_abc3_delta, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)abc3_tsmem());
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_abc3_xbar, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)abc3_smem());
-  if (e == cudaSuccess) init = true;
-  return e;
+  static std::atomic<unsigned long long> done{0};
+  static std::mutex mu;
+  return once_per_device(done, mu, [] {
+    cudaError_t e =
+        cudaFuncSetAttribute(k_abc3_delta, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)abc3_tsmem());
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_abc3_xbar, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)abc3_smem());
+    return e;
+  });
 }
 
 cudaError_t abc3_correct(const AbcArgs3& a, cudaStream_t st) {
@@ -635,13 +637,13 @@ static size_t mlp_grad_smem() {
 template <class NT>
 static cudaError_t mlp_grad_t(const float* params, const float* X, const float* Y, long long n, float* grad,
                               float* loss, int dy_given, cudaStream_t st) {
-  static bool init = false;
+  static std::atomic<unsigned long long> done{0};
+  static std::mutex mu;
   const size_t smem = mlp_grad_smem<NT>();
-  if (!init) {
-    cudaError_t e = cudaFuncSetAttribute(k_mlp_grad<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    init = true;
-  }
+  cudaError_t e = once_per_device(done, mu, [smem] {
+    return cudaFuncSetAttribute(k_mlp_grad<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  });
+  if (e != cudaSuccess) return e;
   if (n == 0) return cudaSuccess;
   const long long ntile = (n + MT - 1) / MT;
   const int grid = (int)std::min<long long>(ntile, 148 * 2);

@@ -7,12 +7,31 @@
 // CPU evaluation of the same expressions.
 #pragma once
 
+#include <atomic>
 #include <cstdint>
+#include <mutex>
 #include <cuda_runtime.h>
 
 #include "../../include/seiswave.h"
 
 namespace sw {
+
+// One-time setup per device (kernel attributes such as the dynamic
+// shared-memory opt-in are per device): runs f() once for each device the
+// calling threads launch on, under a lock; a failed f() is retried next time.
+template <class F>
+inline cudaError_t once_per_device(std::atomic<unsigned long long>& done, std::mutex& mu, F f) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const unsigned long long bit = 1ull << (dev & 63);
+  if (done.load(std::memory_order_acquire) & bit) return cudaSuccess;
+  std::lock_guard<std::mutex> lock(mu);
+  if (done.load(std::memory_order_acquire) & bit) return cudaSuccess;
+  e = f();
+  if (e == cudaSuccess) done.fetch_or(bit, std::memory_order_release);
+  return e;
+}
 
 // slab-compact index of `i` on an axis of length n whose CPML slabs are
 // [0, lo) and [n-hi, n); -1 outside both slabs.
