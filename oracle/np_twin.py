@@ -1,9 +1,10 @@
 """NumPy twin of the oracle (test infrastructure only).
 
-A second, independent transcription of two reference kernels, written with
-whole-array slices instead of loops:
-  * Elastic2D_CPML.update_SSG_VS   (src/Elastic2D_CPML.py:128-200)
-  * Elastic3D_SSG_Tensor.update_SSG (src/Elastic3D_SSG_Tensor.py:166-345)
+A second, independent transcription of three reference kernels, written
+with whole-array slices instead of loops:
+  * Elastic2D_CPML.update_SSG_VS        (src/Elastic2D_CPML.py:128-200)
+  * Elastic3D_SSG_Tensor.update_SSG      (src/Elastic3D_SSG_Tensor.py:166-345)
+  * Elastic3D_SSG_SPML.update_SSG_SPML   (src/Elastic3D_SSG_SPML.py:160-393)
 Every operation is an elementwise IEEE operation in the array dtype, in the
 reference's order, so on the same inputs it must agree bit for bit with the
 C++ oracle (sw_oracle.cpp).  Used on tiny grids only.
@@ -278,3 +279,140 @@ class Twin3DTensor:
         self.syz[B] = self.syz[B] + m4 * (e1 + e2) * dt
         rx, ry, rz = self.rec
         self.data[it] = self.vx[rx, ry, rz].astype(np.float32)
+
+
+class Twin3DSPML(Twin3DTensor):
+    """Elastic3D_SSG_SPML.update_SSG_SPML (src/Elastic3D_SSG_SPML.py:160-393):
+    inside the PML predicate every component is advanced as split parts
+    psi_d = ((1 - dt/2 d) psi_d + dt*term_d) / (1 + dt/2 d) (damping d only)
+    and set to their sum; outside it the plain update.  Normal stresses use
+    the cell's own lam, mu (:300-302); the point force is
+    vz[src] += dt*w / rho[src] after the velocity phase (:294); one receiver
+    records vx (:393)."""
+
+    SPLIT = ("vx_x", "vx_y", "vx_z", "vy_x", "vy_y", "vy_z", "vz_x", "vz_y", "vz_z",
+             "sxx_x", "sxx_y", "sxx_z", "syy_x", "syy_y", "syy_z",
+             "sxy_x", "sxy_y", "sxz_x", "sxz_z", "syz_y", "syz_z",
+             "szz_x", "szz_y", "szz_z")
+
+    def __init__(self, o):
+        """Build from an oracle.Oracle3D of scheme SPML."""
+        super().__init__(o)
+        self.split = {n: np.zeros_like(self.vx) for n in self.SPLIT}
+
+    def _fac(self, q, half, box):
+        """(1 - dt/2 d, 1 + dt/2 d) on axis q at the box's integer or half points."""
+        T = self.T
+        prof, _ = self.axes[q]
+        shape = [1, 1, 1]
+        shape[q] = -1
+        d = prof["pml_half" if half else "pml"][box[q]].reshape(shape)
+        hdt = T(0.5) * self.dt
+        return T(1) - hdt * d, T(1) + hdt * d
+
+    def _split(self, names, terms, halves, axes, mask, box):
+        """Advance the split parts `names` by their terms; returns their sum."""
+        total = None
+        for name, term, half, q in zip(names, terms, halves, axes):
+            n, d = self._fac(q, half, box)
+            old = self.split[name][box]
+            new = (n * old + term) / d
+            self.split[name][box] = np.where(mask, new, old)
+            total = new if total is None else total + new
+        return total
+
+    def step(self, it, w):
+        T, N, dt = self.T, self.N, self.dt
+        nx, ny, nz = self.vx.shape
+        dx, dy, dz = self.h
+        S = lambda a, b: slice(a, b)
+        r, lam, mu = self.rho, self.lam, self.mu
+        with np.errstate(all="ignore"):
+            # vx :182-205
+            B = (S(N, nx - N - 1), S(N + 1, ny - N), S(N + 1, nz - N))
+            d1 = self._d(self.sxx, B, 0, True) / dx
+            d2 = self._d(self.sxy, B, 1, False) / dy
+            d3 = self._d(self.sxz, B, 2, False) / dz
+            ro = T(1) / r[B]
+            mk = self._mask(B, (1, 0, 0))
+            sp = self._split(("vx_x", "vx_y", "vx_z"), (d1 * dt * ro, d2 * dt * ro, d3 * dt * ro),
+                             (True, False, False), (0, 1, 2), mk, B)
+            self.vx[B] = np.where(mk, sp, self.vx[B] + (d1 + d2 + d3) * dt * ro)
+            # vy :207-233
+            B = (S(N + 1, nx - N), S(N, ny - N - 1), S(N + 1, nz - N))
+            Bj = (B[0], S(N + 1, ny - N), B[2])
+            ro = T(1) / (T(0.5) * (r[B] + r[Bj]))
+            d1 = self._d(self.sxy, B, 0, False) / dx
+            d2 = self._d(self.syy, B, 1, True) / dy
+            d3 = self._d(self.syz, B, 2, False) / dz
+            mk = self._mask(B, (0, 1, 0))
+            sp = self._split(("vy_x", "vy_y", "vy_z"), (dt * d1 * ro, dt * d2 * ro, dt * d3 * ro),
+                             (False, True, False), (0, 1, 2), mk, B)
+            self.vy[B] = np.where(mk, sp, self.vy[B] + (d1 + d2 + d3) * dt * ro)
+            # vz :235-259
+            B = (S(N + 1, nx - N), S(N + 1, ny - N), S(N, nz - N - 1))
+            Bj = (B[0], S(N + 2, ny - N + 1), B[2])
+            Bij = (S(N + 2, nx - N + 1), S(N + 2, ny - N + 1), B[2])
+            Bi = (S(N + 2, nx - N + 1), B[1], B[2])
+            ro = T(1) / (T(0.25) * (r[B] + r[Bj] + r[Bij] + r[Bi]))
+            d1 = self._d(self.sxz, B, 0, False) / dx
+            d2 = self._d(self.syz, B, 1, False) / dy
+            d3 = self._d(self.szz, B, 2, True) / dz
+            mk = self._mask(B, (0, 0, 1))
+            sp = self._split(("vz_x", "vz_y", "vz_z"), (dt * d1 * ro, dt * d2 * ro, dt * d3 * ro),
+                             (False, False, True), (0, 1, 2), mk, B)
+            self.vz[B] = np.where(mk, sp, self.vz[B] + (d1 + d2 + d3) * dt * ro)
+            # point force :294
+            s = self.src
+            self.vz[s] = self.vz[s] + (dt * T(np.float32(w))) / r[s]
+            # normal stresses :296-333, the cell's own lam and mu
+            B = (S(N + 1, nx - N), S(N + 1, ny - N), S(N + 1, nz - N))
+            lm, u = lam[B], mu[B]
+            l2m = lm + T(2) * u
+            e1 = self._d(self.vx, B, 0, False) / dx
+            e2 = self._d(self.vy, B, 1, False) / dy
+            e3 = self._d(self.vz, B, 2, False) / dz
+            mk = self._mask(B, (0, 0, 0))
+            h3 = (False, False, False)
+            xyz = (0, 1, 2)
+            sxx = self._split(("sxx_x", "sxx_y", "sxx_z"), (dt * l2m * e1, dt * lm * e2, dt * lm * e3), h3, xyz,
+                              mk, B)
+            syy = self._split(("syy_x", "syy_y", "syy_z"), (dt * lm * e1, dt * l2m * e2, dt * lm * e3), h3, xyz,
+                              mk, B)
+            szz = self._split(("szz_x", "szz_y", "szz_z"), (dt * lm * e1, dt * lm * e2, dt * l2m * e3), h3, xyz,
+                              mk, B)
+            self.sxx[B] = np.where(mk, sxx, self.sxx[B] + (l2m * e1 + lm * (e3 + e2)) * dt)
+            self.syy[B] = np.where(mk, syy, self.syy[B] + (l2m * e2 + lm * (e1 + e3)) * dt)
+            self.szz[B] = np.where(mk, szz, self.szz[B] + (l2m * e3 + lm * (e1 + e2)) * dt)
+            # sxy :334-350
+            B = (S(N + 1, nx - N), S(N + 1, ny - N), S(N, nz - N))
+            Bj = (B[0], S(N + 2, ny - N + 1), B[2])
+            Bi = (S(N + 2, nx - N + 1), B[1], B[2])
+            m4 = T(0.25) * (mu[Bj] + mu[B] + mu[B] + mu[Bi])
+            e1 = self._d(self.vy, B, 0, True) / dx
+            e2 = self._d(self.vx, B, 1, True) / dy
+            mk = self._mask(B, (1, 1, 0))
+            sp = self._split(("sxy_x", "sxy_y"), (dt * m4 * e1, dt * m4 * e2), (True, True), (0, 1), mk, B)
+            self.sxy[B] = np.where(mk, sp, self.sxy[B] + m4 * (e2 + e1) * dt)
+            # sxz :352-371
+            B = (S(N, nx - N - 1), S(N, ny - N), S(N, nz - N - 1))
+            Bi = (S(N + 1, nx - N), B[1], B[2])
+            Bj = (B[0], S(N + 1, ny - N + 1), B[2])
+            m4 = T(0.25) * (mu[B] + mu[Bi] + mu[B] + mu[Bj])
+            e1 = self._d(self.vz, B, 0, True) / dx
+            e3 = self._d(self.vx, B, 2, True) / dz
+            mk = self._mask(B, (1, 0, 1))
+            sp = self._split(("sxz_x", "sxz_z"), (dt * m4 * e1, dt * m4 * e3), (True, True), (0, 2), mk, B)
+            self.sxz[B] = np.where(mk, sp, self.sxz[B] + m4 * (e3 + e1) * dt)
+            # syz :373-391
+            B = (S(N, nx - N), S(N, ny - N - 1), S(N, nz - N - 1))
+            Bj = (B[0], S(N + 1, ny - N), B[2])
+            Bk = (B[0], B[1], S(N + 1, nz - N))
+            m4 = T(0.25) * (mu[Bj] + mu[B] + mu[Bk] + mu[B])
+            e2 = self._d(self.vz, B, 1, True) / dy
+            e3 = self._d(self.vy, B, 2, True) / dz
+            mk = self._mask(B, (0, 1, 1))
+            sp = self._split(("syz_y", "syz_z"), (dt * m4 * e2, dt * m4 * e3), (True, True), (1, 2), mk, B)
+            self.syz[B] = np.where(mk, sp, self.syz[B] + m4 * (e3 + e2) * dt)
+        rx, ry, rz = self.rec
+        self.data[it] = self.vx[rx[0], ry[0], rz[0]].astype(np.float32)
