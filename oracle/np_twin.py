@@ -1,8 +1,9 @@
 """NumPy twin of the oracle (test infrastructure only).
 
-A second, independent transcription of three reference kernels, written
+A second, independent transcription of four reference kernels, written
 with whole-array slices instead of loops:
   * Elastic2D_CPML.update_SSG_VS        (src/Elastic2D_CPML.py:128-200)
+  * Elastic2D_CPML.update_RSG           (src/Elastic2D_CPML.py:277-353)
   * Elastic3D_SSG_Tensor.update_SSG      (src/Elastic3D_SSG_Tensor.py:166-345)
   * Elastic3D_SSG_SPML.update_SSG_SPML   (src/Elastic3D_SSG_SPML.py:160-393)
 Every operation is an elementwise IEEE operation in the array dtype, in the
@@ -116,6 +117,79 @@ class Twin2D:
         dvxdz = self._pml("dvx_dz", dvxdz, Z["b_half"], Z["a_half"], Z["k_half"], mk, I, J, False)
         self.sxz[I, J] = self.sxz[I, J] + mhz * (dvxdz + dvzdx) * dt
         self.data[it] = self.vz[self.rsx, self.rsz]
+
+
+class Twin2DRSG(Twin2D):
+    """Elastic2D_CPML.update_RSG (src/Elastic2D_CPML.py:277-353): rotated
+    staggered grid, velocities at (i, j), stresses at (i+1/2, j+1/2);
+    d/dx = (Drz - Drx)/(2 dx), d/dz = (Drz + Drx)/(2 dz) with the diagonal
+    differences of src/Differential2D.py:32-56; the caller's source value is
+    spread over the 2x2 block vz[isx+a, isz+b] += dt*source/(8 rho), a, b in
+    {-1, 0}; no receiver."""
+
+    # (i, j) offsets of the m-th tap's two samples, per diagonal difference
+    _TAPS = {
+        "rx_f": lambda m: ((m + 1, m + 1), (-m, -m)),
+        "rz_f": lambda m: ((-m, m + 1), (m + 1, -m)),
+        "rx_b": lambda m: ((m, m), (-m - 1, -m - 1)),
+        "rz_b": lambda m: ((-m - 1, m), (m, -m - 1)),
+    }
+
+    def _dr(self, f, I, J, kind):
+        T, N, c = self.T, self.N, self.c
+        v = np.zeros((I.stop - I.start, J.stop - J.start), T)
+        for m in range(N):
+            (ai, aj), (bi, bj) = self._TAPS[kind](m)
+            hi = f[I.start + ai:I.stop + ai, J.start + aj:J.stop + aj]
+            lo = f[I.start + bi:I.stop + bi, J.start + bj:J.stop + bj]
+            v = v + c[m] * (hi - lo)
+        return v
+
+    def step(self, it, source):
+        T, N, dt = self.T, self.N, self.dt
+        nx, nz = self.vx.shape
+        X, Z = self.X, self.Z
+        dx2, dz2 = T(2) * self.dx, T(2) * self.dz
+        # velocities at integer points (:292-320)
+        I, J = slice(N + 1, nx - N), slice(N + 1, nz - N)
+        rx = {f: self._dr(getattr(self, f), I, J, "rx_b") for f in ("sxx", "szz", "sxz")}
+        rz = {f: self._dr(getattr(self, f), I, J, "rz_b") for f in ("sxx", "szz", "sxz")}
+        dsxxdx = (rz["sxx"] - rx["sxx"]) / dx2
+        dszzdz = (rz["szz"] + rx["szz"]) / dz2
+        dsxzdx = (rz["sxz"] - rx["sxz"]) / dx2
+        dsxzdz = (rz["sxz"] + rx["sxz"]) / dz2
+        mk = self._mask(I, J, False, False)
+        dsxxdx = self._pml("sxx_dx", dsxxdx, X["b"], X["a"], X["k"], mk, I, J, True)
+        dszzdz = self._pml("szz_dz", dszzdz, Z["b"], Z["a"], Z["k"], mk, I, J, False)
+        dsxzdx = self._pml("sxz_dx", dsxzdx, X["b"], X["a"], X["k"], mk, I, J, True)
+        dsxzdz = self._pml("sxz_dz", dsxzdz, Z["b"], Z["a"], Z["k"], mk, I, J, False)
+        rho = self.rho[I, J]
+        self.vx[I, J] = self.vx[I, J] + (dsxxdx + dsxzdz) * dt / rho
+        self.vz[I, J] = self.vz[I, J] + (dszzdz + dsxzdx) * dt / rho
+        # source (:322-323)
+        s = T(np.float32(source))
+        for a in (-1, 0):
+            for b in (-1, 0):
+                i, j = self.isx + a, self.isz + b
+                self.vz[i, j] = self.vz[i, j] + dt * s / (T(8) * self.rho[i, j])
+        # stresses at half points (:325-352), the cell's own lam and mu
+        I, J = slice(N, nx - N - 1), slice(N, nz - N - 1)
+        lam, mu = self.lam[I, J], self.mu[I, J]
+        l2m = lam + T(2) * mu
+        vxrx, vxrz = self._dr(self.vx, I, J, "rx_f"), self._dr(self.vx, I, J, "rz_f")
+        vzrx, vzrz = self._dr(self.vz, I, J, "rx_f"), self._dr(self.vz, I, J, "rz_f")
+        dvxdx = (vxrz - vxrx) / dx2
+        dvxdz = (vxrz + vxrx) / dz2
+        dvzdx = (vzrz - vzrx) / dx2
+        dvzdz = (vzrz + vzrx) / dz2
+        mk = self._mask(I, J, True, True)
+        dvxdx = self._pml("dvx_dx", dvxdx, X["b_half"], X["a_half"], X["k_half"], mk, I, J, True)
+        dvxdz = self._pml("dvx_dz", dvxdz, Z["b_half"], Z["a_half"], Z["k_half"], mk, I, J, False)
+        dvzdx = self._pml("dvz_dx", dvzdx, X["b_half"], X["a_half"], X["k_half"], mk, I, J, True)
+        dvzdz = self._pml("dvz_dz", dvzdz, Z["b_half"], Z["a_half"], Z["k_half"], mk, I, J, False)
+        self.sxx[I, J] = self.sxx[I, J] + (l2m * dvxdx + lam * dvzdz) * dt
+        self.szz[I, J] = self.szz[I, J] + (l2m * dvzdz + lam * dvxdx) * dt
+        self.sxz[I, J] = self.sxz[I, J] + (mu * (dvxdz + dvzdx)) * dt
 
 
 class Twin3DTensor:

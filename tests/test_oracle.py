@@ -155,6 +155,27 @@ def test_twin_3d_tensor_bitwise(N):
 
 
 @pytest.mark.parametrize("N,dtype", [(2, np.float32), (3, np.float32), (2, np.float64)])
+def test_twin_2d_rsg_bitwise(N, dtype):
+    """The rotated-grid step (Elastic2D_CPML.py:277-353) with a caller-given
+    source value per step: oracle and numpy transcription bit for bit,
+    wavefields and the eight memory variables."""
+    from seiswave_taichi_b200 import BaseFun
+    nt = 80
+    c = case2d(shape=(48, 40), N=N, npml=6, nt=nt, dtype=dtype)
+    src = BaseFun.series("ricker", nt, c["dt"], c["freq"], 1.0)
+    o = oracle2d(c)
+    t = np_twin.Twin2DRSG(o)
+    o.run("RSG", 0, nt, rsg_sources=src.astype(np.float64))
+    for it in range(nt):
+        t.step(it, src[it])
+    for f in ("vx", "vz", "sxx", "szz", "sxz"):
+        assert np.array_equal(getattr(t, f), getattr(o, f)), f
+    for k, v in t.mem.items():
+        assert np.array_equal(v, o.memory("memory_" + k)), k
+    assert np.abs(o.vz).max() > 0 and np.abs(o.memory("memory_dvx_dx")).max() > 0
+
+
+@pytest.mark.parametrize("N,dtype", [(2, np.float32), (3, np.float32), (2, np.float64)])
 def test_twin_3d_spml_bitwise(N, dtype):
     """The split-field PML step (Elastic3D_SSG_SPML.py:160-393): the C++ oracle
     and the independent numpy transcription agree bit for bit, wavefields,
