@@ -1,10 +1,12 @@
 """NumPy twin of the oracle (test infrastructure only).
 
-A second, independent transcription of four reference kernels, written
+A second, independent transcription of six reference kernels, written
 with whole-array slices instead of loops:
   * Elastic2D_CPML.update_SSG_VS        (src/Elastic2D_CPML.py:128-200)
+  * Elastic2D_CPML.update_SSG_SV        (src/Elastic2D_CPML.py:203-274)
   * Elastic2D_CPML.update_RSG           (src/Elastic2D_CPML.py:277-353)
   * Elastic3D_SSG_Tensor.update_SSG      (src/Elastic3D_SSG_Tensor.py:166-345)
+  * Elastic3D_SSG_CPML.update_SSG        (src/Elastic3D_SSG_CPML.py:144-309)
   * Elastic3D_SSG_SPML.update_SSG_SPML   (src/Elastic3D_SSG_SPML.py:160-393)
 Every operation is an elementwise IEEE operation in the array dtype, in the
 reference's order, so on the same inputs it must agree bit for bit with the
@@ -117,6 +119,63 @@ class Twin2D:
         dvxdz = self._pml("dvx_dz", dvxdz, Z["b_half"], Z["a_half"], Z["k_half"], mk, I, J, False)
         self.sxz[I, J] = self.sxz[I, J] + mhz * (dvxdz + dvzdx) * dt
         self.data[it] = self.vz[self.rsx, self.rsz]
+
+
+class Twin2DSV(Twin2D):
+    """Elastic2D_CPML.update_SSG_SV (src/Elastic2D_CPML.py:203-274): vx at
+    (i+1/2, j) with rho averaged over i, i+1 (as (a+b)/2); vz at (i, j+1/2)
+    with 0.5*(rho[i,j] + rho[i,j+1]); the point force vx[src] += dt*w/rho[src]
+    (:245); normal stresses at integer points with the cell's own lam, mu;
+    sxz at (i+1/2, j+1/2) with mu averaged over the four corners; the receiver
+    records vx (:274)."""
+
+    def step(self, it, w):
+        T, N, dt = self.T, self.N, self.dt
+        nx, nz = self.vx.shape
+        X, Z = self.X, self.Z
+        r, lam, mu = self.rho, self.lam, self.mu
+        # vx (:216-228)
+        I, J = slice(N, nx - N - 1), slice(N + 1, nz - N)
+        dsxxdx = self._d(self.sxx, I, J, 0, True) / self.dx
+        dsxzdz = self._d(self.sxz, I, J, 1, False) / self.dz
+        rhx = (r[I, J] + r[N + 1:nx - N, J]) / T(2)
+        mk = self._mask(I, J, True, False)
+        dsxxdx = self._pml("sxx_dx", dsxxdx, X["b_half"], X["a_half"], X["k_half"], mk, I, J, True)
+        dsxzdz = self._pml("sxz_dz", dsxzdz, Z["b"], Z["a"], Z["k"], mk, I, J, False)
+        self.vx[I, J] = self.vx[I, J] + (dsxxdx + dsxzdz) * dt / rhx
+        # vz (:229-241)
+        I, J = slice(N + 1, nx - N), slice(N, nz - N - 1)
+        rhz = T(0.5) * (r[I, J] + r[I, N + 1:nz - N])
+        dsxzdx = self._d(self.sxz, I, J, 0, False) / self.dx
+        dszzdz = self._d(self.szz, I, J, 1, True) / self.dz
+        mk = self._mask(I, J, False, True)
+        dsxzdx = self._pml("sxz_dx", dsxzdx, X["b"], X["a"], X["k"], mk, I, J, True)
+        dszzdz = self._pml("szz_dz", dszzdz, Z["b_half"], Z["a_half"], Z["k_half"], mk, I, J, False)
+        self.vz[I, J] = self.vz[I, J] + (dszzdz + dsxzdx) * dt / rhz
+        # point force (:245)
+        self.vx[self.isx, self.isz] += dt * T(w) / r[self.isx, self.isz]
+        # sxx szz (:247-259)
+        I, J = slice(N + 1, nx - N), slice(N + 1, nz - N)
+        lm = lam[I, J]
+        l2m = lam[I, J] + T(2) * mu[I, J]
+        dvxdx = self._d(self.vx, I, J, 0, False) / self.dx
+        dvzdz = self._d(self.vz, I, J, 1, False) / self.dz
+        mk = self._mask(I, J, False, False)
+        dvxdx = self._pml("dvx_dx", dvxdx, X["b"], X["a"], X["k"], mk, I, J, True)
+        dvzdz = self._pml("dvz_dz", dvzdz, Z["b"], Z["a"], Z["k"], mk, I, J, False)
+        self.sxx[I, J] = self.sxx[I, J] + (l2m * dvxdx + lm * dvzdz) * dt
+        self.szz[I, J] = self.szz[I, J] + (l2m * dvzdz + lm * dvxdx) * dt
+        # sxz (:261-273)
+        I, J = slice(N + 1, nx - N), slice(N + 1, nz - N)
+        m4 = T(0.25) * (mu[I, N + 2:nz - N + 1] + mu[I, J] + mu[N + 2:nx - N + 1, N + 2:nz - N + 1]
+                        + mu[N + 2:nx - N + 1, J])
+        dvzdx = self._d(self.vz, I, J, 0, True) / self.dx
+        dvxdz = self._d(self.vx, I, J, 1, True) / self.dz
+        mk = self._mask(I, J, True, True)
+        dvzdx = self._pml("dvz_dx", dvzdx, X["b_half"], X["a_half"], X["k_half"], mk, I, J, True)
+        dvxdz = self._pml("dvx_dz", dvxdz, Z["b_half"], Z["a_half"], Z["k_half"], mk, I, J, False)
+        self.sxz[I, J] = self.sxz[I, J] + m4 * (dvxdz + dvzdx) * dt
+        self.data[it] = self.vx[self.rsx, self.rsz]
 
 
 class Twin2DRSG(Twin2D):
@@ -257,13 +316,23 @@ class Twin3DTensor:
         return np.where(mask, d / k + new, d)
 
     def step(self, it, w):
-        T, N, dt = self.T, self.N, self.dt
-        nx, ny, nz = self.vx.shape
-        dx, dy, dz = self.h
+        T = self.T
         s = self.src
         src = T(np.float32(w))
         for f, q in (("sxx", 0), ("syy", 1), ("szz", 2), ("sxy", 3), ("sxz", 4), ("syz", 5)):
             getattr(self, f)[s] += src * (-T(self.mt[q]))
+        self._velocity(True)
+        self._stress()
+        rx, ry, rz = self.rec
+        self.data[it] = self.vx[rx, ry, rz].astype(np.float32)
+
+    def _velocity(self, tensor):
+        """Velocity phase; the tensor scheme sums vz's derivatives x, y, z
+        (Elastic3D_SSG_Tensor.py:243), the point-force scheme z, x, y
+        (Elastic3D_SSG_CPML.py:212)."""
+        T, N, dt = self.T, self.N, self.dt
+        nx, ny, nz = self.vx.shape
+        dx, dy, dz = self.h
         S = lambda a, b: slice(a, b)
         r, lam, mu = self.rho, self.lam, self.mu
         # vx
@@ -301,7 +370,15 @@ class Twin3DTensor:
         d1 = self._pml("sxz_dx", d1, 0, False, mk, B)
         d2 = self._pml("syz_dy", d2, 1, False, mk, B)
         d3 = self._pml("szz_dz", d3, 2, True, mk, B)
-        self.vz[B] = self.vz[B] + (d1 + d2 + d3) * dt / r4
+        vz_sum = (d1 + d2 + d3) if tensor else (d3 + d1 + d2)
+        self.vz[B] = self.vz[B] + vz_sum * dt / r4
+
+    def _stress(self):
+        T, N, dt = self.T, self.N, self.dt
+        nx, ny, nz = self.vx.shape
+        dx, dy, dz = self.h
+        S = lambda a, b: slice(a, b)
+        r, lam, mu = self.rho, self.lam, self.mu
         # normal stresses
         B = (S(N + 1, nx - N), S(N + 1, ny - N), S(N + 1, nz - N))
         Bi = (S(N + 2, nx - N + 1), B[1], B[2])
@@ -351,8 +428,29 @@ class Twin3DTensor:
         e1 = self._pml("dvz_dy", e1, 1, True, mk, B)
         e2 = self._pml("dvy_dz", e2, 2, True, mk, B)
         self.syz[B] = self.syz[B] + m4 * (e1 + e2) * dt
+
+
+class Twin3DCPML(Twin3DTensor):
+    """Elastic3D_SSG_CPML.update_SSG (src/Elastic3D_SSG_CPML.py:144-309): the
+    tensor scheme's stencils and material quirks without the moment-tensor
+    injection, vz's derivatives summed z, x, y (:212), the point force
+    vz[isx+5, isy+5, isz+5] += dt*w / rho there after the velocity phase
+    (:245; the Dirichlet loops of :215-243 only zero cells no update touches);
+    one receiver records vx (:309)."""
+
+    def __init__(self, o):
+        """Build from an oracle.Oracle3D of scheme CPML."""
+        super().__init__(o)
+        self.src = tuple(q + 5 for q in self.src)
+
+    def step(self, it, w):
+        T, dt = self.T, self.dt
+        self._velocity(False)
+        s = self.src
+        self.vz[s] = self.vz[s] + (dt * T(np.float32(w))) / self.rho[s]
+        self._stress()
         rx, ry, rz = self.rec
-        self.data[it] = self.vx[rx, ry, rz].astype(np.float32)
+        self.data[it] = self.vx[rx[0], ry[0], rz[0]].astype(np.float32)
 
 
 class Twin3DSPML(Twin3DTensor):

@@ -155,6 +155,26 @@ def test_twin_3d_tensor_bitwise(N):
 
 
 @pytest.mark.parametrize("N,dtype", [(2, np.float32), (3, np.float32), (2, np.float64)])
+def test_twin_2d_sv_bitwise(N, dtype):
+    """The SV step (Elastic2D_CPML.py:203-274): oracle and numpy
+    transcription bit for bit, wavefields, vx trace and memory variables."""
+    nt = 80
+    c = case2d(shape=(48, 40), N=N, npml=6, nt=nt, dtype=dtype)
+    wav = O.wavelet("ricker", nt, c["dt"], c["freq"], 1.0)
+    o = oracle2d(c, wavelet=wav)
+    t = np_twin.Twin2DSV(o)
+    o.run("SV", 0, nt)
+    for it in range(nt):
+        t.step(it, wav[it])
+    for f in ("vx", "vz", "sxx", "szz", "sxz"):
+        assert np.array_equal(getattr(t, f), getattr(o, f)), f
+    assert np.array_equal(t.data, o.data)
+    for k, v in t.mem.items():
+        assert np.array_equal(v, o.memory("memory_" + k)), k
+    assert np.abs(o.vx).max() > 0 and np.abs(o.data).max() > 0
+
+
+@pytest.mark.parametrize("N,dtype", [(2, np.float32), (3, np.float32), (2, np.float64)])
 def test_twin_2d_rsg_bitwise(N, dtype):
     """The rotated-grid step (Elastic2D_CPML.py:277-353) with a caller-given
     source value per step: oracle and numpy transcription bit for bit,
@@ -173,6 +193,26 @@ def test_twin_2d_rsg_bitwise(N, dtype):
     for k, v in t.mem.items():
         assert np.array_equal(v, o.memory("memory_" + k)), k
     assert np.abs(o.vz).max() > 0 and np.abs(o.memory("memory_dvx_dx")).max() > 0
+
+
+@pytest.mark.parametrize("N,dtype", [(2, np.float32), (4, np.float32), (2, np.float64)])
+def test_twin_3d_cpml_force_bitwise(N, dtype):
+    """The point-force CPML step (Elastic3D_SSG_CPML.py:144-309): oracle and
+    numpy transcription bit for bit, wavefields, vx trace and the 18 memory
+    variables."""
+    c = case3d(scheme="CPML", shape=(28, 26, 30), N=N, npml=5, nt=40, dtype=dtype)
+    wav = O.wavelet("ricker", 40, c["dt"], c["freq"], 1000.0)
+    o = oracle3d(c, wavelet=wav)
+    t = np_twin.Twin3DCPML(o)
+    o.run(0, 40)
+    for it in range(40):
+        t.step(it, wav[it])
+    for f in ("vx", "vy", "vz", "sxx", "syy", "szz", "sxy", "sxz", "syz"):
+        assert np.array_equal(getattr(t, f), getattr(o, f)), f
+    assert np.array_equal(t.data, o.data)
+    for k, v in t.mem.items():
+        assert np.array_equal(v, o.memory("memory_" + k)), k
+    assert len(t.mem) == 18 and np.abs(o.vz).max() > 0
 
 
 @pytest.mark.parametrize("N,dtype", [(2, np.float32), (3, np.float32), (2, np.float64)])
