@@ -7,7 +7,9 @@ scripts), and Taichi cannot run here, so the oracle is pinned by:
     with the C++ oracle bit for bit,
   * the committed golden fixtures of tests/golden/ (made by
     tests/golden/make_golden.py from the oracle and checked by the twin),
-  * physics: P-wave arrival time, mirror symmetry, CPML absorption.
+  * physics: P- and S-wave arrival times, source-receiver reciprocity,
+    mirror symmetry, CPML absorption and reflection against a large domain,
+    and a higher-order stencil converging towards a refined reference.
 """
 from fractions import Fraction
 
@@ -247,6 +249,83 @@ def test_oracle_p_arrival_time():
     t_peak = np.argmax(tr) * c["dt"]
     # Ricker2 peaks at t0 = 1.5/f = 0.06 s, then travels 1000 m at 3000 m/s
     assert abs(t_peak - (0.06 + 1000.0 / 3000.0)) < 0.02
+
+
+def test_oracle_s_arrival_time():
+    """A vertical point force radiates S waves, not P, along the horizontal:
+    the vz peak 1000 m away along x comes at about t0 + r / vs (0.637 s;
+    numerical dispersion of the S wave, ~3 cells per wavelength at the top of
+    the band, delays it by ~20 ms), far from the P time t0 + r / vp (0.393 s)."""
+    c = case2d(shape=(240, 140), N=2, hetero=False, npml=20, nt=760, freq=25.0)
+    c["isx"], c["isz"] = 60, 70
+    c["rsx"], c["rsz"] = 160, 70
+    o = oracle2d(c).run("VS", 0, 760)
+    t_peak = np.argmax(np.abs(o.data)) * c["dt"]
+    assert abs(t_peak - (0.06 + 1000.0 / 1732.0)) < 0.03, t_peak
+
+
+def test_oracle_source_receiver_reciprocity():
+    """Constant density, varying vp and vs: the vz trace at B from a vertical
+    force at A equals the vz trace at A from the force at B (the staggered
+    operators are transposes of each other; the window ends before the waves
+    reach the CPML).  Measured: 1.9e-7 relative."""
+    c = case2d(shape=(160, 160), N=2, hetero=True, npml=20, nt=130, freq=25.0)
+    c["rho"] = np.full(c["shape"], 2000.0, np.float32)
+
+    def trace(src, rec):
+        cc = dict(c)
+        cc["isx"], cc["isz"] = src
+        cc["rsx"], cc["rsz"] = rec
+        return oracle2d(cc).run("VS", 0, 130).data.astype(np.float64)
+
+    ab, ba = trace((70, 80), (86, 74)), trace((86, 74), (70, 80))
+    assert np.abs(ab).max() > 0
+    assert np.linalg.norm(ab - ba) / np.linalg.norm(ab) < 1e-5
+
+
+def test_oracle_cpml_reflection_against_large_domain():
+    """A receiver 8 cells inside the 20-cell CPML's inner edge, 0.5 s: its
+    trace differs from the same point in a domain so large that no boundary
+    echo returns by 3.7e-5 relative L2 (measured); a 5-cell CPML on the same
+    grid reflects about 60 times more."""
+    nt = 500
+
+    def trace(n, npml, src, rec):
+        c = case2d(shape=(n, n), N=2, hetero=False, npml=npml, nt=nt, freq=25.0)
+        c["isx"], c["isz"] = src
+        c["rsx"], c["rsz"] = rec
+        return oracle2d(c).run("VS", 0, nt).data.astype(np.float64)
+
+    big = trace(320, 20, (160, 160), (160, 190))
+    rel = lambda a: np.linalg.norm(a - big) / np.linalg.norm(big)
+    e20 = rel(trace(120, 20, (60, 60), (60, 90)))
+    e5 = rel(trace(120, 5, (60, 60), (60, 90)))
+    assert e20 < 2e-4 and e5 > 10 * e20, (e20, e5)
+
+
+def test_oracle_higher_order_converges():
+    """Grid refinement and stencil order: on a 10 m grid the 4th-order-pair
+    (N=4) stencil reproduces a 5 m, N=4 reference trace (500 m offset, 0.45 s)
+    better than N=2 (measured 2.3% against 6.5% relative L2 after a
+    least-squares amplitude fit), and the fitted amplitude is the cell-area
+    ratio 1/4 of a point force."""
+
+    def trace(n, N, h, dt, nt, npml, src, rec):
+        c = case2d(shape=(n, n), N=N, hetero=False, npml=npml, nt=nt, freq=25.0, dx=h, dz=h, dt=dt)
+        c["isx"], c["isz"] = src
+        c["rsx"], c["rsz"] = rec
+        return oracle2d(c).run("VS", 0, nt).data.astype(np.float64)
+
+    ref = trace(400, 4, 5.0, 5e-4, 900, 40, (200, 200), (200, 300))[1::2]
+
+    def err(N):
+        a = trace(200, N, 10.0, 1e-3, 450, 20, (100, 100), (100, 150))
+        al = np.dot(a, ref) / np.dot(a, a)
+        return np.linalg.norm(al * a - ref) / np.linalg.norm(ref), al
+
+    (e2, a2), (e4, a4) = err(2), err(4)
+    assert e4 < 0.5 * e2 and e4 < 0.04, (e2, e4)
+    assert abs(a4 - 0.25) < 0.01 and abs(a2 - 0.25) < 0.01, (a2, a4)
 
 
 def test_oracle_mirror_symmetry():
