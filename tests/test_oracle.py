@@ -8,7 +8,7 @@ scripts), and Taichi cannot run here, so the oracle is pinned by:
   * the committed golden fixtures of tests/golden/ (made by
     tests/golden/make_golden.py from the oracle and checked by the twin),
   * physics: P- and S-wave arrival times, source-receiver reciprocity,
-    mirror symmetry, CPML absorption and reflection against a large domain,
+    mirror symmetry (2D force, 3D explosion), CPML absorption and reflection against a large domain,
     and a higher-order stencil converging towards a refined reference.
 """
 from fractions import Fraction
@@ -342,6 +342,26 @@ def test_oracle_mirror_symmetry():
     assert np.abs(vz).max() > 0
     # equal up to the rounding of the unsymmetric summation order
     assert np.max(np.abs(lhs - rhs)) <= 1e-4 * np.max(np.abs(vz))
+
+
+def test_oracle_3d_explosion_mirror_symmetry():
+    """3D tensor scheme, explosive source (M = I) at the centre of an odd
+    homogeneous box: the grid and its PML profiles are symmetric about the
+    source, so the normal stresses (integer points) are even and vx (at
+    i + 1/2, mirror i -> 59 - i) is odd under x -> -x, and the stresses even
+    in y and z, up to the rounding of the unsymmetric summation orders
+    (measured below 1e-6 of the maxima)."""
+    c = case3d(shape=(61, 57, 63), N=2, scheme="TENSOR", hetero=False, npml=8, nt=80)
+    c["isx"], c["isy"], c["isz"] = 30, 28, 31
+    c["MT"] = np.eye(3, dtype=np.float32)
+    o = oracle3d(c).run(0, 80)
+    sxx, szz, vx = (getattr(o, f).astype(np.float64) for f in ("sxx", "szz", "vx"))
+    rel = lambda d, f: np.abs(d).max() / np.abs(f).max()
+    assert np.abs(sxx).max() > 0 and np.abs(vx).max() > 0
+    assert rel(sxx - sxx[::-1], sxx) < 1e-5
+    assert rel(szz - szz[::-1], szz) < 1e-5
+    assert rel(vx[:60] + vx[59::-1], vx) < 1e-5
+    assert rel(sxx - sxx[:, ::-1], sxx) < 1e-5 and rel(sxx - sxx[:, :, ::-1], sxx) < 1e-5
 
 
 def test_oracle_cpml_absorbs():
