@@ -27,6 +27,8 @@ def cases():
         ("sv2d", case2d(shape=(44, 50), N=3, nt=50, npml=8), "SV", 50),
         ("tensor3d", case3d(shape=(24, 22, 26), N=2, nt=40, npml=6), "TENSOR", 40),
         ("cpml3d", case3d(shape=(26, 24, 22), N=2, nt=40, npml=6, scheme="CPML"), "CPML", 40),
+        ("spml3d", case3d(shape=(24, 26, 22), N=2, nt=40, npml=6, scheme="SPML"), "SPML", 40),
+        ("rsg2d", case2d(shape=(46, 42), N=2, nt=60, npml=8), "RSG", 60),
     ]
 
 
@@ -42,7 +44,17 @@ def wavelet_of(c, scheme):
     return BaseFun.series("ricker", c["nt"], c["dt"], c["freq"], c["src_scale"])
 
 
+def rsg_sources(c):
+    """update_RSG's caller-given source value of each step (a Ricker series)."""
+    from seiswave_taichi_b200 import BaseFun
+    return BaseFun.series("ricker", c["nt"], c["dt"], c["freq"], 1.0)
+
+
 def run(name, c, scheme, steps):
+    if scheme == "RSG":
+        # update_RSG records no receiver (Elastic2D_CPML.py:277-353): keep vx and vz
+        o = oracle2d(c).run("RSG", 0, steps, rsg_sources=rsg_sources(c).astype(np.float64))
+        return {f"{name}_vx": np.asarray(o.vx), f"{name}_vz": np.asarray(o.vz)}
     if scheme in ("VS", "SV"):
         o = oracle2d(c, wavelet=wavelet_of(c, scheme)).run(scheme, 0, steps)
     else:
