@@ -30,12 +30,14 @@ def torch_dtype(fieldtype) -> torch.dtype:
         raise TypeError(f"fieldtype {fieldtype} is not float32/float64")
     try:
         npd = np.dtype(fieldtype)
+    except TypeError:
+        npd = None  # not a numpy type (e.g. ti.f32): go by its name below
+    if npd is not None:
         if npd == np.float32:
             return torch.float32
         if npd == np.float64:
             return torch.float64
-    except TypeError:
-        pass
+        raise TypeError(f"fieldtype {fieldtype!r} is not float32/float64")
     s = str(fieldtype).lower()
     if "64" in s:
         return torch.float64
