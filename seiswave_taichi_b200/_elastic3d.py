@@ -367,9 +367,8 @@ class Elastic3DBase:
         cached per (GPU, solver class, order, dtype, numeric mode, path, log2
         shape bucket) in the batch autotuner's JSON file
         (SEISWAVE_AUTOTUNE_CACHE).  Returns the chosen chunk length."""
-        import json
         import math
-        from .batch import _cache_path
+        from .batch import cache_load, cache_store
         plan = self._plan or self._build_plan()
         info = plan.info()
         path_name = info["path"]
@@ -385,17 +384,14 @@ class Elastic3DBase:
             else:
                 plan.set_tile(int(chunk))
 
-        cache_file = _cache_path()
-        cache = {}
-        if cache_file.exists():
-            try:
-                cache = json.loads(cache_file.read_text())
-            except (OSError, ValueError):
-                cache = {}
-        if key in cache and not force:
-            apply(int(cache[key]))
-            return int(cache[key])
+        v = cache_load().get(key)
+        if not force and isinstance(v, int) and v in self.AUTOTUNE_CHUNKS and v <= nx:
+            apply(v)
+            return v
+        # every array a trial step writes is saved and restored
         state = [getattr(self, f) for f in FIELDS3] + [m for m in self._mem if m is not None] + [self.data]
+        if self._split is not None:
+            state.append(self._split)
         saved = [t.clone() for t in state]
         gen = torch.Generator(device=state[0].device).manual_seed(0)
         for t in state:
@@ -418,12 +414,7 @@ class Elastic3DBase:
         for t, v in zip(state, saved):
             t.copy_(v)
         apply(best)
-        cache[key] = best
-        try:
-            cache_file.parent.mkdir(parents=True, exist_ok=True)
-            cache_file.write_text(json.dumps(cache, indent=1, sort_keys=True))
-        except OSError:
-            pass
+        cache_store(key, best)
         return best
 
     def check_finite(self) -> int:

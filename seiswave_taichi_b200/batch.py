@@ -41,6 +41,33 @@ def _cache_path() -> Path:
     return Path(p) if p else Path.home() / ".cache" / "seiswave_taichi_b200" / "autotune.json"
 
 
+def cache_load() -> dict:
+    """The autotuners' cache {key: choice}; a missing, unreadable or
+    malformed file reads as empty."""
+    try:
+        d = json.loads(_cache_path().read_text())
+    except (OSError, ValueError):
+        return {}
+    return d if isinstance(d, dict) else {}
+
+
+def cache_store(key: str, value) -> None:
+    """Add key -> value to the cache file, merged with its current entries
+    and written through a temporary file and a rename, so tuners in several
+    processes never leave a torn file; a cache that cannot be written is
+    skipped."""
+    p = _cache_path()
+    try:
+        p.parent.mkdir(parents=True, exist_ok=True)
+        d = cache_load()
+        d[key] = value
+        tmp = p.with_name(f"{p.name}.{os.getpid()}.tmp")
+        tmp.write_text(json.dumps(d, indent=1, sort_keys=True))
+        os.replace(tmp, p)
+    except OSError:
+        pass
+
+
 class ShotBatch2D:
     def __init__(self, waves, scheme: str = "VS", autotune: bool = True):
         if not waves:
@@ -108,17 +135,11 @@ class ShotBatch2D:
         return out
 
     def autotune(self, steps: int = 6, force: bool = False) -> int:
-        path = _cache_path()
         key = self._key()
-        cache = {}
-        if path.exists():
-            try:
-                cache = json.loads(path.read_text())
-            except (OSError, ValueError):
-                cache = {}
-        if key in cache and not force:
-            self.set_tile(int(cache[key]))
-            return int(cache[key])
+        v = cache_load().get(key)
+        if not force and isinstance(v, int) and 0 <= v < len(TILES):
+            self.set_tile(v)
+            return v
         state = self._state()
         saved = [t.clone() for t in state]
         gen = torch.Generator(device=state[0].device).manual_seed(0)
@@ -142,12 +163,7 @@ class ShotBatch2D:
         for t, s in zip(state, saved):
             t.copy_(s)
         self.set_tile(best)
-        cache[key] = best
-        try:
-            path.parent.mkdir(parents=True, exist_ok=True)
-            path.write_text(json.dumps(cache, indent=1, sort_keys=True))
-        except OSError:
-            pass
+        cache_store(key, best)
         return best
 
 
