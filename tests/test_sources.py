@@ -30,3 +30,16 @@ def test_explosive_and_random_tensors():
     a, b = S.random_tensor(7), S.random_tensor(7)
     assert np.array_equal(a, b) and np.array_equal(a, a.T) and a.dtype == np.float32
     assert not np.array_equal(a, S.random_tensor(8))
+
+
+def test_moment_2d_forms():
+    """2D moment tensors as (xx, zz, xz): 'explosive', a 2x2 [[xx, xz], [xz, zz]]
+    array, or a 3x3 tensor's x-z block (x first axis, z last)."""
+    from seiswave_taichi_b200.Elastic2D_CPML import moment_2d
+    assert moment_2d("explosive").tolist() == [1.0, 1.0, 0.0]
+    assert moment_2d([[0.5, -2.0], [-2.0, 3.0]]).tolist() == [0.5, 3.0, -2.0]
+    M = S.double_couple(30, 60, 90)
+    assert np.array_equal(moment_2d(M), np.array([M[0, 0], M[2, 2], M[0, 2]], np.float32))
+    for bad in ("implosive", np.zeros(3), np.zeros((2, 3))):
+        with pytest.raises(ValueError):
+            moment_2d(bad)
