@@ -25,8 +25,7 @@ import torch
 
 from . import _native as N
 from . import pml as P
-from ._common import (as_device, as_numpy, compute_lam, compute_mu, device, receiver_table,
-                      sw_dtype, torch_dtype)
+from ._common import as_device, as_numpy, compute_lam, compute_mu, device, sw_dtype, torch_dtype
 
 FIELDS3 = ("vx", "vy", "vz", "sxx", "syy", "szz", "sxy", "sxz", "syz")
 

@@ -5,7 +5,6 @@ exactly (float64 here, so the comparison is free of accumulated float32
 rounding differences in the host-side chain)."""
 import numpy as np
 import pytest
-import torch
 
 from cases import case2d, product2d
 
