@@ -96,19 +96,23 @@ struct O3Desc {
 namespace {
 
 // Wavelets of src/BaseFun.py, in float as the reference's @ti.func returns ti.f32.
+// `pi**2` there is an expression of Python values only, which Taichi's
+// frontend folds in double before it meets the float arithmetic, so the
+// constant is (float)(pi*pi in double), not pi_f * pi_f.
+constexpr double kPiD = 3.14159265358979323846;
 // BaseFun.py:4-11
 float ricker(int it, float dt, float freq, float scale) {
-  const float pi = 3.14159265358979323846f;
+  const float pi2 = (float)(kPiD * kPiD);
   float t0 = 1.5f / freq;
-  float a = (pi * pi) * (freq * freq);
+  float a = pi2 * (freq * freq);
   float t = (float)it * dt;
   float tau = t - t0;
   return ((((-scale) * 2.0f) * a) * tau) * std::exp((-a) * (tau * tau));
 }
 // BaseFun.py:13-19
 float ricker2(int it, float dt, float t0, float freq, float scale) {
-  const float pi = 3.14159265358979323846f;
-  float a = (pi * pi) * (freq * freq);
+  const float pi2 = (float)(kPiD * kPiD);
+  float a = pi2 * (freq * freq);
   float t = (float)it * dt;
   float tau = t - t0;
   return (scale * (1.0f - (2.0f * a) * (tau * tau))) * std::exp((-a) * (tau * tau));

@@ -9,6 +9,12 @@ per time step, in the same operation order.
 * Ricker2  (BaseFun.py:13-19) src_scale*(1-2a tau^2)*exp(-a tau^2), t0 given
 * Ricker3  (BaseFun.py:21-27) Ricker wavelet shifted by 1.5/freq + t0
 with a = pi^2 freq^2 and tau = nt*dt - t0.
+
+Constant folding follows Taichi's frontend: `pi**2` is an expression of
+Python values only, so Taichi evaluates it in Python (float64) and the result
+enters the float32 arithmetic rounded once (f32(pi^2) = 9.869604, where
+f32(pi)*f32(pi) would give 9.869605).  Integer powers of float32 values
+(`freq**2`, `tau**2`) are single float32 products, as Taichi lowers them.
 """
 from __future__ import annotations
 
@@ -16,6 +22,7 @@ import numpy as np
 
 _f = np.float32
 _PI = _f(np.pi)
+_PI2 = _f(np.pi ** 2)  # pi**2 folded in float64, then rounded once (BaseFun.py:6,15)
 
 
 def _steps(nt) -> np.ndarray:
@@ -26,7 +33,7 @@ def Ricker(nt, dt, freq, src_scale):
     """BaseFun.py:4-11 for step index nt (scalar or array)."""
     freq, dt, s = _f(freq), _f(dt), _f(src_scale)
     t0 = _f(1.5) / freq
-    a = (_PI * _PI) * (freq * freq)
+    a = _PI2 * (freq * freq)
     t = _steps(nt) * dt
     tau = t - t0
     with np.errstate(under="ignore"):
@@ -36,7 +43,7 @@ def Ricker(nt, dt, freq, src_scale):
 def Ricker2(nt, dt, t0, freq, src_scale):
     """BaseFun.py:13-19 for step index nt (scalar or array)."""
     freq, dt, t0, s = _f(freq), _f(dt), _f(t0), _f(src_scale)
-    a = (_PI * _PI) * (freq * freq)
+    a = _PI2 * (freq * freq)
     t = _steps(nt) * dt
     tau = t - t0
     with np.errstate(under="ignore"):

@@ -286,8 +286,10 @@ class ElasticWAVE:
         return plan
 
     def _vs_wavelet(self):
-        """update_SSG_VS's source series: Ricker2 with t0 = 1.5/f0 (:142, :170)."""
-        t0 = np.float32(1.5) / np.float32(self.f0)
+        """update_SSG_VS's source series: Ricker2 with t0 = 1.5/f0 (:142, :170).
+        `1.5/self.f0` is folded in Python (double) by Taichi's frontend and
+        rounded once to float32 when assigned to t0."""
+        t0 = np.float32(1.5 / float(self.f0))
         return BaseFun.series("ricker2", self.nt, self.dt, self.f0, self.src_scale, t0=t0)
 
     def _stream(self) -> int:

@@ -36,7 +36,7 @@ def wavelet_of(c, scheme):
     from seiswave_taichi_b200 import BaseFun
     if scheme == "VS":
         return BaseFun.series("ricker2", c["nt"], c["dt"], c["freq"], c.get("src_scale", 1.0),
-                              t0=np.float32(1.5) / np.float32(c["freq"]))
+                              t0=np.float32(1.5 / float(c["freq"])))
     if scheme == "SV":
         return BaseFun.series("ricker", c["nt"], c["dt"], c["freq"], 1.0)
     if scheme == "TENSOR":

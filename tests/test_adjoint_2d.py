@@ -39,7 +39,7 @@ def _sid(scheme):
 def _wavelet(c):
     from seiswave_taichi_b200 import BaseFun
     return BaseFun.series("ricker2", c["nt"], c["dt"], c["freq"], c["src_scale"],
-                          t0=np.float32(1.5) / np.float32(c["freq"]))
+                          t0=np.float32(1.5 / float(c["freq"])))
 
 
 @pytest.mark.parametrize("scheme", SCHEMES)
