@@ -183,7 +183,7 @@ def cpu_baseline(cfg, min_seconds=10.0, max_steps=60):
         from seiswave_taichi_b200 import BaseFun
         from seiswave_taichi_b200.Elastic2D_CPML import moment_2d
         wav = BaseFun.series("ricker2", cfg["nt"], cfg["dt"], cfg["freq"], cfg.get("src_scale", 1.0),
-                             t0=np.float32(1.5) / np.float32(cfg["freq"]))
+                             t0=np.float32(1.5 / float(cfg["freq"])))
         table = cfg["rsx"].reshape(-1) * cfg["shape"][1] + cfg["rsz"].reshape(-1)
         o = O.Oracle2D(cfg["vs"], cfg["vp"], cfg["rho"], cfg["dx"], cfg["dz"], cfg["dt"], cfg["isx"], cfg["isz"],
                        int(cfg["rsx"].reshape(-1)[0]), int(cfg["rsz"].reshape(-1)[0]), cfg["nt"],
@@ -556,6 +556,8 @@ def main(argv=None):
     ap.add_argument("--config", default="config2", choices=["config2", "config1", "config3", "config4", "config5", "segy"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the float64 error runs")
+    ap.add_argument("--path", default=None, choices=["staged", "fused", "two_pass"],
+                    help="3D execution path of the timed solver (default: the plan's own)")
     args = ap.parse_args(argv)
     args.warmup = max(args.warmup, 3)
 
@@ -584,6 +586,8 @@ def main(argv=None):
     three_d = len(cfg["shape"]) == 3
     w = build_solver(cfg, torch) if three_d else build_solver2d(cfg, torch)
     if three_d:
+        if args.path:
+            (w._plan or w._build_plan()).set_path(args.path)
         w.autotune()  # x planes per work unit, outside the timed region
     nt = cfg["nt"]
     ncell = int(np.prod(cfg["shape"]))

@@ -173,8 +173,9 @@ SW_API int sw3d_plan_create(const sw3d_desc* desc, sw_plan** plan);
 SW_API int sw_plan_set_tile(sw_plan* plan, int32_t x_chunk);
 
 /* Block until the stream is idle and report a device-side failure recorded
- * by the plan's kernels since creation (SW_ERR_TIMEOUT: a bounded wait for
- * TMA data, or a grid barrier of the 2D persistent run, gave up).  No reference counterpart (the reference has no error
+ * by the plan's kernels since the previous status read (SW_ERR_TIMEOUT: a
+ * bounded wait for TMA data, or a grid barrier of the 2D persistent run, gave
+ * up); a failure is reported once and then cleared, so a caller may retry.  No reference counterpart (the reference has no error
  * path); it is the status read the drivers' loops can add after run(). */
 SW_API int sw_plan_status(sw_plan* plan, void* stream);
 
@@ -406,7 +407,10 @@ SW_API int sw_check_finite(sw_plan* plan, void* stream, int64_t* nonfinite);
  * any is non-zero.  Blocks on the stream.  Each call zeroes the counters it
  * uses before its scan, so nothing must be zero on entry.  The first call on
  * each device (that device current) resolves the counters' address with
- * cudaGetSymbolAddress; make it before any stream capture.  The counters are
+ * cudaGetSymbolAddress, and with lazy module loading (CUDA_MODULE_LOADING=LAZY,
+ * the default) that first use may load this library's device code, which the
+ * driver backs with device memory: make the first call on each device before
+ * any stream capture and before any region where allocation is forbidden.  The counters are
  * shared by every caller on a device: calls that overlap in time on one device
  * (several host threads) race and return mixed counts, so serialise them. */
 #define SW_NOALLOC_MAX_ARRAYS 64

@@ -49,12 +49,31 @@ def segy_layout(raw: np.ndarray) -> dict:
     return dict(dt_us=dt_us, ns=ns, fmt=fmt, first=first, rec=rec, ntraces=body // rec if ns > 0 else 0)
 
 
+def check_body(body, ntraces: int, ns: int, fmt: int) -> None:
+    """Refuse a decode that would read past the end of `body`: the format must
+    be known, ntraces and ns non-negative, and body a contiguous uint8 CUDA
+    tensor of at least ntraces * (240 + bytes per sample * ns) bytes (the
+    library takes no byte length, so this is its bounds check)."""
+    if not isinstance(body, torch.Tensor) or body.dtype != torch.uint8:
+        raise ValueError("decode_traces takes a uint8 tensor")
+    if int(fmt) not in BYTES:
+        raise ValueError(f"sample format {fmt} not supported (1 IBM float, 2 int32, 3 int16, 5 IEEE float, 8 int8)")
+    if int(ntraces) < 0 or int(ns) < 0:
+        raise ValueError("ntraces and ns must be non-negative")
+    need = int(ntraces) * (240 + BYTES[int(fmt)] * int(ns))
+    if body.numel() < need:
+        raise ValueError(f"body holds {body.numel()} bytes, {ntraces} traces of {ns} samples need {need}")
+    if not body.is_contiguous():
+        raise ValueError("body must be contiguous")
+    if body.device.type != "cuda":
+        raise ValueError("decode_traces takes a CUDA tensor")
+
+
 def decode_traces(body: torch.Tensor, ntraces: int, ns: int, fmt: int):
     """Decode trace records already in device memory (uint8, the bytes from the
     first trace header on): (ntraces, ns) float32 samples, (ntraces,) int32
     SourceX."""
-    if body.device.type != "cuda" or body.dtype != torch.uint8:
-        raise ValueError("decode_traces takes a uint8 CUDA tensor")
+    check_body(body, ntraces, ns, fmt)
     out = torch.empty((ntraces, ns), dtype=torch.float32, device=body.device)
     srcx = torch.empty(ntraces, dtype=torch.int32, device=body.device)
     st = torch.cuda.current_stream(body.device).cuda_stream

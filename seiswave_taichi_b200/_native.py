@@ -199,17 +199,41 @@ def struct_sizes() -> dict:
 NOALLOC_MAX_ARRAYS = 64
 
 
-def count_nonfinite_noalloc(tensors, stream: int = 0) -> list[int]:
-    """Per-tensor NaN/Inf counts through sw_count_nonfinite_noalloc, which
-    allocates no device memory (at most NOALLOC_MAX_ARRAYS contiguous tensors
-    of one dtype, float32 or float64)."""
+def validate_noalloc_inputs(tensors) -> None:
+    """Refuse, before any pointer reaches the library, every tensor that the
+    scan could not read within bounds on the current device: not a torch
+    tensor, not float32/float64 (the kernel reads 4 or 8 bytes per element),
+    mixed dtypes, not contiguous, not on the current CUDA device."""
     import torch
-    n = len(tensors)
-    if n and any(t.dtype != tensors[0].dtype for t in tensors):
+    if not tensors:
+        return
+    cur = torch.cuda.current_device() if torch.cuda.is_available() else None
+    for t in tensors:
+        if not isinstance(t, torch.Tensor):
+            raise TypeError("count_nonfinite_noalloc takes torch tensors")
+        if t.dtype not in (torch.float32, torch.float64):
+            raise ValueError(f"tensors must be float32 or float64, not {t.dtype}")
+    if any(t.dtype != tensors[0].dtype for t in tensors):
         raise ValueError("tensors must share one dtype")
     if any(not t.is_contiguous() for t in tensors):
         raise ValueError("tensors must be contiguous")
+    for t in tensors:
+        if not t.is_cuda or t.device.index != cur:
+            raise ValueError(f"tensors must be on the current CUDA device (cuda:{cur}), not {t.device}")
+
+
+def count_nonfinite_noalloc(tensors, stream: int | None = None) -> list[int]:
+    """Per-tensor NaN/Inf counts through sw_count_nonfinite_noalloc, which
+    allocates no device memory (at most NOALLOC_MAX_ARRAYS contiguous tensors
+    of one dtype, float32 or float64, on the current CUDA device; stream
+    defaults to torch's current stream)."""
+    import torch
+    tensors = list(tensors)
+    n = len(tensors)
+    validate_noalloc_inputs(tensors)
     dt = SW_F64 if n and tensors[0].dtype == torch.float64 else SW_F32
+    if stream is None:
+        stream = torch.cuda.current_stream().cuda_stream if n else 0
     arr = (C.c_void_p * max(n, 1))(*[ptr(t) for t in tensors])
     lens = (C.c_int64 * max(n, 1))(*[t.numel() for t in tensors])
     out = (C.c_int64 * max(n, 1))()

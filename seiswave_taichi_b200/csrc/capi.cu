@@ -767,6 +767,12 @@ int sw_plan_status(sw_plan* pl, void* stream) {
     int h = 0;
     e = cudaMemcpy(&h, pl->d_err, sizeof h, cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return cuda_fail(e, "sw_plan_status");
+    if (h != 0) {
+      // reported once: clear the word so that a retry after a transient
+      // timeout reads the status of the runs since this read
+      e = cudaMemset(pl->d_err, 0, sizeof(int));
+      if (e != cudaSuccess) return cuda_fail(e, "sw_plan_status");
+    }
     if (h & 1) return fail(SW_ERR_TIMEOUT, "a bounded device wait gave up (TMA data never arrived)");
     if (h & 2) return fail(SW_ERR_TIMEOUT, "a bounded device wait gave up (grid barrier of the persistent run)");
   }

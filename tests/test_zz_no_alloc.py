@@ -45,6 +45,28 @@ def test_noalloc_matches_check_finite(cuda):
     assert math.isnan(float(fields[0].view(-1)[5]))
 
 
+def test_noalloc_allocates_nothing(cuda):
+    """After a first call on the device (which resolves the counters' address
+    and may load the module), a loop of calls changes neither the device's
+    free memory nor torch's allocator state."""
+    import torch
+    from seiswave_taichi_b200 import _native as N
+    fields = [torch.zeros(100_000, device="cuda") for _ in range(9)]
+    fields[3][7] = float("nan")
+    assert N.count_nonfinite_noalloc(fields) == [0, 0, 0, 1, 0, 0, 0, 0, 0]
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    alloc0 = torch.cuda.memory_allocated()
+    reserved0 = torch.cuda.memory_reserved()
+    for _ in range(50):
+        assert N.count_nonfinite_noalloc(fields) == [0, 0, 0, 1, 0, 0, 0, 0, 0]
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    assert torch.cuda.memory_allocated() == alloc0
+    assert torch.cuda.memory_reserved() == reserved0
+
+
 def test_noalloc_float64_and_limits(cuda):
     import torch
     from seiswave_taichi_b200 import _native as N
