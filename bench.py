@@ -167,40 +167,77 @@ def algorithmic_bytes(cfg, npml=20):
     return 52 * ncell + 32 * S
 
 
-def cpu_baseline(cfg, min_seconds=10.0, max_steps=60):
-    """The oracle on all host cores, on a bounded sample (whole grid, the
-    first few time steps) of the same workload."""
+def oracle_for(cfg):
+    """The CPU oracle (C++/OpenMP restatement of the reference kernels) set up
+    for workload cfg, and a function advancing it by n time steps from it."""
     from oracle import oracle as O
-    threads = os.cpu_count() or 1
-    O.set_threads(threads)
     if len(cfg["shape"]) == 3:
         o = O.Oracle3D("TENSOR", cfg["vs"], cfg["vp"], cfg["rho"], cfg["dx"], cfg["dy"], cfg["dz"], cfg["dt"],
                        cfg["isx"], cfg["isy"], cfg["isz"], cfg["rsx"], cfg["rsy"], cfg["rsz"], cfg["nt"],
                        cfg["accuracy"], cfg["freq"], cfg["surface"], cfg["pml"], MT=cfg["MT"],
                        src_scale=cfg["src_scale"])
-        step = lambda it, n: o.run(it, n)
-    else:
-        from seiswave_taichi_b200 import BaseFun
-        from seiswave_taichi_b200.Elastic2D_CPML import moment_2d
-        wav = BaseFun.series("ricker2", cfg["nt"], cfg["dt"], cfg["freq"], cfg.get("src_scale", 1.0),
-                             t0=np.float32(1.5 / float(cfg["freq"])))
-        table = cfg["rsx"].reshape(-1) * cfg["shape"][1] + cfg["rsz"].reshape(-1)
-        o = O.Oracle2D(cfg["vs"], cfg["vp"], cfg["rho"], cfg["dx"], cfg["dz"], cfg["dt"], cfg["isx"], cfg["isz"],
-                       int(cfg["rsx"].reshape(-1)[0]), int(cfg["rsz"].reshape(-1)[0]), cfg["nt"],
-                       cfg["accuracy"], cfg["freq"], cfg["surface"], cfg["pml"], wavelet=wav,
-                       MT=moment_2d(cfg["MT"]) if cfg.get("MT") is not None else None, rec_index=table)
-        step = lambda it, n: o.run("VS", it, n)
-    step(0, 1)  # first touch of the state pages
+        return lambda it, n: o.run(it, n)
+    from seiswave_taichi_b200 import BaseFun
+    from seiswave_taichi_b200.Elastic2D_CPML import moment_2d
+    wav = BaseFun.series("ricker2", cfg["nt"], cfg["dt"], cfg["freq"], cfg.get("src_scale", 1.0),
+                         t0=np.float32(1.5 / float(cfg["freq"])))
+    table = cfg["rsx"].reshape(-1) * cfg["shape"][1] + cfg["rsz"].reshape(-1)
+    o = O.Oracle2D(cfg["vs"], cfg["vp"], cfg["rho"], cfg["dx"], cfg["dz"], cfg["dt"], cfg["isx"], cfg["isz"],
+                   int(cfg["rsx"].reshape(-1)[0]), int(cfg["rsz"].reshape(-1)[0]), cfg["nt"],
+                   cfg["accuracy"], cfg["freq"], cfg["surface"], cfg["pml"], wavelet=wav,
+                   MT=moment_2d(cfg["MT"]) if cfg.get("MT") is not None else None, rec_index=table)
+    return lambda it, n: o.run("VS", it, n)
+
+
+# above this many cell updates a whole CPU run would take too long for one
+# bench invocation (config 3: 6.4e10); the sample is then the run's first steps
+CPU_FULL_RUN_MAX_UPDATES = 2.0e10
+
+
+def cpu_segments(cfg, nseg: int):
+    """Time the oracle over the workload's time loop from rest, split into nseg
+    consecutive segments: [(time steps, seconds)].  The whole loop of nt steps
+    is run when it has at most CPU_FULL_RUN_MAX_UPDATES cell updates, else
+    its first steps up to that many."""
+    from oracle import oracle as O
+    O.set_threads(os.cpu_count() or 1)
     ncell = int(np.prod(cfg["shape"]))
-    t0 = time.perf_counter()
-    done = 0
-    while done < max_steps and (time.perf_counter() - t0) < min_seconds:
-        step(1 + done, 1)
-        done += 1
-    el = time.perf_counter() - t0
-    return {"value": ncell * done / el / 1e9, "unit": "Gcell-updates/s", "cores": threads, "kind": "port",
-            "sample": f"time steps 1..{done} of the full {'x'.join(map(str, cfg['shape']))} grid "
-                      f"({el:.1f} s, C++/OpenMP oracle restating the reference kernels)"}
+    total = min(cfg["nt"], max(1, int(CPU_FULL_RUN_MAX_UPDATES // ncell)))
+    nseg = max(1, min(int(nseg), total))
+    step = oracle_for(cfg)
+    bounds = [round(total * q / nseg) for q in range(nseg + 1)]
+    out = []
+    for a, b in zip(bounds[:-1], bounds[1:]):
+        t0 = time.perf_counter()
+        step(a, b - a)
+        out.append((b - a, time.perf_counter() - t0))
+    return out, total
+
+
+def cpu_sample_text(cfg, total, seconds):
+    run = "all" if total == cfg["nt"] else "the first"
+    return (f"{run} {total} of the {cfg['nt']} time steps of the full {'x'.join(map(str, cfg['shape']))} grid "
+            f"from rest ({seconds:.1f} s; C++/OpenMP oracle restating the reference kernels, "
+            f"bit-identical to them)")
+
+
+def cpu_baseline(cfg):
+    """The oracle on all host cores over the workload's time loop (one run,
+    timed whole; see cpu_segments for the cap)."""
+    segs, total = cpu_segments(cfg, 1)
+    el = sum(t for _, t in segs)
+    ncell = int(np.prod(cfg["shape"]))
+    return {"value": ncell * total / el / 1e9, "unit": "Gcell-updates/s", "cores": os.cpu_count() or 1,
+            "kind": "port", "sample": cpu_sample_text(cfg, total, el)}
+
+
+def workload_config(cfg, world):
+    """The `config` object of both arms' JSON lines (identical by construction)."""
+    three_d = len(cfg["shape"]) == 3
+    return {"workload": cfg["name"], "grid": list(cfg["shape"]), "time_steps": cfg["nt"],
+            "accuracy": cfg["accuracy"], "parallelism": f"replicas{world}",
+            "l2": "state larger than L2 (no flush needed)" if three_d else
+                  "state fits in L2 (2D 400^2); %HBM not meaningful"}
 
 
 def get_config(name):
@@ -241,23 +278,22 @@ def run_reference(args, rank, world):
             "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}), flush=True)
         return 0
     cfg = get_config(args.config)
-    samples = []
-    for s in range(args.warmup + args.steps):
-        b = cpu_baseline(cfg, min_seconds=4.0, max_steps=20)
-        if s >= args.warmup:
-            samples.append(b)
-    v = float(np.mean([b["value"] for b in samples]))
-    cb = dict(samples[-1])
-    cb["value"] = v
     ncell = int(np.prod(cfg["shape"]))
+    # warm-up: short runs from rest (caches, page faults, thread pool), untimed
+    for _ in range(args.warmup):
+        oracle_for(cfg)(0, 2)
+    # timed: the time loop from rest split into `steps` consecutive segments,
+    # so the timed region is one whole run (or its capped prefix)
+    segs, total = cpu_segments(cfg, args.steps)
+    el = sum(t for _, t in segs)
+    v = ncell * total / el / 1e9
     line = {
         "impl": "reference", "metric": "Gcell-updates/s", "value": v, "unit": "Gcell-updates/s",
-        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ncell * cfg["nt"] / (v * 1e9) * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": cfg["name"], "grid": list(cfg["shape"]), "time_steps": cfg["nt"],
-                   "accuracy": cfg["accuracy"]},
-        "cpu_baseline": cb,
+        "n_gpus": world, "steps": len(segs), "warmup": args.warmup, "ms_per_step": el / len(segs) * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": workload_config(cfg, world),
+        "cpu_baseline": {"value": v, "unit": "Gcell-updates/s", "cores": os.cpu_count() or 1, "kind": "port",
+                         "sample": cpu_sample_text(cfg, total, el) + f", timed as {len(segs)} segments"},
         "e2e": {"value": v, "unit": "Gcell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -327,6 +363,23 @@ def run_batch(args, rank, world, local):
         torch.cuda.synchronize()
     ms = max_over_ranks(e0.elapsed_time(e1), dist)
     value = whole_job_value(world, cells, nt, args.steps, ms)
+    # error of the batched float32 forward against float64 runs of the same
+    # scheme (the first four shots, one by one)
+    err64 = None
+    if rank == 0 and not args.no_fp64:
+        tr, fv = [], []
+        for c, w32 in list(zip(shots, waves))[:4]:
+            w64 = ElasticWAVE(c["vs"], c["vp"], c["rho"], c["dx"], c["dz"], c["dt"], c["isx"], c["isz"],
+                              c["rsx"], c["rsz"], c["nt"], c["accuracy"], c["freq"], torch.float64, MT=c["MT"],
+                              src_scale=c["src_scale"])
+            w64.SetADEPML2D(c["surface"], c["pml"])
+            w64.run(nt)
+            torch.cuda.synchronize()
+            for dst, a32, a64 in ((tr, w32.data, w64.data), (fv, w32.vx, w64.vx)):
+                dst.append(float(torch.linalg.norm(a32.double() - a64) / torch.linalg.norm(a64)))
+            del w64
+        err64 = {"shots": len(tr), "traces_rel_l2_max": max(tr), "final_vx_rel_l2_max": max(fv),
+                 "against": "float64 runs of the same scheme (f32 stencil coefficients, as the reference's f64 mode)"}
     # end to end: observed traces from host memory in, misfit gradient out
     d_obs = [w.data.detach().cpu().pin_memory() for w in waves]
     h2d = sum(t.numel() * t.element_size() for t in d_obs)
@@ -365,6 +418,7 @@ def run_batch(args, rank, world, local):
             "gpu_launches": args.steps * (2 * nt + 1),
             "clocks": clk.summary(),
             "cpu_baseline": None,
+            "fp64_error": err64,
         }
         print(json.dumps(line), flush=True)
     if dist:
@@ -527,6 +581,17 @@ def run_thin_layer(args, rank, world, local):
         e1.record()
         torch.cuda.synchronize()
         out[tag] = e0.elapsed_time(e1) / args.steps
+        if tag == "cpml20" and rank == 0 and not args.no_fp64:
+            # the 20-cell CPML run (the last timed shot) against float64
+            w64 = LA.solver3d(*m, h, dt, c, c, c, nt, npml=npml, freq=f0, dtype=torch.float64)
+            w64.run(nt)
+            torch.cuda.synchronize()
+            out["fp64"] = {"traces_rel_l2": float(torch.linalg.norm(w.data.double() - w64.data)
+                                                  / torch.linalg.norm(w64.data)),
+                           "final_vx_rel_l2": float(torch.linalg.norm(w.vx.double() - w64.vx)
+                                                    / torch.linalg.norm(w64.vx)),
+                           "scheme": "20-cell CPML grid (300^3 at n = 256), float64 run of the same scheme"}
+            del w64
         del w
     if rank == 0:
         cells = n ** 3
@@ -539,6 +604,7 @@ def run_thin_layer(args, rank, world, local):
                        "grids": {"cpml20": n + 2 * pad20, "learned6": n + 2 * pad6}, "time_steps": nt},
             "shots_per_s": {"learned6": 1e3 / out["learned6"], "cpml20": 1e3 / out["cpml20"]},
             "learned_over_cpml20": out["cpml20"] / out["learned6"],
+            "fp64_error": out.get("fp64"),
             "note": "shots run one after the other (no 3D shot batching); error gate measured on small grids "
                     "in tests/test_learned_abc3d.py",
             "gpu_launches": args.steps * (2 * nt + 2 * nt + 1),
@@ -690,11 +756,9 @@ def main(argv=None):
             "metric": "Gcell-updates/s", "value": value, "unit": "Gcell-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": cfg["name"], "grid": list(cfg["shape"]), "time_steps": nt,
-                       "accuracy": cfg["accuracy"], "parallelism": f"replicas{world}",
-                       "path": info, "numerics": "exact (bit-identical to the CPU oracle)",
-                       "l2": "state larger than L2 (no flush needed)" if three_d else
-                             "state fits in L2 (2D 400^2); %HBM not meaningful"},
+            "config": workload_config(cfg, world),
+            "implementation": {"path": info, "numerics": "exact (bit-identical to the reference's own source "
+                                                           "and to the CPU oracle)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "kernel": kname + " (one time step)",

@@ -114,8 +114,10 @@ class LearnedABC3D:
         return wave
 
 
-def solver3d(vp, vs, rho, h, dt, isx, isy, isz, nt, npml=L, N_=2, freq=15.0, MT=None, src_scale=1e6, rec=None):
-    """3D moment-tensor solver (exact numerics) with an npml-cell CPML."""
+def solver3d(vp, vs, rho, h, dt, isx, isy, isz, nt, npml=L, N_=2, freq=15.0, MT=None, src_scale=1e6, rec=None,
+             dtype=None):
+    """3D moment-tensor solver (exact numerics) with an npml-cell CPML
+    (float32 unless dtype is given)."""
     from .Elastic3D_SSG_Tensor import ElasticWAVE
     from .synthetic import pml_parameter
     nx, ny, nz = vp.shape
@@ -124,7 +126,7 @@ def solver3d(vp, vs, rho, h, dt, isx, isy, isz, nt, npml=L, N_=2, freq=15.0, MT=
     M = np.eye(3, dtype=np.float32) if MT is None else np.asarray(MT, np.float32)
     rx, ry, rz = (np.asarray(r, np.int64).reshape(1, -1) for r in rec)
     w = ElasticWAVE(vs, vp, rho, h, h, h, dt, isx, isy, isz, rx, ry, rz, M, src_scale, nt, N_, freq,
-                    torch.float32, exact=True)
+                    dtype or torch.float32, exact=True)
     w.SetADEPML3D([True] * 6, pml_parameter(float(vp.max()), float(vs.max()), h, freq, npml, dims=3))
     w._build_plan()
     return w
