@@ -146,7 +146,7 @@ struct sw_plan {
   bool staged = false;
   sw::StagedMaps svm{}, ssm{};
   sw::StagedArgs sa{};
-  int staged_grid = 0, staged_N = 0;
+  int staged_grid = 0, staged_N = 0, staged_tz = 32;
   // 0: register-queue two-pass kernels (2D: two launches per step), 1: staged
   // two-pass, 2: fused single pass, 3: 2D persistent (one cooperative launch
   // per run)
@@ -361,6 +361,14 @@ cudaError_t enqueue3(sw_plan* pl, const sw::P3<T>& p, int it, bool first, bool l
     if (e != cudaSuccess) return e;
   }
   if (pl->scheme == SW3D_SPML) {
+    if constexpr (std::is_same<T, float>::value) {
+      if (pl->path >= 1 && pl->staged) {
+        e = sw::sw3_staged_step(pl->staged_N, pl->staged_tz, true, false, p, pl->svm, pl->ssm, pl->sa, it,
+                                pl->src_kind == SW_SRC_FORCE, false, pl->gather_in_stress, st);
+        if (e == cudaSuccess && !pl->gather_in_stress) e = sw::sw3_gather<T>(p, it, st);
+        return e;
+      }
+    }
     e = sw::sw3_spml_step<T>(q, pl->order, it, pl->gather_in_stress, st);
     if (e == cudaSuccess && !pl->gather_in_stress) e = sw::sw3_gather<T>(p, it, st);
     return e;
@@ -380,7 +388,7 @@ cudaError_t enqueue3(sw_plan* pl, const sw::P3<T>& p, int it, bool first, bool l
   if constexpr (std::is_same<T, float>::value) {
     if (pl->path >= 1 && pl->staged) {
       const bool inject_next = moment && !last && !unfold;
-      e = sw::sw3_staged_step(pl->staged_N, tensor, p, pl->svm, pl->ssm, pl->sa, pl->staged_grid, it, force,
+      e = sw::sw3_staged_step(pl->staged_N, pl->staged_tz, false, tensor, p, pl->svm, pl->ssm, pl->sa, it, force,
                               inject_next, pl->gather_in_stress, st);
       if (e != cudaSuccess) return e;
       if (!pl->gather_in_stress) e = sw::sw3_gather<T>(p, it, st);
@@ -518,10 +526,10 @@ int units_grid(int units, int per_sm) {
 void staged_chunks(sw_plan* pl, int len) {
   const auto& p = pl->p3f;
   sw::StagedConfig sc;
-  sw::sw3_staged_config(pl->staged_N, &sc);
+  sw::sw3_staged_config(pl->staged_N, pl->staged_tz, &sc);
   auto& a = pl->sa;
   a.tiles_y = (p.ny + sc.TY - 1) / sc.TY;
-  a.tiles_z = (p.nz + 31) / 32;
+  a.tiles_z = (p.nz + sc.TZ - 1) / sc.TZ;
   if (len <= 0) {
     // about five work units per resident CTA
     int dev = 0, sms = 148;
@@ -545,12 +553,18 @@ void staged_chunks(sw_plan* pl, int len) {
 void setup_staged(sw_plan* pl) {
   pl->staged = false;
   if (pl->dim != 3 || pl->dtype != SW_F32) return;
-  if (pl->scheme != SW3D_CPML_TENSOR && pl->scheme != SW3D_CPML_FORCE) return;
+  if (pl->scheme != SW3D_CPML_TENSOR && pl->scheme != SW3D_CPML_FORCE && pl->scheme != SW3D_SPML) return;
   if (!pl->src_in_kernel) return;
-  sw::StagedConfig sc;
-  if (!sw::sw3_staged_config(pl->order, &sc)) return;
   auto& p = pl->p3f;
+  // the staged passes stream planes [N, nx-N): a point force outside them
+  // needs the per-cell split-PML kernels
+  if (pl->scheme == SW3D_SPML && pl->src_kind != SW_SRC_NONE && (p.si < pl->order || p.si >= p.nx - pl->order))
+    return;
   if (p.nz % 4 != 0) return;
+  // z tile width: the one leaving fewer idle cells in the last tile (32 on ties)
+  const int tz = (p.nz + 39) / 40 * 40 < (p.nz + 31) / 32 * 32 ? 40 : 32;
+  sw::StagedConfig sc;
+  if (!sw::sw3_staged_config(pl->order, tz, &sc)) return;
   for (int q = 0; q < 9; ++q)
     if (!aligned(p.f[q], 16)) return;
   if (!aligned(p.rho, 16) || !aligned(p.lam, 16) || !aligned(p.mu, 16)) return;
@@ -562,8 +576,9 @@ void setup_staged(sw_plan* pl) {
     if (cudaMalloc(&pl->d_err, sizeof(int)) != cudaSuccess) { cudaGetLastError(); return; }
     cudaMemset(pl->d_err, 0, sizeof(int));
   }
-  if (!sw::sw3_staged_maps(pl->order, p, &pl->svm, &pl->ssm)) return;
+  if (!sw::sw3_staged_maps(pl->order, tz, p, &pl->svm, &pl->ssm)) return;
   pl->staged_N = pl->order;
+  pl->staged_tz = tz;
   pl->sa.err = pl->d_err;
   pl->sa.exact = 1;
   staged_chunks(pl, 0);

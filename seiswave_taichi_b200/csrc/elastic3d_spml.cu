@@ -15,14 +15,6 @@ namespace sw {
 constexpr int TSZ = 32;
 constexpr int TSY = 8;
 
-// split-field order (reference names)
-enum {
-  PVX_X = 0, PVX_Y, PVX_Z, PVY_X, PVY_Y, PVY_Z, PVZ_X, PVZ_Y, PVZ_Z,
-  PSXX_X, PSXX_Y, PSXX_Z, PSYY_X, PSYY_Y, PSYY_Z,
-  PSXY_X, PSXY_Y, PSXZ_X, PSXZ_Z, PSYZ_Y, PSYZ_Z,
-  PSZZ_X, PSZZ_Y, PSZZ_Z
-};
-
 template <typename T, int N>
 __device__ __forceinline__ T d_fm(const T* f, long long idx, long long s, const T* c) {
   T v = 0;

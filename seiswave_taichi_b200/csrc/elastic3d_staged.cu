@@ -36,13 +36,18 @@ namespace sw {
 // kernels, with shorter chains, keep four cells (482 us; 594 with two).
 constexpr int staged_q(bool exact) { return exact ? 2 : 4; }
 
-template <int N, int TY, int D, int Q>
+// TZ: z cells of a tile, 32 or 40 (the plan takes the width that covers nz
+// with the fewest idle cells: 40 divides the 200-cell grids of the 3D
+// workloads, where 32-wide tiles leave a last tile of 8)
+template <int N, int TY, int D, int Q, int TZ_ = 32>
 struct SG {
-  static constexpr int TZ = 32;
+  static constexpr int TZ = TZ_;
   static constexpr int CQ = TZ / Q;            // threads along z: Q cells each
   static constexpr int NT = TY * CQ;
-  static constexpr int MINB = 3;              // CTAs per SM the register budget aims at
-  static constexpr int MINB_S = Q == 4 ? 3 : 2;  // same for the stress pass
+  // CTAs per SM the register budget aims at (velocity pass, stress pass)
+  static constexpr int MINB = NT <= 256 ? 3 : 2;
+  static constexpr int MINB_S = Q == 4 && TZ == 32 ? 3 : 2;
+  static_assert(TZ % 4 == 0 && TZ % Q == 0, "z tile");
   static constexpr int H4 = ((N + 3) / 4) * 4; // z halo, rounded to 16 bytes
   static constexpr int WZ = TZ + 2 * H4;       // width of boxes with a z halo
   static constexpr int HY = TY + 2 * N;        // height of boxes with a y halo
@@ -68,14 +73,17 @@ struct SG {
   static constexpr int V_YZ = V_YY + R1 * pad(B_Y);
   static constexpr int V_ZZ = V_YZ + R1 * pad(B_YZ);
   static constexpr int V_R = V_ZZ + R1 * pad(B_Z);
-  static constexpr int V_FLOATS = V_R + R2 * pad(B_R);
+  static constexpr int V_TAB = V_R + R2 * pad(B_R);  // CPML tables of the unit's rows and z cells
+  static constexpr int TAB = pad(6 * (TY + TZ));
+  static constexpr int V_FLOATS = V_TAB + TAB;
   // stress pass layout (floats)
   static constexpr int S_VX = 0;
   static constexpr int S_VY = S_VX + RX * pad(B_YZ);
   static constexpr int S_VZ = S_VY + RX * pad(B_YZ);
   static constexpr int S_L = S_VZ + RX * pad(B_YZ);
   static constexpr int S_M = S_L + R2 * pad(B_L);
-  static constexpr int S_FLOATS = S_M + R2 * pad(B_M);
+  static constexpr int S_TAB = S_M + R2 * pad(B_M);
+  static constexpr int S_FLOATS = S_TAB + TAB;
   static constexpr size_t V_BYTES = (size_t)V_FLOATS * 4 + 8 * (D + 1) + 128;
   static constexpr size_t S_BYTES = (size_t)S_FLOATS * 4 + 8 * (D + 1) + 128;
   static_assert(N <= 4 || H4 >= N, "z window");
@@ -108,6 +116,21 @@ template <int Q>
 __device__ __forceinline__ Vq<Q> ldgq(const float* p) {
   return __ldg(reinterpret_cast<const Vq<Q>*>(p));
 }
+// Exact mode with two z cells per thread computes on cell pairs with the
+// packed two-lane FP32 instructions of sm_100 (__fadd2_rn, __fmul2_rn,
+// __ffma2_rn): each lane is one IEEE round-to-nearest operation, the same
+// bits as the scalar instruction, at half the instruction count.
+#ifndef SW_STAGED_PACKED
+#define SW_STAGED_PACKED 1
+#endif
+template <bool EX, int Q>
+constexpr bool packed() { return SW_STAGED_PACKED && EX && Q == 2; }
+__device__ __forceinline__ float2 sp2(float c) { return make_float2(c, c); }
+// a - b with one rounding: fma(b, -1, a)
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, sp2(-1.f), a); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+
 __device__ __forceinline__ float g4(const float4& v, int e) { return e == 0 ? v.x : e == 1 ? v.y : e == 2 ? v.z : v.w; }
 __device__ __forceinline__ void s4(float4& v, int e, float x) {
   if (e == 0) v.x = x; else if (e == 1) v.y = x; else if (e == 2) v.z = x; else v.w = x;
@@ -116,18 +139,22 @@ __device__ __forceinline__ float g4(const float2& v, int e) { return e == 0 ? v.
 __device__ __forceinline__ void s4(float2& v, int e, float x) {
   if (e == 0) v.x = x; else v.y = x;
 }
-__device__ __forceinline__ int rslot(int plane, int R) {
-  int s = plane % R;
-  return s < 0 ? s + R : s;
-}
+// ring slot of an x plane: planes are never negative here (the loops start
+// at x0 >= N and reach back at most N planes), so an unsigned remainder
+// needs no sign fix-up
+__device__ __forceinline__ int rslot(int plane, int R) { return (int)((unsigned)plane % (unsigned)R); }
 
 // acc += c * (a - b) lane by lane in the reference's operation order (exact
 // mode), or acc = fma(c, a - b, acc) with the spacing folded into c (fast mode)
 template <bool EX, int Q>
 __device__ __forceinline__ void tapq(Vq<Q>& acc, float c, const Vq<Q>& a, const Vq<Q>& b) {
+  if constexpr (packed<EX, Q>()) {
+    acc = add2(acc, mul2(sp2(c), sub2(a, b)));
+  } else {
 #pragma unroll
-  for (int e = 0; e < Q; ++e)
-    s4(acc, e, EX ? g4(acc, e) + c * (g4(a, e) - g4(b, e)) : __fmaf_rn(c, g4(a, e) - g4(b, e), g4(acc, e)));
+    for (int e = 0; e < Q; ++e)
+      s4(acc, e, EX ? g4(acc, e) + c * (g4(a, e) - g4(b, e)) : __fmaf_rn(c, g4(a, e) - g4(b, e), g4(acc, e)));
+  }
 }
 
 // derivative across ring planes: pl[q] is the plane (centre - N + q + FWD)
@@ -194,10 +221,22 @@ __device__ __forceinline__ void div_group(Vq<Q> (&v)[K], const float (&d)[K], co
 #pragma unroll
     for (int e = 0; e < Q; ++e) ok = ok & mk_ok(g4(v[k], e));
   if (ok) {
+    if constexpr (packed<true, Q>()) {
+      // Markstein's correction on pairs; a zero numerator gives +0 like
+      // mk_div (a stencil sum, which starts from +0 + c*(a-b), is never -0)
 #pragma unroll
-    for (int k = 0; k < K; ++k)
+      for (int k = 0; k < K; ++k) {
+        const float2 rr = sp2(r[k]);
+        const float2 q = mul2(v[k], rr);
+        const float2 e = __ffma2_rn(q, sp2(-d[k]), v[k]);
+        v[k] = __ffma2_rn(e, rr, q);
+      }
+    } else {
 #pragma unroll
-      for (int e = 0; e < Q; ++e) s4(v[k], e, mk_div(g4(v[k], e), d[k], r[k]));
+      for (int k = 0; k < K; ++k)
+#pragma unroll
+        for (int e = 0; e < Q; ++e) s4(v[k], e, mk_div(g4(v[k], e), d[k], r[k]));
+    }
   } else {
 #pragma unroll
     for (int k = 0; k < K; ++k)
@@ -212,106 +251,235 @@ __device__ __forceinline__ float dvv(float x, float d) {
   return EX ? div_v(x, d) : __fdividef(x, d);
 }
 
-// CPML on a quad: x and y slabs are per plane / per row, z per cell.
-// comp: memory-variable component; h: 0 integer / 1 half point per axis;
-// bits: predicate bits of the three axes (fx, fy, fz per cell).
-struct QuadPml {
-  int xi, yj, i, j, k;
-  uint8_t fx, fy;
-};
+// CPML memory variables.  Outside the slab of an axis the reference's update
+// of that axis's memory variable, psi = b*psi + a*d and d = d/kappa + psi, is
+// an exact no-op (a = 0, b = 1 and kappa = 1 there, and psi stays 0), so only
+// slab cells store memory variables (slab-compact layout) and only they run
+// the update.  A slab cell lies inside that axis's PML, where the reference's
+// CPML predicate holds, so the update is gated by the component's update
+// range alone.  x slabs are whole planes (a uniform branch), y slabs whole
+// rows of a thread, z slabs single cells.
 
-// Memory variables of one quad on the slabs it lies in, components
-// c0 .. c0+2 of each axis: x and y slab rows as vectors, z slab per cell.
-// quad_mem_load issues every load before any update, so the latencies of the
-// up to nine rows overlap instead of forming one load-update-store chain per
-// component and axis; quad_mem_store writes them back after the updates.
-template <int Q>
-struct QuadMem {
-  Vq<Q> x[3], y[3];
-  float z[3][Q];
-  int zk[Q];
-};
-
-__device__ __forceinline__ float* memx_ptr(const P3<float>& p, const QuadPml& q, int comp) {
-  return p.mem[0] + comp * p.mcomp[0] + ((size_t)q.xi * p.ny + q.j) * p.nz + q.k;
-}
-__device__ __forceinline__ float* memy_ptr(const P3<float>& p, const QuadPml& q, int comp) {
-  return p.mem[1] + comp * p.mcomp[1] + ((size_t)q.i * p.sn[1] + q.yj) * p.nz + q.k;
-}
-__device__ __forceinline__ float* memz_ptr(const P3<float>& p, const QuadPml& q, int comp, int zk) {
-  return p.mem[2] + comp * p.mcomp[2] + ((size_t)q.i * p.ny + q.j) * p.sn[2] + zk;
+// psi update of one value: returns the new psi; d becomes d/kappa + psi
+template <bool EX>
+__device__ __forceinline__ float cpml1(float& d, float psi, float b, float aa, float kk) {
+  const float np = b * psi + aa * d;
+  d = dvv<EX>(d, kk) + np;
+  return np;
 }
 
-template <int Q>
-__device__ __forceinline__ void quad_mem_load(const P3<float>& p, const QuadPml& q, int c0, QuadMem<Q>& m) {
-#pragma unroll
-  for (int e = 0; e < Q; ++e) m.zk[e] = q.k + e < p.nz ? slab_index(q.k + e, p.nz, p.lo[2], p.hi[2]) : -1;
-  if (q.xi >= 0) {
-#pragma unroll
-    for (int c = 0; c < 3; ++c) m.x[c] = ldq<Q>(memx_ptr(p, q, c0 + c));
-  }
-  if (q.yj >= 0) {
-#pragma unroll
-    for (int c = 0; c < 3; ++c) m.y[c] = ldq<Q>(memy_ptr(p, q, c0 + c));
-  }
+// one derivative pair d on an axis whose coefficients are the same for the
+// pair's cells (x and y), memory variables o, update mask m
+template <bool EX, int Q>
+__device__ __forceinline__ void cpml_pair(Vq<Q>& d, Vq<Q>& o, const bool (&m)[Q], float b, float aa, float kk) {
 #pragma unroll
   for (int e = 0; e < Q; ++e)
-    if (m.zk[e] >= 0) {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) m.z[c][e] = *memz_ptr(p, q, c0 + c, m.zk[e]);
+    if (m[e]) {
+      float de = g4(d, e);
+      s4(o, e, cpml1<EX>(de, g4(o, e), b, aa, kk));
+      s4(d, e, de);
     }
+}
+
+// per-unit CPML table of the tile's rows (y) or z cells: row q of the axis
+// coefficient table (b, a, kappa at integer points, then at half points)
+__device__ __forceinline__ float tab(const float* t, int row, int len, int at) { return t[row * len + at]; }
+
+// fill the unit's y and z tables; the previous unit's readers have passed the
+// last barrier of its plane loop, and the first wait of this unit's loop ends
+// in a barrier before any read
+template <int TY, int TZ, int NT>
+__device__ __forceinline__ void fill_tables(const P3<float>& p, float* tyt, float* tzt, int j0, int k0, int tid) {
+  for (int q = tid; q < 6 * (TY + TZ); q += NT) {
+    if (q < 6 * TY) {
+      const int row = q / TY, jj = j0 + q % TY;
+      tyt[q] = jj < p.ny ? __ldg(p.cf[1] + row * p.ny + jj) : 0.f;
+    } else {
+      const int q2 = q - 6 * TY, row = q2 / TZ, kk = k0 + q2 % TZ;
+      tzt[q2] = kk < p.nz ? __ldg(p.cf[2] + row * p.nz + kk) : 0.f;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// split-field PML (src/Elastic3D_SSG_SPML.py:160-393) on the same staged
+// tiles: inside a component's PML predicate its split parts advance as
+//   psi_d = ((1 - dt/2 d) psi_d + term_d) / (1 + dt/2 d)
+// and the field is set to their sum; elsewhere the plain update.  The split
+// fields live on the PML shell (shell_index); a cell with a predicate bit set
+// lies in the shell.
+// ---------------------------------------------------------------------------
+enum { SCH_CPML = 0, SCH_SPML = 1 };
+
+__device__ __forceinline__ float spml_part(float psi, float term, float damp, float hdt) {
+  return div_v((1.f - hdt * damp) * psi + term, 1.f + hdt * damp);
 }
 
 template <int Q>
-__device__ __forceinline__ void quad_mem_store(const P3<float>& p, const QuadPml& q, int c0, const QuadMem<Q>& m) {
-  if (q.xi >= 0) {
+__device__ __forceinline__ void spml_velocity(const P3<float>& p, int i, int j, int k, uint8_t fy,
+                                              const uint8_t (&fz)[Q], float dt, const bool (&mx)[Q],
+                                              const bool (&my)[Q], const bool (&mz)[Q], const Vq<Q>& a1,
+                                              const Vq<Q>& a2, const Vq<Q>& a3, const Vq<Q>& b1, const Vq<Q>& b2,
+                                              const Vq<Q>& b3, const Vq<Q>& c1, const Vq<Q>& c2, const Vq<Q>& c3,
+                                              const Vq<Q>& rc, const Vq<Q>& rn, const Vq<Q>& r1c, const Vq<Q>& r1n,
+                                              Vq<Q>& vx, Vq<Q>& vy, Vq<Q>& vz) {
+  const int nx = p.nx, ny = p.ny, nz = p.nz;
+  const uint8_t fx = p.fl[0][i];
+  const float hdt = 0.5f * dt;
+  const float *dpx = p.dmp[0], *dpy = p.dmp[1], *dpz = p.dmp[2];
+  float* sp = p.split;
+  const long long G = p.scomp;
 #pragma unroll
-    for (int c = 0; c < 3; ++c) stq<Q>(memx_ptr(p, q, c0 + c), m.x[c]);
-  }
-  if (q.yj >= 0) {
-#pragma unroll
-    for (int c = 0; c < 3; ++c) stq<Q>(memy_ptr(p, q, c0 + c), m.y[c]);
-  }
-#pragma unroll
-  for (int e = 0; e < Q; ++e)
-    if (m.zk[e] >= 0) {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) *memz_ptr(p, q, c0 + c, m.zk[e]) = m.z[c][e];
+  for (int e = 0; e < Q; ++e) {
+    const int kk = k + e;
+    const uint8_t fze = fz[e];
+    const long long sh = (fx | fy | fze) ? shell_index(p, i, j, kk) : 0;
+    const float rce = g4(rc, e), rne = g4(rn, e);
+    // vx (:182-205): x half, y and z integer; rho unaveraged
+    if (mx[e]) {
+      const float ro = __fdiv_rn(1.f, rce);
+      const float d1 = g4(a1, e), d2 = g4(a2, e), d3 = g4(a3, e);
+      if ((fx & 2) || (fy & 1) || (fze & 1)) {
+        float* s = sp + PVX_X * G + sh;
+        const float A = spml_part(s[0], d1 * dt * ro, __ldg(dpx + nx + i), hdt);
+        const float B = spml_part(s[G], d2 * dt * ro, __ldg(dpy + j), hdt);
+        const float C = spml_part(s[2 * G], d3 * dt * ro, __ldg(dpz + kk), hdt);
+        s[0] = A;
+        s[G] = B;
+        s[2 * G] = C;
+        s4(vx, e, A + B + C);
+      } else {
+        s4(vx, e, g4(vx, e) + (d1 + d2 + d3) * dt * ro);
+      }
     }
+    // vy (:209-233): y half; rho averaged over j, j+1
+    if (my[e]) {
+      const float ro = __fdiv_rn(1.f, 0.5f * (rce + rne));
+      const float d1 = g4(b1, e), d2 = g4(b2, e), d3 = g4(b3, e);
+      if ((fx & 1) || (fy & 2) || (fze & 1)) {
+        float* s = sp + PVY_X * G + sh;
+        const float A = spml_part(s[0], dt * d1 * ro, __ldg(dpx + i), hdt);
+        const float B = spml_part(s[G], dt * d2 * ro, __ldg(dpy + ny + j), hdt);
+        const float C = spml_part(s[2 * G], dt * d3 * ro, __ldg(dpz + kk), hdt);
+        s[0] = A;
+        s[G] = B;
+        s[2 * G] = C;
+        s4(vy, e, A + B + C);
+      } else {
+        s4(vy, e, g4(vy, e) + (d1 + d2 + d3) * dt * ro);
+      }
+    }
+    // vz (:235-259): z half; rho averaged over the x-y quad
+    if (mz[e]) {
+      const float ro = __fdiv_rn(1.f, 0.25f * (rce + rne + g4(r1n, e) + g4(r1c, e)));
+      const float d1 = g4(c1, e), d2 = g4(c2, e), d3 = g4(c3, e);
+      if ((fx & 1) || (fy & 1) || (fze & 2)) {
+        float* s = sp + PVZ_X * G + sh;
+        const float A = spml_part(s[0], dt * d1 * ro, __ldg(dpx + i), hdt);
+        const float B = spml_part(s[G], dt * d2 * ro, __ldg(dpy + j), hdt);
+        const float C = spml_part(s[2 * G], dt * d3 * ro, __ldg(dpz + nz + kk), hdt);
+        s[0] = A;
+        s[G] = B;
+        s[2 * G] = C;
+        s4(vz, e, A + B + C);
+      } else {
+        s4(vz, e, g4(vz, e) + (d1 + d2 + d3) * dt * ro);
+      }
+    }
+  }
 }
 
-// CPML of one derivative quad d on axis AX from the preloaded memory
-// variables (component c of m), updated in place
-template <int AX, bool EX, int Q>
-__device__ __forceinline__ void pml_quad_m(const P3<float>& p, const QuadPml& q, int c, int half, const int* pm,
-                                           Vq<Q>& d, QuadMem<Q>& m) {
-  const float* cf = p.cf[AX];
-  const int n = AX == 0 ? p.nx : AX == 1 ? p.ny : p.nz;
-  const int ob = half ? CBH : CB, oa = half ? CAH : CA, ok = half ? CKH : CK;
-  if (AX == 0 || AX == 1) {
-    const int si = AX == 0 ? q.xi : q.yj;
-    if (si < 0) return;
-    const int idx = AX == 0 ? q.i : q.j;
-    const float b = __ldg(cf + ob * n + idx), a = __ldg(cf + oa * n + idx), kk = __ldg(cf + ok * n + idx);
-    Vq<Q>& o = AX == 0 ? m.x[c] : m.y[c];
+template <int Q>
+__device__ __forceinline__ void spml_stress(const P3<float>& p, int i, int j, int k, uint8_t fy,
+                                            const uint8_t (&fz)[Q], float dt, const bool (&mn)[Q],
+                                            const bool (&mxy)[Q], const bool (&mxz)[Q], const bool (&myz)[Q],
+                                            const Vq<Q>& e1, const Vq<Q>& e2, const Vq<Q>& e3, const Vq<Q>& f1,
+                                            const Vq<Q>& f2, const Vq<Q>& h1, const Vq<Q>& h2, const Vq<Q>& q1,
+                                            const Vq<Q>& q2, const Vq<Q>& l0, const Vq<Q>& u0, const Vq<Q>& u1,
+                                            const Vq<Q>& unj, const float (&unk)[Q], Vq<Q>& sxx, Vq<Q>& syy,
+                                            Vq<Q>& szz, Vq<Q>& sxy, Vq<Q>& sxz, Vq<Q>& syz) {
+  const int nx = p.nx, ny = p.ny, nz = p.nz;
+  const uint8_t fx = p.fl[0][i];
+  const float hdt = 0.5f * dt;
+  const float *dpx = p.dmp[0], *dpy = p.dmp[1], *dpz = p.dmp[2];
+  float* sp = p.split;
+  const long long G = p.scomp;
 #pragma unroll
-    for (int e = 0; e < Q; ++e) {
-      if (!pm[e]) continue;
-      const float de = g4(d, e);
-      const float psi = b * g4(o, e) + a * de;
-      s4(o, e, psi);
-      s4(d, e, dvv<EX>(de, kk) + psi);
+  for (int e = 0; e < Q; ++e) {
+    const int kk = k + e;
+    const uint8_t fze = fz[e];
+    const long long sh = (fx | fy | fze) ? shell_index(p, i, j, kk) : 0;
+    const float u = g4(u0, e);
+    // normal stresses (:296-333): unaveraged lambda and mu
+    if (mn[e]) {
+      const float lm = g4(l0, e);
+      const float l2m = lm + 2.f * u;
+      const float A = g4(e1, e), B = g4(e2, e), Cc = g4(e3, e);
+      if ((fx | fy | fze) & 1) {
+        const float dX = __ldg(dpx + i), dY = __ldg(dpy + j), dZ = __ldg(dpz + kk);
+        float* s = sp + sh;
+        const float xx = spml_part(s[PSXX_X * G], dt * l2m * A, dX, hdt);
+        const float xy = spml_part(s[PSXX_Y * G], dt * lm * B, dY, hdt);
+        const float xz = spml_part(s[PSXX_Z * G], dt * lm * Cc, dZ, hdt);
+        const float yx = spml_part(s[PSYY_X * G], dt * lm * A, dX, hdt);
+        const float yy = spml_part(s[PSYY_Y * G], dt * l2m * B, dY, hdt);
+        const float yz = spml_part(s[PSYY_Z * G], dt * lm * Cc, dZ, hdt);
+        const float zx = spml_part(s[PSZZ_X * G], dt * lm * A, dX, hdt);
+        const float zy = spml_part(s[PSZZ_Y * G], dt * lm * B, dY, hdt);
+        const float zz = spml_part(s[PSZZ_Z * G], dt * l2m * Cc, dZ, hdt);
+        s[PSXX_X * G] = xx; s[PSXX_Y * G] = xy; s[PSXX_Z * G] = xz;
+        s[PSYY_X * G] = yx; s[PSYY_Y * G] = yy; s[PSYY_Z * G] = yz;
+        s[PSZZ_X * G] = zx; s[PSZZ_Y * G] = zy; s[PSZZ_Z * G] = zz;
+        s4(sxx, e, xx + xy + xz);
+        s4(syy, e, yx + yy + yz);
+        s4(szz, e, zx + zy + zz);
+      } else {
+        s4(sxx, e, g4(sxx, e) + (l2m * A + lm * (Cc + B)) * dt);
+        s4(syy, e, g4(syy, e) + (l2m * B + lm * (A + Cc)) * dt);
+        s4(szz, e, g4(szz, e) + (l2m * Cc + lm * (A + B)) * dt);
+      }
     }
-  } else {
-#pragma unroll
-    for (int e = 0; e < Q; ++e) {
-      if (!pm[e] || m.zk[e] < 0) continue;
-      const int kk_ = q.k + e;
-      const float b = __ldg(cf + ob * n + kk_), a = __ldg(cf + oa * n + kk_), kk = __ldg(cf + ok * n + kk_);
-      const float de = g4(d, e);
-      const float psi = b * m.z[c][e] + a * de;
-      m.z[c][e] = psi;
-      s4(d, e, dvv<EX>(de, kk) + psi);
+    // sxy (:334-350): x half, y half
+    if (mxy[e]) {
+      const float m4 = 0.25f * (g4(unj, e) + u + u + g4(u1, e));
+      if ((fx & 2) || (fy & 2) || (fze & 1)) {
+        float* s = sp + PSXY_X * G + sh;
+        const float a = spml_part(s[0], dt * m4 * g4(f1, e), __ldg(dpx + nx + i), hdt);
+        const float b = spml_part(s[G], dt * m4 * g4(f2, e), __ldg(dpy + ny + j), hdt);
+        s[0] = a;
+        s[G] = b;
+        s4(sxy, e, a + b);
+      } else {
+        s4(sxy, e, g4(sxy, e) + m4 * (g4(f2, e) + g4(f1, e)) * dt);
+      }
+    }
+    // sxz (:352-371): x half, z half
+    if (mxz[e]) {
+      const float m4 = 0.25f * (u + g4(u1, e) + u + g4(unj, e));
+      if ((fx & 2) || (fy & 1) || (fze & 2)) {
+        float* s = sp + PSXZ_X * G + sh;
+        const float a = spml_part(s[0], dt * m4 * g4(h1, e), __ldg(dpx + nx + i), hdt);
+        const float b = spml_part(s[G], dt * m4 * g4(h2, e), __ldg(dpz + nz + kk), hdt);
+        s[0] = a;
+        s[G] = b;
+        s4(sxz, e, a + b);
+      } else {
+        s4(sxz, e, g4(sxz, e) + m4 * (g4(h2, e) + g4(h1, e)) * dt);
+      }
+    }
+    // syz (:373-391): y half, z half; its plain update adds dvy/dz + dvz/dy
+    if (myz[e]) {
+      const float m4 = 0.25f * (g4(unj, e) + u + unk[e] + u);
+      if ((fx & 1) || (fy & 2) || (fze & 2)) {
+        float* s = sp + PSYZ_Y * G + sh;
+        const float a = spml_part(s[0], dt * m4 * g4(q1, e), __ldg(dpy + ny + j), hdt);
+        const float b = spml_part(s[G], dt * m4 * g4(q2, e), __ldg(dpz + nz + kk), hdt);
+        s[0] = a;
+        s[G] = b;
+        s4(syz, e, a + b);
+      } else {
+        s4(syz, e, g4(syz, e) + m4 * (g4(q2, e) + g4(q1, e)) * dt);
+      }
     }
   }
 }
@@ -319,13 +487,15 @@ __device__ __forceinline__ void pml_quad_m(const P3<float>& p, const QuadPml& q,
 // ---------------------------------------------------------------------------
 // velocity pass
 // ---------------------------------------------------------------------------
-template <int N, int TY, int D, bool TENSOR, bool EX, int Q>
-__global__ void __launch_bounds__(SG<N, TY, D, Q>::NT, SG<N, TY, D, Q>::MINB)
+template <int N, int TY, int D, bool TENSOR, bool EX, int Q, int TZ, int SCH>
+__global__ void __launch_bounds__(SG<N, TY, D, Q, TZ>::NT, SG<N, TY, D, Q, TZ>::MINB)
 k3s_velocity(const __grid_constant__ P3<float> p, const __grid_constant__ StagedMaps maps,
              const __grid_constant__ StagedArgs a, int it, int force_here) {
-  using G = SG<N, TY, D, Q>;
+  using G = SG<N, TY, D, Q, TZ>;
   extern __shared__ __align__(128) float sm[];
   uint64_t* bars = reinterpret_cast<uint64_t*>(sm + G::V_FLOATS);
+  float* tyt = sm + G::V_TAB;   // [6][TY]
+  float* tzt = tyt + 6 * TY;    // [6][TZ]
   const int tid = threadIdx.x;
   const int nx = p.nx, ny = p.ny, nz = p.nz;
   const size_t nyz = (size_t)ny * nz;
@@ -372,21 +542,31 @@ k3s_velocity(const __grid_constant__ P3<float> p, const __grid_constant__ Staged
     const int j0 = tyi * TY, k0 = tzi * G::TZ;
     const int x0 = max(ch * a.chunk_len, N), x1 = min(min((ch + 1) * a.chunk_len, nx - N), nx);
     if (x0 >= x1) continue;
+    if (SCH == SCH_CPML) fill_tables<TY, G::TZ, G::NT>(p, tyt, tzt, j0, k0, tid);
     const int j = j0 + r, k = k0 + Q * cq;
     const bool jin = j < ny, kin = k < nz;
-    // tile-level interior test (y and z): every cell inside every update
-    // range and outside the CPML slabs
-    const bool tile_in = j0 >= N + 1 && j0 + TY <= ny - N - 1 && k0 >= N + 1 && k0 + G::TZ <= nz - N - 1 &&
-                         j0 >= p.lo[1] && j0 + TY <= ny - p.hi[1] && k0 >= p.lo[2] && k0 + G::TZ <= nz - p.hi[2];
-    const int yj = jin ? slab_index(j, ny, p.lo[1], p.hi[1]) : -1;
-    const uint8_t fy = jin ? p.fl[1][j] : 0;
-    bool zslab = false;
-    uint8_t fz[Q];
+    const int yj = SCH == SCH_CPML && jin ? slab_index(j, ny, p.lo[1], p.hi[1]) : -1;
+    int zk[Q];
+    bool zany = false;
 #pragma unroll
     for (int e = 0; e < Q; ++e) {
-      const int kk = k + e;
-      fz[e] = kk < nz ? p.fl[2][kk] : 0;
-      zslab = zslab || (kk < nz && slab_index(kk, nz, p.lo[2], p.hi[2]) >= 0);
+      zk[e] = SCH == SCH_CPML && k + e < nz ? slab_index(k + e, nz, p.lo[2], p.hi[2]) : -1;
+      zany = zany || zk[e] >= 0;
+    }
+    // update ranges in y and z (Elastic3D_SSG_Tensor.py:194,210,226):
+    // vx and vz rows j in [N+1, ny-N), vy rows j in [N, ny-N-1); vx and vy
+    // cells k in [N+1, nz-N), vz cells k in [N, nz-N-1)
+    const bool jxz = j >= N + 1 && j < ny - N, jy = j >= N && j < ny - N - 1;
+    // split PML: predicate flags of the row and of the z cells
+    const uint8_t fy = SCH == SCH_SPML && jin ? p.fl[1][j] : 0;
+    uint8_t fz[Q];
+#pragma unroll
+    for (int e = 0; e < Q; ++e) fz[e] = SCH == SCH_SPML && k + e < nz ? p.fl[2][k + e] : 0;
+    bool kxy[Q], kz[Q];
+#pragma unroll
+    for (int e = 0; e < Q; ++e) {
+      kxy[e] = k + e >= N + 1 && k + e < nz - N;
+      kz[e] = k + e >= N && k + e < nz - N - 1;
     }
 
     auto issue = [&](int s, bool first, uint32_t stage) {
@@ -422,10 +602,7 @@ k3s_velocity(const __grid_constant__ P3<float> p, const __grid_constant__ Staged
         ok = false;
         break;
       }
-      const int xi = slab_index(i, nx, p.lo[0], p.hi[0]);
-      const bool interior = tile_in && i >= N + 1 && i < nx - N - 1 && xi < 0 &&
-                            !(force_here && i == p.si && p.sj >= j0 && p.sj < j0 + TY && p.sk >= k0 &&
-                              p.sk < k0 + G::TZ);
+      const int xi = SCH == SCH_CPML ? slab_index(i, nx, p.lo[0], p.hi[0]) : -1;
       if (jin && kin) {
         const float* pxx[2 * N];
         const float* pxy[2 * N];
@@ -439,7 +616,6 @@ k3s_velocity(const __grid_constant__ P3<float> p, const __grid_constant__ Staged
         const float* r0 = rho_p(i);
         const float* r1 = rho_p(i + 1);
         const size_t gi = (size_t)i * nyz + (size_t)j * nz + k;
-        const Vq<Q> rc = ldq<Q>(r0 + o_xx), rn = ldq<Q>(r0 + o_xx + G::TZ);
         // derivatives of the three components (Dx3fm/Dy3bm/Dz3bm etc.)
         Vq<Q> dv[9] = {dxq<N, EX, Q>(pxx, o_xx, cx),
                         dyq<N, false, EX, Q>(sxy_p(i), o_y, G::TZ, cy),
@@ -458,21 +634,105 @@ k3s_velocity(const __grid_constant__ P3<float> p, const __grid_constant__ Staged
         Vq<Q> a1 = dv[0], a2 = dv[1], a3 = dv[2], b1 = dv[3], b2 = dv[4], b3 = dv[5], c1 = dv[6], c2 = dv[7],
                c3 = dv[8];
         Vq<Q> vx = ldgq<Q>(p.f[0] + gi), vy = ldgq<Q>(p.f[1] + gi), vz = ldgq<Q>(p.f[2] + gi);
-        if (interior) {
-          const Vq<Q> r1c = ldq<Q>(r1 + o_xx), r1n = ldq<Q>(r1 + o_xx + G::TZ);
-          // numerators and densities of the 12 updates, then their quotients
-          // as one group (see div_group: no per-lane range branch)
-          float tn[3 * Q], td[3 * Q];
+        // update masks: vx i in [N, nx-N-1), vy and vz i in [N+1, nx-N)
+        const bool ix = i < nx - N - 1, iyz = i >= N + 1;
+        bool mx[Q], my[Q], mz[Q];
 #pragma unroll
-          for (int e = 0; e < Q; ++e) {
-            const float rce = g4(rc, e), rne = g4(rn, e);
-            tn[e] = (g4(a1, e) + g4(a3, e) + g4(a2, e)) * dt;
-            td[e] = rce;
-            tn[Q + e] = (g4(b1, e) + g4(b2, e) + g4(b3, e)) * dt;
-            td[Q + e] = 0.5f * (rce + rne);
-            const float sum = TENSOR ? (g4(c1, e) + g4(c2, e) + g4(c3, e)) : (g4(c3, e) + g4(c1, e) + g4(c2, e));
-            tn[2 * Q + e] = sum * dt;
-            td[2 * Q + e] = 0.25f * (rce + rne + g4(r1n, e) + g4(r1c, e));
+        for (int e = 0; e < Q; ++e) {
+          mx[e] = ix && jxz && kxy[e];
+          my[e] = iyz && jy && kxy[e];
+          mz[e] = iyz && jxz && kz[e];
+        }
+        const Vq<Q> rc = ldq<Q>(r0 + o_xx), rn = ldq<Q>(r0 + o_xx + G::TZ);
+        const Vq<Q> r1c = ldq<Q>(r1 + o_xx), r1n = ldq<Q>(r1 + o_xx + G::TZ);
+        if constexpr (SCH == SCH_SPML) {
+          spml_velocity<Q>(p, i, j, k, fy, fz, dt, mx, my, mz, a1, a2, a3, b1, b2, b3, c1, c2, c3, rc, rn, r1c, r1n,
+                           vx, vy, vz);
+        } else {
+          // CPML: components 0 (vx), 1 (vy), 2 (vz) of each axis; vx is at
+          // the x half point, vy at the y half point, vz at the z half point
+          if (xi >= 0) {
+            const float* cf = p.cf[0];
+            const float bi = __ldg(cf + CB * nx + i), ai = __ldg(cf + CA * nx + i), ki = __ldg(cf + CK * nx + i);
+            const float bh = __ldg(cf + CBH * nx + i), ah = __ldg(cf + CAH * nx + i),
+                        kh = __ldg(cf + CKH * nx + i);
+            float* m0 = p.mem[0] + ((size_t)xi * ny + j) * nz + k;
+            const long long mc = p.mcomp[0];
+            Vq<Q> s0 = ldq<Q>(m0), s1 = ldq<Q>(m0 + mc), s2 = ldq<Q>(m0 + 2 * mc);
+            cpml_pair<EX, Q>(a1, s0, mx, bh, ah, kh);
+            cpml_pair<EX, Q>(b1, s1, my, bi, ai, ki);
+            cpml_pair<EX, Q>(c1, s2, mz, bi, ai, ki);
+            stq<Q>(m0, s0);
+            stq<Q>(m0 + mc, s1);
+            stq<Q>(m0 + 2 * mc, s2);
+          }
+          if (yj >= 0) {
+            const float bi = tab(tyt, CB, TY, r), ai = tab(tyt, CA, TY, r), ki = tab(tyt, CK, TY, r);
+            const float bh = tab(tyt, CBH, TY, r), ah = tab(tyt, CAH, TY, r), kh = tab(tyt, CKH, TY, r);
+            float* m1 = p.mem[1] + ((size_t)i * p.sn[1] + yj) * nz + k;
+            const long long mc = p.mcomp[1];
+            Vq<Q> s0 = ldq<Q>(m1), s1 = ldq<Q>(m1 + mc), s2 = ldq<Q>(m1 + 2 * mc);
+            cpml_pair<EX, Q>(a2, s0, mx, bi, ai, ki);
+            cpml_pair<EX, Q>(b2, s1, my, bh, ah, kh);
+            cpml_pair<EX, Q>(c2, s2, mz, bi, ai, ki);
+            stq<Q>(m1, s0);
+            stq<Q>(m1 + mc, s1);
+            stq<Q>(m1 + 2 * mc, s2);
+          }
+          if (zany) {
+            float* m2 = p.mem[2] + ((size_t)i * ny + j) * p.sn[2];
+            const long long mc = p.mcomp[2];
+#pragma unroll
+            for (int e = 0; e < Q; ++e)
+              if (zk[e] >= 0) {
+                const int kk = Q * cq + e;
+                const float bi = tab(tzt, CB, G::TZ, kk), ai = tab(tzt, CA, G::TZ, kk),
+                            ki = tab(tzt, CK, G::TZ, kk);
+                const float bh = tab(tzt, CBH, G::TZ, kk), ah = tab(tzt, CAH, G::TZ, kk),
+                            kh = tab(tzt, CKH, G::TZ, kk);
+                float* q0 = m2 + zk[e];
+                if (mx[e]) {
+                  float d = g4(a3, e);
+                  *q0 = cpml1<EX>(d, *q0, bi, ai, ki);
+                  s4(a3, e, d);
+                }
+                if (my[e]) {
+                  float d = g4(b3, e);
+                  q0[mc] = cpml1<EX>(d, q0[mc], bi, ai, ki);
+                  s4(b3, e, d);
+                }
+                if (mz[e]) {
+                  float d = g4(c3, e);
+                  q0[2 * mc] = cpml1<EX>(d, q0[2 * mc], bh, ah, kh);
+                  s4(c3, e, d);
+                }
+              }
+          }
+          // numerators and densities of the 3Q updates, then their quotients
+          // as one group (no per-lane range branch); masked cells keep their value
+          float tn[3 * Q], td[3 * Q];
+          if constexpr (packed<EX, Q>()) {
+            const float2 dt2 = sp2(dt), rcn = add2(rc, rn);
+            const float2 n0 = mul2(add2(add2(a1, a3), a2), dt2);
+            const float2 n1 = mul2(add2(add2(b1, b2), b3), dt2);
+            const float2 n2 = mul2(TENSOR ? add2(add2(c1, c2), c3) : add2(add2(c3, c1), c2), dt2);
+            const float2 d1 = mul2(sp2(0.5f), rcn);
+            const float2 d2 = mul2(sp2(0.25f), add2(add2(rcn, r1n), r1c));
+            tn[0] = n0.x; tn[1] = n0.y; tn[2] = n1.x; tn[3] = n1.y; tn[4] = n2.x; tn[5] = n2.y;
+            td[0] = rc.x; td[1] = rc.y; td[2] = d1.x; td[3] = d1.y; td[4] = d2.x; td[5] = d2.y;
+          } else {
+#pragma unroll
+            for (int e = 0; e < Q; ++e) {
+              const float rce = g4(rc, e), rne = g4(rn, e);
+              tn[e] = (g4(a1, e) + g4(a3, e) + g4(a2, e)) * dt;
+              td[e] = rce;
+              tn[Q + e] = (g4(b1, e) + g4(b2, e) + g4(b3, e)) * dt;
+              td[Q + e] = 0.5f * (rce + rne);
+              const float sum =
+                  TENSOR ? (g4(c1, e) + g4(c2, e) + g4(c3, e)) : (g4(c3, e) + g4(c1, e) + g4(c2, e));
+              tn[2 * Q + e] = sum * dt;
+              td[2 * Q + e] = 0.25f * (rce + rne + g4(r1n, e) + g4(r1c, e));
+            }
           }
           if (EX) {
             bool okq = true;
@@ -491,87 +751,17 @@ k3s_velocity(const __grid_constant__ P3<float> p, const __grid_constant__ Staged
           }
 #pragma unroll
           for (int e = 0; e < Q; ++e) {
-            s4(vx, e, g4(vx, e) + tn[e]);
-            s4(vy, e, g4(vy, e) + tn[Q + e]);
-            s4(vz, e, g4(vz, e) + tn[2 * Q + e]);
+            if (mx[e]) s4(vx, e, g4(vx, e) + tn[e]);
+            if (my[e]) s4(vy, e, g4(vy, e) + tn[Q + e]);
+            if (mz[e]) s4(vz, e, g4(vz, e) + tn[2 * Q + e]);
           }
-        } else {
-          QuadPml q{xi, yj, i, j, k, p.fl[0][i], fy};
-          const bool anyslab = xi >= 0 || yj >= 0 || zslab;
-          QuadMem<Q> mm;
-          if (anyslab) quad_mem_load(p, q, 0, mm);
-          // vx (x half, y int, z int): i in [N, nx-N-1), j in [N+1, ny-N), k in [N+1, nz-N)
-          if (i < nx - N - 1 && j >= N + 1 && j < ny - N) {
-            int pm[Q], upd[Q];
-#pragma unroll
-            for (int e = 0; e < Q; ++e) {
-              upd[e] = k + e >= N + 1 && k + e < nz - N;
-              pm[e] = upd[e] && ((q.fx & 2) || (fy & 1) || (fz[e] & 1));
-            }
-            if (anyslab) {
-              pml_quad_m<0, EX, Q>(p, q, 0, 1, pm, a1, mm);
-              pml_quad_m<1, EX, Q>(p, q, 0, 0, pm, a2, mm);
-              pml_quad_m<2, EX, Q>(p, q, 0, 0, pm, a3, mm);
-            }
-#pragma unroll
-            for (int e = 0; e < Q; ++e)
-              if (upd[e]) {
-                const float t = (g4(a1, e) + g4(a3, e) + g4(a2, e)) * dt;
-                s4(vx, e, g4(vx, e) + dvv<EX>(t, g4(rc, e)));
-              }
-          }
-          // vy (x int, y half, z int): i in [N+1, nx-N), j in [N, ny-N-1), k in [N+1, nz-N)
-          if (i >= N + 1 && j < ny - N - 1 && j >= N) {
-            int pm[Q], upd[Q];
-#pragma unroll
-            for (int e = 0; e < Q; ++e) {
-              upd[e] = k + e >= N + 1 && k + e < nz - N;
-              pm[e] = upd[e] && ((q.fx & 1) || (fy & 2) || (fz[e] & 1));
-            }
-            if (anyslab) {
-              pml_quad_m<0, EX, Q>(p, q, 1, 0, pm, b1, mm);
-              pml_quad_m<1, EX, Q>(p, q, 1, 1, pm, b2, mm);
-              pml_quad_m<2, EX, Q>(p, q, 1, 0, pm, b3, mm);
-            }
-#pragma unroll
-            for (int e = 0; e < Q; ++e)
-              if (upd[e]) {
-                const float rhy = 0.5f * (g4(rc, e) + g4(rn, e));
-                const float t = (g4(b1, e) + g4(b2, e) + g4(b3, e)) * dt;
-                s4(vy, e, g4(vy, e) + dvv<EX>(t, rhy));
-              }
-          }
-          // vz (x int, y int, z half): i in [N+1, nx-N), j in [N+1, ny-N), k in [N, nz-N-1)
-          if (i >= N + 1 && j >= N + 1 && j < ny - N) {
-            const Vq<Q> r1c = ldq<Q>(r1 + o_xx), r1n = ldq<Q>(r1 + o_xx + G::TZ);
-            int pm[Q], upd[Q];
-#pragma unroll
-            for (int e = 0; e < Q; ++e) {
-              upd[e] = k + e >= N && k + e < nz - N - 1;
-              pm[e] = upd[e] && ((q.fx & 1) || (fy & 1) || (fz[e] & 2));
-            }
-            if (anyslab) {
-              pml_quad_m<0, EX, Q>(p, q, 2, 0, pm, c1, mm);
-              pml_quad_m<1, EX, Q>(p, q, 2, 0, pm, c2, mm);
-              pml_quad_m<2, EX, Q>(p, q, 2, 1, pm, c3, mm);
-            }
-#pragma unroll
-            for (int e = 0; e < Q; ++e)
-              if (upd[e]) {
-                const float r4 = 0.25f * (g4(rc, e) + g4(rn, e) + g4(r1n, e) + g4(r1c, e));
-                const float sum =
-                    TENSOR ? (g4(c1, e) + g4(c2, e) + g4(c3, e)) : (g4(c3, e) + g4(c1, e) + g4(c2, e));
-                const float t = sum * dt;
-                s4(vz, e, g4(vz, e) + dvv<EX>(t, r4));
-              }
-          }
-          if (anyslab) quad_mem_store(p, q, 0, mm);
-          // point force (Elastic3D_SSG_CPML.py:245), after the update
-          if (force_here && i == p.si && j == p.sj && p.sk >= k && p.sk < k + Q) {
-            const int e = p.sk - k;
-            const float t = dt * wf;
-            s4(vz, e, g4(vz, e) + dvv<EX>(t, g4(rc, e)));
-          }
+        }
+        // point force (Elastic3D_SSG_CPML.py:245, Elastic3D_SSG_SPML.py:294),
+        // after the update
+        if (force_here && i == p.si && j == p.sj && p.sk >= k && p.sk < k + Q) {
+          const int e = p.sk - k;
+          const float t = dt * wf;
+          s4(vz, e, g4(vz, e) + dvv<EX>(t, g4(rc, e)));
         }
         stq<Q>(p.f[0] + gi, vx);
         stq<Q>(p.f[1] + gi, vy);
@@ -588,13 +778,15 @@ k3s_velocity(const __grid_constant__ P3<float> p, const __grid_constant__ Staged
 // ---------------------------------------------------------------------------
 // stress pass
 // ---------------------------------------------------------------------------
-template <int N, int TY, int D, bool EX, int Q>
-__global__ void __launch_bounds__(SG<N, TY, D, Q>::NT, SG<N, TY, D, Q>::MINB_S)
+template <int N, int TY, int D, bool EX, int Q, int TZ, int SCH>
+__global__ void __launch_bounds__(SG<N, TY, D, Q, TZ>::NT, SG<N, TY, D, Q, TZ>::MINB_S)
 k3s_stress(const __grid_constant__ P3<float> p, const __grid_constant__ StagedMaps maps,
            const __grid_constant__ StagedArgs a, int it, int inject_next, int gather) {
-  using G = SG<N, TY, D, Q>;
+  using G = SG<N, TY, D, Q, TZ>;
   extern __shared__ __align__(128) float sm[];
   uint64_t* bars = reinterpret_cast<uint64_t*>(sm + G::S_FLOATS);
+  float* tyt = sm + G::S_TAB;   // [6][TY]
+  float* tzt = tyt + 6 * TY;    // [6][TZ]
   const int tid = threadIdx.x;
   const int nx = p.nx, ny = p.ny, nz = p.nz;
   const size_t nyz = (size_t)ny * nz;
@@ -641,19 +833,31 @@ k3s_stress(const __grid_constant__ P3<float> p, const __grid_constant__ StagedMa
     const int j0 = tyi * TY, k0 = tzi * G::TZ;
     const int x0 = max(ch * a.chunk_len, N), x1 = min((ch + 1) * a.chunk_len, nx - N);
     if (x0 >= x1) continue;
+    if (SCH == SCH_CPML) fill_tables<TY, G::TZ, G::NT>(p, tyt, tzt, j0, k0, tid);
     const int j = j0 + r, k = k0 + Q * cq;
     const bool jin = j < ny, kin = k < nz;
-    const bool tile_in = j0 >= N + 1 && j0 + TY <= ny - N - 1 && k0 >= N + 1 && k0 + G::TZ <= nz - N - 1 &&
-                         j0 >= p.lo[1] && j0 + TY <= ny - p.hi[1] && k0 >= p.lo[2] && k0 + G::TZ <= nz - p.hi[2];
-    const int yj = jin ? slab_index(j, ny, p.lo[1], p.hi[1]) : -1;
-    const uint8_t fy = jin ? p.fl[1][j] : 0;
-    bool zslab = false;
-    uint8_t fz[Q];
+    const int yj = SCH == SCH_CPML && jin ? slab_index(j, ny, p.lo[1], p.hi[1]) : -1;
+    int zk[Q];
+    bool zany = false;
 #pragma unroll
     for (int e = 0; e < Q; ++e) {
-      const int kk = k + e;
-      fz[e] = kk < nz ? p.fl[2][kk] : 0;
-      zslab = zslab || (kk < nz && slab_index(kk, nz, p.lo[2], p.hi[2]) >= 0);
+      zk[e] = SCH == SCH_CPML && k + e < nz ? slab_index(k + e, nz, p.lo[2], p.hi[2]) : -1;
+      zany = zany || zk[e] >= 0;
+    }
+    // update ranges in y and z (Elastic3D_SSG_Tensor.py:247,267,281,295):
+    // normal stresses j, k in [N+1, n-N); sxy j in [N+1, ny-N), k in [N, nz-N);
+    // sxz j in [N, ny-N), k in [N, nz-N-1); syz j in [N, ny-N-1), k in [N, nz-N-1)
+    const bool jn = j >= N + 1 && j < ny - N, jxz = j >= N && j < ny - N, jyz = j >= N && j < ny - N - 1;
+    const uint8_t fy = SCH == SCH_SPML && jin ? p.fl[1][j] : 0;
+    uint8_t fz[Q];
+#pragma unroll
+    for (int e = 0; e < Q; ++e) fz[e] = SCH == SCH_SPML && k + e < nz ? p.fl[2][k + e] : 0;
+    bool kn[Q], kxy[Q], kh[Q];
+#pragma unroll
+    for (int e = 0; e < Q; ++e) {
+      kn[e] = k + e >= N + 1 && k + e < nz - N;
+      kxy[e] = k + e >= N && k + e < nz - N;
+      kh[e] = k + e >= N && k + e < nz - N - 1;
     }
 
     auto issue = [&](int s, bool first, uint32_t stage) {
@@ -688,11 +892,8 @@ k3s_stress(const __grid_constant__ P3<float> p, const __grid_constant__ StagedMa
         ok = false;
         break;
       }
-      const int xi = slab_index(i, nx, p.lo[0], p.hi[0]);
+      const int xi = SCH == SCH_CPML ? slab_index(i, nx, p.lo[0], p.hi[0]) : -1;
       const bool src = inject_next && i == p.si && p.sj == j && p.sk >= k && p.sk < k + Q;
-      const bool interior = tile_in && i >= N + 1 && i < nx - N - 1 && xi < 0 &&
-                            !(inject_next && i == p.si && p.sj >= j0 && p.sj < j0 + TY && p.sk >= k0 &&
-                              p.sk < k0 + G::TZ);
       if (jin && kin) {
         const float* pvx[2 * N];  // vx planes i-N .. i+N-1  (Dx3bm)
         const float* pvy[2 * N];  // vy planes i-N+1 .. i+N  (Dx3fm)
@@ -707,15 +908,6 @@ k3s_stress(const __grid_constant__ P3<float> p, const __grid_constant__ StagedMa
         const float* vyi = vy_p(i);
         const float* vzi = vz_p(i);
         const size_t gi = (size_t)i * nyz + (size_t)j * nz + k;
-        Vq<Q> sxx = ldgq<Q>(p.f[3] + gi), syy = ldgq<Q>(p.f[4] + gi), szz = ldgq<Q>(p.f[5] + gi);
-        Vq<Q> sxy = ldgq<Q>(p.f[6] + gi), sxz = ldgq<Q>(p.f[7] + gi), syz = ldgq<Q>(p.f[8] + gi);
-        const Vq<Q> l0 = ldq<Q>(lam_p(i) + o_l), l1 = ldq<Q>(lam_p(i + 1) + o_l);
-        const float* m0p = mu_p(i);
-        const Vq<Q> u0 = ldq<Q>(m0p + o_m), u1 = ldq<Q>(mu_p(i + 1) + o_m), unj = ldq<Q>(m0p + o_m + G::WM);
-        float unk[Q];  // mu[k+1 .. k+Q] for the k+1 neighbours
-#pragma unroll
-        for (int e = 0; e + 1 < Q; ++e) unk[e] = g4(u0, e + 1);
-        unk[Q - 1] = m0p[o_m + Q];
         // derivatives: dvx/dx dvy/dy dvz/dz dvy/dx dvx/dy dvz/dx dvx/dz dvz/dy dvy/dz
         Vq<Q> dv[9] = {dxq<N, EX, Q>(pvx, o_v, cx),
                         dyq<N, false, EX, Q>(vyi, o_v, G::WZ, cy),
@@ -733,125 +925,151 @@ k3s_stress(const __grid_constant__ P3<float> p, const __grid_constant__ StagedMa
         }
         Vq<Q> e1 = dv[0], e2 = dv[1], e3 = dv[2], f1 = dv[3], f2 = dv[4], h1 = dv[5], h2 = dv[6], q1 = dv[7],
                q2 = dv[8];
-        if (interior) {
+        Vq<Q> sxx = ldgq<Q>(p.f[3] + gi), syy = ldgq<Q>(p.f[4] + gi), szz = ldgq<Q>(p.f[5] + gi);
+        Vq<Q> sxy = ldgq<Q>(p.f[6] + gi), sxz = ldgq<Q>(p.f[7] + gi), syz = ldgq<Q>(p.f[8] + gi);
+        // update masks: normal stresses and sxy i in [N+1, nx-N), sxz i in
+        // [N, nx-N-1), syz every plane of the loop
+        const bool in_ = i >= N + 1, ixz = i < nx - N - 1;
+        bool mn[Q], mxy[Q], mxz[Q], myz[Q];
 #pragma unroll
-          for (int e = 0; e < Q; ++e) {
-            const float lhx = 0.5f * (g4(l0, e) + g4(l1, e));
-            const float mhx = 0.5f * (g4(u0, e) + g4(u1, e));
-            const float lpm = lhx + 2.0f * mhx;
-            const float A = g4(e1, e), B = g4(e2, e), Cc = g4(e3, e);
-            s4(sxx, e, g4(sxx, e) + (lpm * A + lhx * (Cc + B)) * dt);
-            s4(syy, e, g4(syy, e) + (lpm * B + lhx * (A + Cc)) * dt);
-            s4(szz, e, g4(szz, e) + (lpm * Cc + lhx * (A + B)) * dt);
-            const float u = g4(u0, e);
-            const float mxy = 0.25f * (g4(unj, e) + u + u + g4(u1, e));
-            s4(sxy, e, g4(sxy, e) + mxy * (g4(f2, e) + g4(f1, e)) * dt);
-            const float mxz = 0.25f * (u + g4(u1, e) + u + g4(unj, e));
-            s4(sxz, e, g4(sxz, e) + mxz * (g4(h2, e) + g4(h1, e)) * dt);
-            const float myz = 0.25f * (g4(unj, e) + u + unk[e] + u);
-            s4(syz, e, g4(syz, e) + myz * (g4(q1, e) + g4(q2, e)) * dt);
-          }
+        for (int e = 0; e < Q; ++e) {
+          mn[e] = in_ && jn && kn[e];
+          mxy[e] = in_ && jn && kxy[e];
+          mxz[e] = ixz && jxz && kh[e];
+          myz[e] = jyz && kh[e];
+        }
+        const Vq<Q> l0 = ldq<Q>(lam_p(i) + o_l), l1 = ldq<Q>(lam_p(i + 1) + o_l);
+        const float* m0p = mu_p(i);
+        const Vq<Q> u0 = ldq<Q>(m0p + o_m), u1 = ldq<Q>(mu_p(i + 1) + o_m), unj = ldq<Q>(m0p + o_m + G::WM);
+        float unk[Q];  // mu[k+1 .. k+Q] for the k+1 neighbours
+#pragma unroll
+        for (int e = 0; e + 1 < Q; ++e) unk[e] = g4(u0, e + 1);
+        unk[Q - 1] = m0p[o_m + Q];
+        if constexpr (SCH == SCH_SPML) {
+          spml_stress<Q>(p, i, j, k, fy, fz, dt, mn, mxy, mxz, myz, e1, e2, e3, f1, f2, h1, h2, q1, q2, l0, u0, u1,
+                         unj, unk, sxx, syy, szz, sxy, sxz, syz);
         } else {
-          QuadPml q{xi, yj, i, j, k, p.fl[0][i], fy};
-          const bool anyslab = xi >= 0 || yj >= 0 || zslab;
-          QuadMem<Q> mm;
-          if (anyslab) quad_mem_load(p, q, 3, mm);
-          // normal stresses: i, j, k in [N+1, n-N)
-          if (i >= N + 1 && j >= N + 1 && j < ny - N) {
-            int pm[Q], upd[Q];
-#pragma unroll
-            for (int e = 0; e < Q; ++e) {
-              upd[e] = k + e >= N + 1 && k + e < nz - N;
-              pm[e] = upd[e] && ((q.fx | fy | fz[e]) & 1);
-            }
-            if (anyslab) {
-              pml_quad_m<0, EX, Q>(p, q, 0, 0, pm, e1, mm);
-              pml_quad_m<1, EX, Q>(p, q, 0, 0, pm, e2, mm);
-              pml_quad_m<2, EX, Q>(p, q, 0, 0, pm, e3, mm);
-            }
+          // CPML: components 3 (normal), 4, 5 of each axis
+          if (xi >= 0) {
+            const float* cf = p.cf[0];
+            const float bi = __ldg(cf + CB * nx + i), ai = __ldg(cf + CA * nx + i), ki = __ldg(cf + CK * nx + i);
+            const float bh = __ldg(cf + CBH * nx + i), ah = __ldg(cf + CAH * nx + i),
+                        khx = __ldg(cf + CKH * nx + i);
+            const long long mc = p.mcomp[0];
+            float* m0 = p.mem[0] + 3 * mc + ((size_t)xi * ny + j) * nz + k;
+            Vq<Q> s0 = ldq<Q>(m0), s1 = ldq<Q>(m0 + mc), s2 = ldq<Q>(m0 + 2 * mc);
+            cpml_pair<EX, Q>(e1, s0, mn, bi, ai, ki);    // dvx_dx
+            cpml_pair<EX, Q>(f1, s1, mxy, bh, ah, khx);  // dvy_dx
+            cpml_pair<EX, Q>(h1, s2, mxz, bh, ah, khx);  // dvz_dx
+            stq<Q>(m0, s0);
+            stq<Q>(m0 + mc, s1);
+            stq<Q>(m0 + 2 * mc, s2);
+          }
+          if (yj >= 0) {
+            const float bi = tab(tyt, CB, TY, r), ai = tab(tyt, CA, TY, r), ki = tab(tyt, CK, TY, r);
+            const float bh = tab(tyt, CBH, TY, r), ah = tab(tyt, CAH, TY, r), khy = tab(tyt, CKH, TY, r);
+            const long long mc = p.mcomp[1];
+            float* m1 = p.mem[1] + 3 * mc + ((size_t)i * p.sn[1] + yj) * nz + k;
+            Vq<Q> s0 = ldq<Q>(m1), s1 = ldq<Q>(m1 + mc), s2 = ldq<Q>(m1 + 2 * mc);
+            cpml_pair<EX, Q>(e2, s0, mn, bi, ai, ki);    // dvy_dy
+            cpml_pair<EX, Q>(f2, s1, mxy, bh, ah, khy);  // dvx_dy
+            cpml_pair<EX, Q>(q1, s2, myz, bh, ah, khy);  // dvz_dy
+            stq<Q>(m1, s0);
+            stq<Q>(m1 + mc, s1);
+            stq<Q>(m1 + 2 * mc, s2);
+          }
+          if (zany) {
+            const long long mc = p.mcomp[2];
+            float* m2 = p.mem[2] + 3 * mc + ((size_t)i * ny + j) * p.sn[2];
 #pragma unroll
             for (int e = 0; e < Q; ++e)
-              if (upd[e]) {
+              if (zk[e] >= 0) {
+                const int kk = Q * cq + e;
+                const float bi = tab(tzt, CB, G::TZ, kk), ai = tab(tzt, CA, G::TZ, kk),
+                            ki = tab(tzt, CK, G::TZ, kk);
+                const float bh = tab(tzt, CBH, G::TZ, kk), ah = tab(tzt, CAH, G::TZ, kk),
+                            khz = tab(tzt, CKH, G::TZ, kk);
+                float* q0 = m2 + zk[e];
+                if (mn[e]) {  // dvz_dz
+                  float d = g4(e3, e);
+                  *q0 = cpml1<EX>(d, *q0, bi, ai, ki);
+                  s4(e3, e, d);
+                }
+                if (mxz[e]) {  // dvx_dz
+                  float d = g4(h2, e);
+                  q0[mc] = cpml1<EX>(d, q0[mc], bh, ah, khz);
+                  s4(h2, e, d);
+                }
+                if (myz[e]) {  // dvy_dz
+                  float d = g4(q2, e);
+                  q0[2 * mc] = cpml1<EX>(d, q0[2 * mc], bh, ah, khz);
+                  s4(q2, e, d);
+                }
+              }
+          }
+          if constexpr (packed<EX, Q>()) {
+            const float2 dt2 = sp2(dt), half = sp2(0.5f), quarter = sp2(0.25f);
+            const float2 lhx = mul2(half, add2(l0, l1));
+            const float2 mhx = mul2(half, add2(u0, u1));
+            const float2 lpm = add2(lhx, mul2(sp2(2.0f), mhx));
+            const float2 nxx = add2(sxx, mul2(add2(mul2(lpm, e1), mul2(lhx, add2(e3, e2))), dt2));
+            const float2 nyy = add2(syy, mul2(add2(mul2(lpm, e2), mul2(lhx, add2(e1, e3))), dt2));
+            const float2 nzz = add2(szz, mul2(add2(mul2(lpm, e3), mul2(lhx, add2(e1, e2))), dt2));
+            const float2 uu = add2(unj, u0);
+            const float2 mxy4 = mul2(quarter, add2(add2(uu, u0), u1));
+            const float2 nxy = add2(sxy, mul2(mul2(mxy4, add2(f2, f1)), dt2));
+            const float2 mxz4 = mul2(quarter, add2(add2(add2(u0, u1), u0), unj));
+            const float2 nxz = add2(sxz, mul2(mul2(mxz4, add2(h2, h1)), dt2));
+            const float2 myz4 = mul2(quarter, add2(add2(uu, make_float2(unk[0], unk[1])), u0));
+            const float2 nyz = add2(syz, mul2(mul2(myz4, add2(q1, q2)), dt2));
+#pragma unroll
+            for (int e = 0; e < Q; ++e) {
+              if (mn[e]) {
+                s4(sxx, e, g4(nxx, e));
+                s4(syy, e, g4(nyy, e));
+                s4(szz, e, g4(nzz, e));
+              }
+              if (mxy[e]) s4(sxy, e, g4(nxy, e));
+              if (mxz[e]) s4(sxz, e, g4(nxz, e));
+              if (myz[e]) s4(syz, e, g4(nyz, e));
+            }
+          } else {
+#pragma unroll
+            for (int e = 0; e < Q; ++e) {
+              const float u = g4(u0, e);
+              if (mn[e]) {
                 const float lhx = 0.5f * (g4(l0, e) + g4(l1, e));
-                const float mhx = 0.5f * (g4(u0, e) + g4(u1, e));
+                const float mhx = 0.5f * (u + g4(u1, e));
                 const float lpm = lhx + 2.0f * mhx;
                 const float A = g4(e1, e), B = g4(e2, e), Cc = g4(e3, e);
                 s4(sxx, e, g4(sxx, e) + (lpm * A + lhx * (Cc + B)) * dt);
                 s4(syy, e, g4(syy, e) + (lpm * B + lhx * (A + Cc)) * dt);
                 s4(szz, e, g4(szz, e) + (lpm * Cc + lhx * (A + B)) * dt);
               }
-          }
-          // sxy (x half, y half, z int): i, j in [N+1, n-N), k in [N, nz-N)
-          if (i >= N + 1 && j >= N + 1 && j < ny - N) {
-            int pm[Q], upd[Q];
-#pragma unroll
-            for (int e = 0; e < Q; ++e) {
-              upd[e] = k + e >= N && k + e < nz - N;
-              pm[e] = upd[e] && ((q.fx & 2) || (fy & 2) || (fz[e] & 1));
-            }
-            if (anyslab) {
-              pml_quad_m<0, EX, Q>(p, q, 1, 1, pm, f1, mm);
-              pml_quad_m<1, EX, Q>(p, q, 1, 1, pm, f2, mm);
-            }
-#pragma unroll
-            for (int e = 0; e < Q; ++e)
-              if (upd[e]) {
-                const float u = g4(u0, e);
+              if (mxy[e]) {
                 const float m4 = 0.25f * (g4(unj, e) + u + u + g4(u1, e));
                 s4(sxy, e, g4(sxy, e) + m4 * (g4(f2, e) + g4(f1, e)) * dt);
               }
-          }
-          // sxz (x half, y int, z half): i in [N, nx-N-1), j in [N, ny-N), k in [N, nz-N-1)
-          if (i < nx - N - 1 && j >= N && j < ny - N) {
-            int pm[Q], upd[Q];
-#pragma unroll
-            for (int e = 0; e < Q; ++e) {
-              upd[e] = k + e >= N && k + e < nz - N - 1;
-              pm[e] = upd[e] && ((q.fx & 2) || (fy & 1) || (fz[e] & 2));
-            }
-            if (anyslab) {
-              pml_quad_m<0, EX, Q>(p, q, 2, 1, pm, h1, mm);
-              pml_quad_m<2, EX, Q>(p, q, 1, 1, pm, h2, mm);
-            }
-#pragma unroll
-            for (int e = 0; e < Q; ++e)
-              if (upd[e]) {
-                const float u = g4(u0, e);
+              if (mxz[e]) {
                 const float m4 = 0.25f * (u + g4(u1, e) + u + g4(unj, e));
                 s4(sxz, e, g4(sxz, e) + m4 * (g4(h2, e) + g4(h1, e)) * dt);
               }
-          }
-          // syz (x int, y half, z half): i in [N, nx-N), j in [N, ny-N-1), k in [N, nz-N-1)
-          if (j >= N && j < ny - N - 1) {
-            int pm[Q], upd[Q];
-#pragma unroll
-            for (int e = 0; e < Q; ++e) {
-              upd[e] = k + e >= N && k + e < nz - N - 1;
-              pm[e] = upd[e] && ((q.fx & 1) || (fy & 2) || (fz[e] & 2));
-            }
-            if (anyslab) {
-              pml_quad_m<1, EX, Q>(p, q, 2, 1, pm, q1, mm);
-              pml_quad_m<2, EX, Q>(p, q, 2, 1, pm, q2, mm);
-            }
-#pragma unroll
-            for (int e = 0; e < Q; ++e)
-              if (upd[e]) {
-                const float u = g4(u0, e);
+              if (myz[e]) {
                 const float m4 = 0.25f * (g4(unj, e) + u + unk[e] + u);
                 s4(syz, e, g4(syz, e) + m4 * (g4(q1, e) + g4(q2, e)) * dt);
               }
+            }
           }
-          if (anyslab) quad_mem_store(p, q, 3, mm);
-          if (src) {
-            // next step's moment-tensor source (Elastic3D_SSG_Tensor.py:186-193)
-            const int e = p.sk - k;
-            s4(sxx, e, g4(sxx, e) + wn * p.mneg[0]);
-            s4(syy, e, g4(syy, e) + wn * p.mneg[1]);
-            s4(szz, e, g4(szz, e) + wn * p.mneg[2]);
-            s4(sxy, e, g4(sxy, e) + wn * p.mneg[3]);
-            s4(sxz, e, g4(sxz, e) + wn * p.mneg[4]);
-            s4(syz, e, g4(syz, e) + wn * p.mneg[5]);
-          }
+        }
+        if (src) {
+          // next step's moment-tensor source (Elastic3D_SSG_Tensor.py:186-193)
+          const int e = p.sk - k;
+          s4(sxx, e, g4(sxx, e) + wn * p.mneg[0]);
+          s4(syy, e, g4(syy, e) + wn * p.mneg[1]);
+          s4(szz, e, g4(szz, e) + wn * p.mneg[2]);
+          s4(sxy, e, g4(sxy, e) + wn * p.mneg[3]);
+          s4(sxz, e, g4(sxz, e) + wn * p.mneg[4]);
+          s4(syz, e, g4(syz, e) + wn * p.mneg[5]);
         }
         stq<Q>(p.f[3] + gi, sxx);
         stq<Q>(p.f[4] + gi, syy);
@@ -895,9 +1113,9 @@ static bool map3(CUtensorMap* m, const void* base, int nx, int ny, int nz, int b
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-template <int N, int TY, int D>
+template <int N, int TY, int D, int TZ>
 static bool staged_maps_t(const P3<float>& p, StagedMaps* vm, StagedMaps* sm_) {
-  using G = SG<N, TY, D, 4>;  // box shapes do not depend on the cells per thread
+  using G = SG<N, TY, D, 4, TZ>;  // box shapes do not depend on the cells per thread
   const int nx = p.nx, ny = p.ny, nz = p.nz;
   bool ok = true;
   // velocity pass: sxx sxy sxz syy syz szz rho
@@ -917,77 +1135,138 @@ static bool staged_maps_t(const P3<float>& p, StagedMaps* vm, StagedMaps* sm_) {
   return ok;
 }
 
-template <int N, int TY, int D>
+template <int N, int TY, int D, int TZ>
 static StagedConfig staged_cfg_t() {
-  using G = SG<N, TY, D, staged_q(true)>;
-  return StagedConfig{N, TY, D, G::NT, G::V_BYTES, G::S_BYTES};
+  using G = SG<N, TY, D, staged_q(true), TZ>;
+  return StagedConfig{N, TY, D, TZ, G::NT, G::V_BYTES, G::S_BYTES};
 }
 
-bool sw3_staged_config(int N, StagedConfig* out) {
-  switch (N) {
-    case 1: *out = staged_cfg_t<1, 16, 2>(); return true;
-    case 2: *out = staged_cfg_t<2, 16, 1>(); return true;
-    case 3: *out = staged_cfg_t<3, 16, 2>(); return true;
-    case 4: *out = staged_cfg_t<4, 16, 1>(); return true;
-    default: return false;
+// tile shapes per order: (TY, D); TZ is 32 or 40
+#define SW_STAGED_SWITCH(N_, TZ_, CALL)                         \
+  switch ((N_) * 100 + (TZ_)) {                                 \
+    case 132: CALL(1, 16, 2, 32) case 140: CALL(1, 16, 2, 40)   \
+    case 232: CALL(2, 16, 1, 32) case 240: CALL(2, 16, 1, 40)   \
+    case 332: CALL(3, 16, 2, 32) case 340: CALL(3, 16, 2, 40)   \
+    case 432: CALL(4, 16, 1, 32) case 440: CALL(4, 16, 1, 40)   \
+    default: break;                                             \
   }
-}
 
-bool sw3_staged_maps(int N, const P3<float>& p, StagedMaps* vm, StagedMaps* sm_) {
-  switch (N) {
-    case 1: return staged_maps_t<1, 16, 2>(p, vm, sm_);
-    case 2: return staged_maps_t<2, 16, 1>(p, vm, sm_);
-    case 3: return staged_maps_t<3, 16, 2>(p, vm, sm_);
-    case 4: return staged_maps_t<4, 16, 1>(p, vm, sm_);
-    default: return false;
+bool sw3_staged_config(int N, int tz, StagedConfig* out) {
+#define SW_CFG(a, b, c, d)           \
+  {                                  \
+    *out = staged_cfg_t<a, b, c, d>(); \
+    return true;                     \
   }
+  SW_STAGED_SWITCH(N, tz, SW_CFG)
+#undef SW_CFG
+  return false;
 }
 
-template <int N, int TY, int D, bool EX>
-static cudaError_t staged_launch(bool tensor, const P3<float>& p, const StagedMaps& vm, const StagedMaps& smp,
-                                 const StagedArgs& a, int grid, int it, bool force_here, bool inject_next,
-                                 bool gather, cudaStream_t st) {
+bool sw3_staged_maps(int N, int tz, const P3<float>& p, StagedMaps* vm, StagedMaps* sm_) {
+#define SW_MAPS(a, b, c, d) \
+  { return staged_maps_t<a, b, c, d>(p, vm, sm_); }
+  SW_STAGED_SWITCH(N, tz, SW_MAPS)
+#undef SW_MAPS
+  return false;
+}
+
+// Resident CTAs per SM of each pass (registers, shared memory and threads
+// together), queried once per device; each pass is launched with that many
+// CTAs per SM (at most one per work unit), so the persistent unit loop runs
+// in one wave.
+struct StagedOcc {
+  int vel = 0, str = 0, sms = 0;
+};
+
+template <int N, int TY, int D, int TZ, bool EX, int SCH>
+static cudaError_t staged_setup(bool tensor, StagedOcc* occ) {
   constexpr int Q = staged_q(EX);
-  using G = SG<N, TY, D, Q>;
+  using G = SG<N, TY, D, Q, TZ>;
   static std::atomic<unsigned long long> done{0};
   static std::mutex mu;
-  cudaError_t e0 = once_per_device(done, mu, [] {
-    cudaError_t e = cudaFuncSetAttribute(k3s_velocity<N, TY, D, true, EX, Q>,
+  static StagedOcc per_dev[64][2];
+  int dev = 0;
+  cudaError_t e0 = cudaGetDevice(&dev);
+  if (e0 != cudaSuccess) return e0;
+  e0 = once_per_device(done, mu, [dev] {
+    cudaError_t e = cudaFuncSetAttribute(k3s_velocity<N, TY, D, false, EX, Q, TZ, SCH>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::V_BYTES);
     if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(k3s_velocity<N, TY, D, false, EX, Q>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)G::V_BYTES);
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(k3s_stress<N, TY, D, EX, Q>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      e = cudaFuncSetAttribute(k3s_stress<N, TY, D, EX, Q, TZ, SCH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)G::S_BYTES);
+    StagedOcc& o0 = per_dev[dev & 63][0];
+    if (e == cudaSuccess)
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o0.vel, k3s_velocity<N, TY, D, false, EX, Q, TZ, SCH>,
+                                                        G::NT, G::V_BYTES);
+    if constexpr (SCH == SCH_CPML) {
+      StagedOcc& o1 = per_dev[dev & 63][1];
+      if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k3s_velocity<N, TY, D, true, EX, Q, TZ, SCH>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::V_BYTES);
+      if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o1.vel, k3s_velocity<N, TY, D, true, EX, Q, TZ, SCH>,
+                                                          G::NT, G::V_BYTES);
+    }
+    int str = 0, sms = 0;
+    if (e == cudaSuccess)
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&str, k3s_stress<N, TY, D, EX, Q, TZ, SCH>, G::NT,
+                                                        G::S_BYTES);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    for (int t = 0; t < 2; ++t) {
+      StagedOcc& o = per_dev[dev & 63][t];
+      if (t == 1 && SCH != SCH_CPML) o.vel = per_dev[dev & 63][0].vel;
+      o.str = str;
+      o.sms = sms;
+      if (o.vel < 1) o.vel = 1;
+      if (o.str < 1) o.str = 1;
+    }
     return e;
   });
   if (e0 != cudaSuccess) return e0;
-  if (tensor) k3s_velocity<N, TY, D, true, EX, Q><<<grid, G::NT, G::V_BYTES, st>>>(p, vm, a, it, 0);
-  else k3s_velocity<N, TY, D, false, EX, Q><<<grid, G::NT, G::V_BYTES, st>>>(p, vm, a, it, force_here ? 1 : 0);
-  k3s_stress<N, TY, D, EX, Q><<<grid, G::NT, G::S_BYTES, st>>>(p, smp, a, it, inject_next ? 1 : 0, gather ? 1 : 0);
+  *occ = per_dev[dev & 63][tensor ? 1 : 0];
+  return cudaSuccess;
+}
+
+template <int N, int TY, int D, int TZ, bool EX, int SCH>
+static cudaError_t staged_launch(bool tensor, const P3<float>& p, const StagedMaps& vm, const StagedMaps& smp,
+                                 const StagedArgs& a, int it, bool force_here, bool inject_next, bool gather,
+                                 cudaStream_t st) {
+  constexpr int Q = staged_q(EX);
+  using G = SG<N, TY, D, Q, TZ>;
+  StagedOcc o;
+  cudaError_t e0 = staged_setup<N, TY, D, TZ, EX, SCH>(tensor, &o);
+  if (e0 != cudaSuccess) return e0;
+  const int units = a.tiles_y * a.tiles_z * a.chunks;
+  const int gv = units < o.sms * o.vel ? units : o.sms * o.vel;
+  const int gs = units < o.sms * o.str ? units : o.sms * o.str;
+  if constexpr (SCH == SCH_CPML) {
+    if (tensor) k3s_velocity<N, TY, D, true, EX, Q, TZ, SCH><<<gv, G::NT, G::V_BYTES, st>>>(p, vm, a, it, 0);
+    else
+      k3s_velocity<N, TY, D, false, EX, Q, TZ, SCH><<<gv, G::NT, G::V_BYTES, st>>>(p, vm, a, it, force_here ? 1 : 0);
+  } else {
+    k3s_velocity<N, TY, D, false, EX, Q, TZ, SCH><<<gv, G::NT, G::V_BYTES, st>>>(p, vm, a, it, force_here ? 1 : 0);
+  }
+  k3s_stress<N, TY, D, EX, Q, TZ, SCH><<<gs, G::NT, G::S_BYTES, st>>>(p, smp, a, it, inject_next ? 1 : 0,
+                                                                       gather ? 1 : 0);
   return cudaGetLastError();
 }
 
-template <int N, int TY, int D>
-static cudaError_t staged_step_t(bool tensor, const P3<float>& p, const StagedMaps& vm, const StagedMaps& smp,
-                                 const StagedArgs& a, int grid, int it, bool force_here, bool inject_next,
-                                 bool gather, cudaStream_t st) {
-  return a.exact ? staged_launch<N, TY, D, true>(tensor, p, vm, smp, a, grid, it, force_here, inject_next, gather, st)
-                 : staged_launch<N, TY, D, false>(tensor, p, vm, smp, a, grid, it, force_here, inject_next, gather,
-                                                  st);
-}
-
-cudaError_t sw3_staged_step(int N, bool tensor, const P3<float>& p, const StagedMaps& vm, const StagedMaps& smp,
-                            const StagedArgs& a, int grid, int it, bool force_here, bool inject_next, bool gather,
-                            cudaStream_t st) {
-  switch (N) {
-    case 1: return staged_step_t<1, 16, 2>(tensor, p, vm, smp, a, grid, it, force_here, inject_next, gather, st);
-    case 2: return staged_step_t<2, 16, 1>(tensor, p, vm, smp, a, grid, it, force_here, inject_next, gather, st);
-    case 3: return staged_step_t<3, 16, 2>(tensor, p, vm, smp, a, grid, it, force_here, inject_next, gather, st);
-    case 4: return staged_step_t<4, 16, 1>(tensor, p, vm, smp, a, grid, it, force_here, inject_next, gather, st);
-    default: return cudaErrorInvalidValue;
+cudaError_t sw3_staged_step(int N, int tz, bool spml, bool tensor, const P3<float>& p, const StagedMaps& vm,
+                            const StagedMaps& smp, const StagedArgs& a, int it, bool force_here, bool inject_next,
+                            bool gather, cudaStream_t st) {
+  // the split-field PML runs exact numerics only
+#define SW_STEP(a_, b, c, d)                                                                                     \
+  {                                                                                                              \
+    if (spml)                                                                                                    \
+      return staged_launch<a_, b, c, d, true, SCH_SPML>(false, p, vm, smp, a, it, force_here, false, gather, st); \
+    return a.exact ? staged_launch<a_, b, c, d, true, SCH_CPML>(tensor, p, vm, smp, a, it, force_here,            \
+                                                                inject_next, gather, st)                         \
+                   : staged_launch<a_, b, c, d, false, SCH_CPML>(tensor, p, vm, smp, a, it, force_here,           \
+                                                                 inject_next, gather, st);                       \
   }
+  SW_STAGED_SWITCH(N, tz, SW_STEP)
+#undef SW_STEP
+  return cudaErrorInvalidValue;
 }
 
 }  // namespace sw

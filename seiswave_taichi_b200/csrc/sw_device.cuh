@@ -41,6 +41,14 @@ __host__ __device__ __forceinline__ int slab_index(int i, int n, int lo, int hi)
 
 // coefficient table rows (sw_pml_axis.coef): 6 rows of n values
 enum { CB = 0, CA = 1, CK = 2, CBH = 3, CAH = 4, CKH = 5 };
+// split-PML fields, rows of P3::split in the reference's order
+// (vx_x .. szz_z, Elastic3D_SSG_SPML.py:107-138)
+enum {
+  PVX_X = 0, PVX_Y, PVX_Z, PVY_X, PVY_Y, PVY_Z, PVZ_X, PVZ_Y, PVZ_Z,
+  PSXX_X, PSXX_Y, PSXX_Z, PSYY_X, PSYY_Y, PSYY_Z,
+  PSXY_X, PSXY_Y, PSXZ_X, PSXZ_Z, PSYZ_Y, PSYZ_Z,
+  PSZZ_X, PSZZ_Y, PSZZ_Z
+};
 
 // 3D CPML memory-variable components, 6 per direction.
 //   x: 0 sxx_dx(vx) 1 sxy_dx(vy) 2 sxz_dx(vz) 3 dvx_dx(normal) 4 dvy_dx(sxy) 5 dvz_dx(sxz)

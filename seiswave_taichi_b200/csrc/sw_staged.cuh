@@ -19,16 +19,19 @@ struct StagedArgs {
   int exact;  // 1: IEEE-exact reference order (bit-identical to the CPU oracle)
 };
 
+// tile of TY rows x TZ z cells (TZ 32 or 40), D planes prefetched
 struct StagedConfig {
-  int N, TY, D, threads;
+  int N, TY, D, TZ, threads;
   size_t vel_smem, str_smem;
 };
 
-bool sw3_staged_config(int N, StagedConfig* out);
-bool sw3_staged_maps(int N, const P3<float>& p, StagedMaps* vel, StagedMaps* str);
-// velocity pass then stress pass of step it, in place
-cudaError_t sw3_staged_step(int N, bool tensor, const P3<float>& p, const StagedMaps& vel, const StagedMaps& str,
-                            const StagedArgs& a, int grid, int it, bool force_here, bool inject_next, bool gather,
-                            cudaStream_t st);
+bool sw3_staged_config(int N, int tz, StagedConfig* out);
+bool sw3_staged_maps(int N, int tz, const P3<float>& p, StagedMaps* vel, StagedMaps* str);
+// velocity pass then stress pass of step it, in place; spml: the
+// split-field PML scheme (exact numerics), else the CPML schemes.  Each pass
+// gets as many CTAs as fit on the device at once (at most one per work unit).
+cudaError_t sw3_staged_step(int N, int tz, bool spml, bool tensor, const P3<float>& p, const StagedMaps& vel,
+                            const StagedMaps& str, const StagedArgs& a, int it, bool force_here, bool inject_next,
+                            bool gather, cudaStream_t st);
 
 }  // namespace sw

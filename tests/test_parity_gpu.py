@@ -55,6 +55,10 @@ CASES3 = [
     dict(scheme="TENSOR", N=3, hetero=False, surface=(True, True, True, True, False, True)),
     dict(scheme="CPML", N=2),
     dict(scheme="CPML", N=4, shape=(42, 40, 38)),
+    # z extents whose staged tiles are 40 wide (nz=76: a partial last tile)
+    dict(scheme="TENSOR", N=2, shape=(36, 34, 76)),
+    dict(scheme="CPML", N=3, shape=(34, 38, 40)),
+    dict(scheme="SPML", N=2, shape=(36, 34, 80)),
     dict(scheme="SPML", N=2),
     dict(scheme="SPML", N=3, shape=(38, 42, 40)),
     dict(scheme="TENSOR", N=2, dtype=np.float64),
