@@ -5,6 +5,7 @@
 // then only enqueue kernels.  sw_run replays a cached CUDA graph of the whole
 // step sequence so the per-step launch cost of the reference's Python loop
 // (test2d_homegenous.py:55-56) disappears.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -1359,10 +1360,13 @@ struct sw_batch {
   int nshots = 0, scheme = 0, dtype = 0, order = 0, nt_max = 0;
   bool fold = true;                       // next-step moment source folded into the stress pass
   std::vector<sw_plan*> plans;            // per-shot validated plans
-  void* d_shots = nullptr;                // device P2<T>[nshots]
+  std::vector<char> shots;                // host P2<T>[nshots], passed to the kernels by value
   int2* d_work = nullptr;                 // device, per tile shape: one work item per block
   long long work_off[SW_BATCH_TILES] = {};
   int total[SW_BATCH_TILES] = {};
+  // per tile shape and group of SW_BATCH_GROUP shots: first work item and count
+  std::vector<long long> grp_off[SW_BATCH_TILES];
+  std::vector<int> grp_n[SW_BATCH_TILES];
   int cfg = 0;
   long long cells = 0;
   cudaStream_t cap_stream = nullptr;
@@ -1372,30 +1376,41 @@ struct sw_batch {
 
 namespace {
 
+// group g of the batch (shots g*SW_BATCH_GROUP ..) for the current tile shape
 template <typename T>
-sw::Batch2<T> batch_view(const sw_batch* b) {
-  return sw::Batch2<T>{(const sw::P2<T>*)b->d_shots, b->d_work + b->work_off[b->cfg], b->nshots};
+sw::Batch2<T> batch_group(const sw_batch* b, int g) {
+  sw::Batch2<T> v{};
+  v.first = g * SW_BATCH_GROUP;
+  v.n = std::min(SW_BATCH_GROUP, b->nshots - v.first);
+  memcpy(v.shots, b->shots.data() + sizeof(sw::P2<T>) * v.first, sizeof(sw::P2<T>) * v.n);
+  v.work = b->d_work + b->grp_off[b->cfg][g];
+  return v;
 }
 
-cudaError_t batch_sequence(sw_batch* b, int it0, int n, cudaStream_t st) {
+template <typename T>
+cudaError_t batch_sequence_t(sw_batch* b, int it0, int n, cudaStream_t st) {
+  const int groups = (b->nshots + SW_BATCH_GROUP - 1) / SW_BATCH_GROUP;
+  std::vector<sw::Batch2<T>> views;
+  for (int g = 0; g < groups; ++g) views.push_back(batch_group<T>(b, g));
   for (int s = 0; s < n; ++s) {
     const int it = it0 + s;
     const bool pre = s == 0 || !b->fold, nxt = b->fold && s != n - 1;
-    cudaError_t e = b->dtype == SW_F32
-                        ? sw::sw2b_step<float>(batch_view<float>(b), b->scheme, b->order, b->cfg, b->total[b->cfg],
-                                               it, pre, nxt, st)
-                        : sw::sw2b_step<double>(batch_view<double>(b), b->scheme, b->order, b->cfg,
-                                                b->total[b->cfg], it, pre, nxt, st);
-    if (e != cudaSuccess) return e;
+    for (int g = 0; g < groups; ++g) {
+      cudaError_t e = sw::sw2b_step<T>(views[g], b->scheme, b->order, b->cfg, b->grp_n[b->cfg][g], it, pre, nxt, st);
+      if (e != cudaSuccess) return e;
+    }
   }
   return cudaSuccess;
+}
+
+cudaError_t batch_sequence(sw_batch* b, int it0, int n, cudaStream_t st) {
+  return b->dtype == SW_F32 ? batch_sequence_t<float>(b, it0, n, st) : batch_sequence_t<double>(b, it0, n, st);
 }
 
 void batch_free(sw_batch* b) {
   if (!b) return;
   if (b->gexec) cudaGraphExecDestroy(b->gexec);
   if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
-  if (b->d_shots) cudaFree(b->d_shots);
   if (b->d_work) cudaFree(b->d_work);
   for (sw_plan* p : b->plans) sw_plan_destroy(p);
   delete b;
@@ -1437,10 +1452,10 @@ int sw2d_batch_create(const sw2d_desc* shots, int32_t nshots, sw_batch** out) {
     b->cells += (long long)d.nx * d.nz;
   }
   const size_t psz = b->dtype == SW_F32 ? sizeof(sw::P2<float>) : sizeof(sw::P2<double>);
-  std::vector<char> host(psz * nshots);
+  b->shots.resize(psz * nshots);
   for (int s = 0; s < nshots; ++s) {
-    if (b->dtype == SW_F32) memcpy(host.data() + psz * s, &b->plans[s]->p2f, psz);
-    else memcpy(host.data() + psz * s, &b->plans[s]->p2d, psz);
+    if (b->dtype == SW_F32) memcpy(b->shots.data() + psz * s, &b->plans[s]->p2f, psz);
+    else memcpy(b->shots.data() + psz * s, &b->plans[s]->p2d, psz);
   }
   // work items, shot by shot, tile rows (x) outer, tile columns (z) inner
   std::vector<int2> work;
@@ -1449,6 +1464,10 @@ int sw2d_batch_create(const sw2d_desc* shots, int32_t nshots, sw_batch** out) {
     sw::sw2b_tile_shape(c, &bx, &bz);
     b->work_off[c] = (long long)work.size();
     for (int s = 0; s < nshots; ++s) {
+      if (s % SW_BATCH_GROUP == 0) {
+        b->grp_off[c].push_back((long long)work.size());
+        b->grp_n[c].push_back(0);
+      }
       const int tx = (shots[s].nx + bx - 1) / bx, tz = (shots[s].nz + bz - 1) / bz;
       if (tx > 0xffff || tz > 0xffff) {
         batch_free(b);
@@ -1456,6 +1475,12 @@ int sw2d_batch_create(const sw2d_desc* shots, int32_t nshots, sw_batch** out) {
       }
       for (int x = 0; x < tx; ++x)
         for (int z = 0; z < tz; ++z) work.push_back(make_int2(s, (x << 16) | z));
+      const long long gn = (long long)work.size() - b->grp_off[c].back();
+      if (gn > 0x7fffffffLL) {
+        batch_free(b);
+        return fail(SW_ERR_ARG, "sw2d_batch_create: batch too large for one launch");
+      }
+      b->grp_n[c].back() = (int)gn;
     }
     const long long tot = (long long)work.size() - b->work_off[c];
     if (tot > 0x7fffffffLL) {
@@ -1464,9 +1489,7 @@ int sw2d_batch_create(const sw2d_desc* shots, int32_t nshots, sw_batch** out) {
     }
     b->total[c] = (int)tot;
   }
-  cudaError_t e = cudaMalloc(&b->d_shots, psz * nshots);
-  if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_work, work.size() * sizeof(int2));
-  if (e == cudaSuccess) e = cudaMemcpy(b->d_shots, host.data(), psz * nshots, cudaMemcpyHostToDevice);
+  cudaError_t e = cudaMalloc((void**)&b->d_work, work.size() * sizeof(int2));
   if (e == cudaSuccess) e = cudaMemcpy(b->d_work, work.data(), work.size() * sizeof(int2), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
     batch_free(b);

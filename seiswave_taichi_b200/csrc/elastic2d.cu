@@ -590,34 +590,19 @@ template cudaError_t sw2_persistent<double>(const P2<double>&, int, int, int, in
 // ---------------------------------------------------------------------------
 // batched ragged shots: one launch per phase covers every tile of every shot
 // ---------------------------------------------------------------------------
-// the block's shot parameter block, copied once into shared memory so that
-// every thread reads it from there instead of global memory
-template <typename T, int NT>
-__device__ __forceinline__ const P2<T>& stage_shot(const Batch2<T>& bt, int s, P2<T>* sp) {
-  static_assert(sizeof(P2<T>) % 4 == 0, "parameter block size");
-  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-  const uint32_t* src = reinterpret_cast<const uint32_t*>(bt.shots + s);
-  uint32_t* dst = reinterpret_cast<uint32_t*>(sp);
-  for (int q = tid; q < (int)(sizeof(P2<T>) / 4); q += NT) dst[q] = src[q];
-  __syncthreads();
-  return *sp;
-}
-
 template <typename T, int N, int S, int BX, int BZ>
-__global__ void __launch_bounds__(BX * BZ) k2b_velocity(Batch2<T> bt, int it) {
-  __shared__ P2<T> sp;
+__global__ void __launch_bounds__(BX * BZ) k2b_velocity(const __grid_constant__ Batch2<T> bt, int it) {
   const int2 wk = bt.work[blockIdx.x];
-  const P2<T>& p = stage_shot<T, BX * BZ>(bt, wk.x, &sp);
+  const P2<T>& p = bt.shots[wk.x - bt.first];
   const int j = (wk.y & 0xffff) * BZ + threadIdx.x, i = (wk.y >> 16) * BX + threadIdx.y;
   if (i >= p.nx || j >= p.nz) return;
   vel2_cell<T, N, S>(p, i, j, it, (T)0, p.src_kind == SW_SRC_FORCE ? 1 : 0);
 }
 
 template <typename T, int N, int S, int BX, int BZ>
-__global__ void __launch_bounds__(BX * BZ) k2b_stress(Batch2<T> bt, int it, int inject_next) {
-  __shared__ P2<T> sp;
+__global__ void __launch_bounds__(BX * BZ) k2b_stress(const __grid_constant__ Batch2<T> bt, int it, int inject_next) {
   const int2 wk = bt.work[blockIdx.x];
-  const P2<T>& p = stage_shot<T, BX * BZ>(bt, wk.x, &sp);
+  const P2<T>& p = bt.shots[wk.x - bt.first];
   const int tx = wk.y >> 16, tz = wk.y & 0xffff;
   {
     // receivers of the velocity fields: the shot's first tiles cover them
@@ -631,9 +616,9 @@ __global__ void __launch_bounds__(BX * BZ) k2b_stress(Batch2<T> bt, int it, int 
 }
 
 template <typename T>
-__global__ void k2b_inject(Batch2<T> bt, int it) {
+__global__ void k2b_inject(const __grid_constant__ Batch2<T> bt, int it) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= bt.nshots) return;
+  if (s >= bt.n) return;
   const P2<T>& p = bt.shots[s];
   if (p.src_kind != SW_SRC_MOMENT) return;
   const long long c = (long long)p.si * p.nz + p.sk;
@@ -648,7 +633,7 @@ constexpr int kBatchTiles[SW_BATCH_TILES][2] = {{8, 32}, {4, 32}, {16, 32}, {4, 
 
 template <typename T, int N, int S, int BX, int BZ>
 static cudaError_t launch2b(const Batch2<T>& bt, int total, int it, bool pre, bool nxt, cudaStream_t st) {
-  if (pre) k2b_inject<T><<<(bt.nshots + 127) / 128, 128, 0, st>>>(bt, it);
+  if (pre) k2b_inject<T><<<1, SW_BATCH_GROUP, 0, st>>>(bt, it);
   dim3 block(BZ, BX);
   k2b_velocity<T, N, S, BX, BZ><<<total, block, 0, st>>>(bt, it);
   k2b_stress<T, N, S, BX, BZ><<<total, block, 0, st>>>(bt, it, nxt ? 1 : 0);

@@ -112,15 +112,19 @@ struct P2 {
   T mneg[3];                // moment-tensor source: -M_xx, -M_zz, -M_xz
 };
 
-// a batch of 2D shots: per-shot parameter blocks in device memory and, for
-// the current tile shape, one work item per block: x = shot, y = tile row
-// (x direction) << 16 | tile column (z direction)
+// A group of at most SW_BATCH_GROUP shots of a 2D batch, passed to the
+// batched kernels by value: the shots' parameter blocks live in kernel
+// parameter space (read through the constant cache like a single shot's
+// parameters, 64 x 368 bytes at most, under the 32 KB parameter limit), and
+// work holds the group's work items, one per block: x = shot index in the
+// batch, y = tile row (x direction) << 16 | tile column (z direction).
 #define SW_BATCH_TILES 4
+#define SW_BATCH_GROUP 64
 template <typename T>
 struct Batch2 {
-  const P2<T>* shots;
+  P2<T> shots[SW_BATCH_GROUP];
   const int2* work;
-  int nshots;
+  int first, n;  // batch index of shots[0]; shots in the group
 };
 
 template <typename T>
