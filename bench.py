@@ -114,6 +114,13 @@ class ClockSampler:
 
 
 def build_solver(cfg, torch, exact=True, dtype=None, coef64=False):
+    if cfg.get("scheme") == "SPML":
+        from seiswave_taichi_b200.Elastic3D_SSG_SPML import ElasticWAVE as SPML
+        w = SPML(cfg["vs"], cfg["vp"], cfg["rho"], cfg["dx"], cfg["dy"], cfg["dz"], cfg["dt"], cfg["isx"],
+                 cfg["isy"], cfg["isz"], cfg["rsx"], cfg["rsy"], cfg["rsz"], cfg["nt"], cfg["accuracy"], cfg["freq"],
+                 cfg["src_scale"], dtype or torch.float32, exact=exact, coef64=coef64)
+        w.SetADEPML3D(cfg["surface"], cfg["pml"])
+        return w
     from seiswave_taichi_b200.Elastic3D_SSG_Tensor import ElasticWAVE
     w = ElasticWAVE(cfg["vs"], cfg["vp"], cfg["rho"], cfg["dx"], cfg["dy"], cfg["dz"], cfg["dt"],
                     cfg["isx"], cfg["isy"], cfg["isz"], cfg["rsx"], cfg["rsy"], cfg["rsz"], cfg["MT"],
@@ -151,6 +158,19 @@ def fp64_error(cfg, w32, torch):
     return out
 
 
+def spml_config():
+    """The split-field PML scheme on config 2's grid: 200^3 homogeneous,
+    dx = 10 m, dt = 1 ms, 1000 steps, N = 2, 20-cell PML, a 15 Hz point force
+    (the scheme's source, Elastic3D_SSG_SPML.py:294) at the centre, one vx
+    receiver (:393)."""
+    from seiswave_taichi_b200 import synthetic as S
+    c = dict(S.config2())
+    n = c["shape"][0]
+    c.update(name=f"3d-ssg-spml-{n}^3-nt{c['nt']}", scheme="SPML", rsx=n // 2 - 30, rsy=n // 2, rsz=c["accuracy"] + 5,
+             src_scale=1.0e6, MT=None)
+    return c
+
+
 def algorithmic_bytes(cfg, npml=20):
     """Fused minimum bytes per time step: every wavefield read and written
     once, the material read once, and each CPML memory variable read and
@@ -158,6 +178,11 @@ def algorithmic_bytes(cfg, npml=20):
     S_d = 2*npml*(product of the other two extents)."""
     shape = cfg["shape"]
     ncell = int(np.prod(shape))
+    if cfg.get("scheme") == "SPML":
+        # 84 B/cell + 24 split fields read and written on the PML cells
+        nx, ny, nz = shape
+        npml_cells = ncell - (nx - 2 * npml) * (ny - 2 * npml) * (nz - 2 * npml)
+        return 84 * ncell + 8 * 24 * npml_cells
     if len(shape) == 3:
         nx, ny, nz = shape
         S = 2 * npml * (ny * nz + nx * nz + nx * ny)
@@ -172,9 +197,9 @@ def oracle_for(cfg):
     for workload cfg, and a function advancing it by n time steps from it."""
     from oracle import oracle as O
     if len(cfg["shape"]) == 3:
-        o = O.Oracle3D("TENSOR", cfg["vs"], cfg["vp"], cfg["rho"], cfg["dx"], cfg["dy"], cfg["dz"], cfg["dt"],
-                       cfg["isx"], cfg["isy"], cfg["isz"], cfg["rsx"], cfg["rsy"], cfg["rsz"], cfg["nt"],
-                       cfg["accuracy"], cfg["freq"], cfg["surface"], cfg["pml"], MT=cfg["MT"],
+        o = O.Oracle3D(cfg.get("scheme", "TENSOR"), cfg["vs"], cfg["vp"], cfg["rho"], cfg["dx"], cfg["dy"],
+                       cfg["dz"], cfg["dt"], cfg["isx"], cfg["isy"], cfg["isz"], cfg["rsx"], cfg["rsy"], cfg["rsz"],
+                       cfg["nt"], cfg["accuracy"], cfg["freq"], cfg["surface"], cfg["pml"], MT=cfg["MT"],
                        src_scale=cfg["src_scale"])
         return lambda it, n: o.run(it, n)
     from seiswave_taichi_b200 import BaseFun
@@ -248,6 +273,8 @@ def get_config(name):
         return S.config1()
     if name == "config3":
         return S.config3()
+    if name == "spml":
+        return spml_config()
     raise SystemExit(f"unknown config {name}")
 
 
@@ -619,7 +646,7 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="config2", choices=["config2", "config1", "config3", "config4", "config5", "segy"])
+    ap.add_argument("--config", default="config2", choices=["config2", "config1", "config3", "config4", "config5", "segy", "spml"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the float64 error runs")
     ap.add_argument("--path", default=None, choices=["staged", "fused", "two_pass"],
@@ -716,7 +743,7 @@ def main(argv=None):
 
     # the opt-in fast numeric mode (exact=False) on the same workload
     fast = None
-    if three_d:
+    if three_d and cfg.get("scheme") != "SPML":  # the split-field PML runs exact numerics only
         wf = build_solver(cfg, torch, exact=False)
         wf.autotune()
         for _ in range(2):

@@ -117,19 +117,45 @@ __device__ __forceinline__ Vq<Q> ldgq(const float* p) {
   return __ldg(reinterpret_cast<const Vq<Q>*>(p));
 }
 // Exact mode with two z cells per thread computes on cell pairs with the
-// packed two-lane FP32 instructions of sm_100 (__fadd2_rn, __fmul2_rn,
-// __ffma2_rn): each lane is one IEEE round-to-nearest operation, the same
-// bits as the scalar instruction, at half the instruction count.
+// packed two-lane FP32 instructions of sm_100 (add/mul/fma .rn.f32x2): each
+// lane is one IEEE round-to-nearest operation, the same bits as the scalar
+// instruction, at half the instruction count.  They are written as inline
+// PTX with the explicit .rn modifier, which the optimizer never contracts
+// (a multiply and an add fused into one fma would round once instead of
+// twice and leave the reference's operation order).
 #ifndef SW_STAGED_PACKED
-#define SW_STAGED_PACKED 1
+#define SW_STAGED_PACKED 0
 #endif
 template <bool EX, int Q>
 constexpr bool packed() { return SW_STAGED_PACKED && EX && Q == 2; }
 __device__ __forceinline__ float2 sp2(float c) { return make_float2(c, c); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) {
+  float2 d;
+  asm("{\n .reg .b64 ra, rb, rd;\n mov.b64 ra, {%2, %3};\n mov.b64 rb, {%4, %5};\n"
+      " add.rn.f32x2 rd, ra, rb;\n mov.b64 {%0, %1}, rd;\n}"
+      : "=f"(d.x), "=f"(d.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return d;
+}
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) {
+  float2 d;
+  asm("{\n .reg .b64 ra, rb, rd;\n mov.b64 ra, {%2, %3};\n mov.b64 rb, {%4, %5};\n"
+      " mul.rn.f32x2 rd, ra, rb;\n mov.b64 {%0, %1}, rd;\n}"
+      : "=f"(d.x), "=f"(d.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return d;
+}
+// a * b + c with one rounding
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
+  float2 d;
+  asm("{\n .reg .b64 ra, rb, rc, rd;\n mov.b64 ra, {%2, %3};\n mov.b64 rb, {%4, %5};\n"
+      " mov.b64 rc, {%6, %7};\n fma.rn.f32x2 rd, ra, rb, rc;\n mov.b64 {%0, %1}, rd;\n}"
+      : "=f"(d.x), "=f"(d.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+  return d;
+}
 // a - b with one rounding: fma(b, -1, a)
-__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, sp2(-1.f), a); }
-__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
-__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return fma2(b, sp2(-1.f), a); }
 
 __device__ __forceinline__ float g4(const float4& v, int e) { return e == 0 ? v.x : e == 1 ? v.y : e == 2 ? v.z : v.w; }
 __device__ __forceinline__ void s4(float4& v, int e, float x) {
@@ -213,14 +239,29 @@ __device__ __forceinline__ Vq<Q> dzq(const float* s, int off, const float* c) {
 // rounding, 53 >= 2*24+2), the same result div_c gives -- again without a
 // per-lane branch.  Keeping range tests off the per-lane path leaves the
 // group's independent lanes free to interleave.
+// The group test, the same predicate as mk_ok on every lane, in three
+// instructions per value: the smallest of 2*bits - 2 (unsigned; a zero of
+// either sign maps to 0xfffffffe, a magnitude below 2^-100 below
+// 2*0x0d800000 - 2) and the largest |x| (NaN is ignored by fmaxf; it stays
+// NaN on either path).
+struct RangeAcc {
+  unsigned lo = 0xffffffffu;
+  float hi = 0.f;
+  __device__ __forceinline__ void add(float x) {
+    lo = min(lo, __float_as_uint(x) * 2u - 2u);
+    hi = fmaxf(hi, fabsf(x));
+  }
+  __device__ __forceinline__ bool ok() const { return lo >= 2u * 0x0D800000u - 2u && hi < 0x1p100f; }
+};
+
 template <int K, int Q>
 __device__ __forceinline__ void div_group(Vq<Q> (&v)[K], const float (&d)[K], const float (&r)[K], int fast) {
-  bool ok = fast != 0;
+  RangeAcc acc;
 #pragma unroll
   for (int k = 0; k < K; ++k)
 #pragma unroll
-    for (int e = 0; e < Q; ++e) ok = ok & mk_ok(g4(v[k], e));
-  if (ok) {
+    for (int e = 0; e < Q; ++e) acc.add(g4(v[k], e));
+  if (fast != 0 && acc.ok()) {
     if constexpr (packed<true, Q>()) {
       // Markstein's correction on pairs; a zero numerator gives +0 like
       // mk_div (a stencil sum, which starts from +0 + c*(a-b), is never -0)
@@ -228,8 +269,8 @@ __device__ __forceinline__ void div_group(Vq<Q> (&v)[K], const float (&d)[K], co
       for (int k = 0; k < K; ++k) {
         const float2 rr = sp2(r[k]);
         const float2 q = mul2(v[k], rr);
-        const float2 e = __ffma2_rn(q, sp2(-d[k]), v[k]);
-        v[k] = __ffma2_rn(e, rr, q);
+        const float2 e = fma2(q, sp2(-d[k]), v[k]);
+        v[k] = fma2(e, rr, q);
       }
     } else {
 #pragma unroll
@@ -238,10 +279,19 @@ __device__ __forceinline__ void div_group(Vq<Q> (&v)[K], const float (&d)[K], co
         for (int e = 0; e < Q; ++e) s4(v[k], e, mk_div(g4(v[k], e), d[k], r[k]));
     }
   } else {
+    // some lane of the group is tiny, huge or the path is unverified: each
+    // value takes its own route, and only the lanes that need it enter the
+    // out-of-line double-precision quotient
 #pragma unroll
     for (int k = 0; k < K; ++k)
 #pragma unroll
-      for (int e = 0; e < Q; ++e) s4(v[k], e, dd_div(g4(v[k], e), d[k]));
+      for (int e = 0; e < Q; ++e) {
+        const float x = g4(v[k], e);
+        float y;
+        if (fast != 0 && mk_ok(x)) y = mk_div(x, d[k], r[k]);
+        else y = div_rare(x, d[k]);
+        s4(v[k], e, y);
+      }
   }
 }
 
@@ -735,15 +785,19 @@ k3s_velocity(const __grid_constant__ P3<float> p, const __grid_constant__ Staged
             }
           }
           if (EX) {
-            bool okq = true;
+            RangeAcc acc;
 #pragma unroll
-            for (int q = 0; q < 3 * Q; ++q) okq = okq & mk_ok(tn[q]);
-            if (okq) {
+            for (int q = 0; q < 3 * Q; ++q) acc.add(tn[q]);
+            if (acc.ok()) {
 #pragma unroll
               for (int q = 0; q < 3 * Q; ++q) tn[q] = tn[q] == 0.f ? tn[q] : __fdiv_rn(tn[q], td[q]);
             } else {
 #pragma unroll
-              for (int q = 0; q < 3 * Q; ++q) tn[q] = dd_div(tn[q], td[q]);
+              for (int q = 0; q < 3 * Q; ++q) {
+                const float x = tn[q];
+                if (mk_ok(x)) tn[q] = x == 0.f ? x : __fdiv_rn(x, td[q]);
+                else tn[q] = div_rare(x, td[q]);
+              }
             }
           } else {
 #pragma unroll
@@ -1142,10 +1196,16 @@ static StagedConfig staged_cfg_t() {
 }
 
 // tile shapes per order: (TY, D); TZ is 32 or 40
+#ifndef SW_TY240
+#define SW_TY240 16
+#endif
+#ifndef SW_D240
+#define SW_D240 1
+#endif
 #define SW_STAGED_SWITCH(N_, TZ_, CALL)                         \
   switch ((N_) * 100 + (TZ_)) {                                 \
     case 132: CALL(1, 16, 2, 32) case 140: CALL(1, 16, 2, 40)   \
-    case 232: CALL(2, 16, 1, 32) case 240: CALL(2, 16, 1, 40)   \
+    case 232: CALL(2, 16, 1, 32) case 240: CALL(2, SW_TY240, SW_D240, 40)   \
     case 332: CALL(3, 16, 2, 32) case 340: CALL(3, 16, 2, 40)   \
     case 432: CALL(4, 16, 1, 32) case 440: CALL(4, 16, 1, 40)   \
     default: break;                                             \
