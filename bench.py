@@ -390,6 +390,18 @@ def run_batch(args, rank, world, local):
         torch.cuda.synchronize()
     ms = max_over_ranks(e0.elapsed_time(e1), dist)
     value = whole_job_value(world, cells, nt, args.steps, ms)
+    # the same shots one after the other, each through its own cached graph
+    for w in waves:
+        w.reset()
+        w.run(nt)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for w in waves:
+        w.reset()
+        w.run(nt)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    seq_ms = max_over_ranks(e0.elapsed_time(e1), dist)
     # error of the batched float32 forward against float64 runs of the same
     # scheme (the first four shots, one by one)
     err64 = None
@@ -436,6 +448,9 @@ def run_batch(args, rank, world, local):
                        "time_steps": nt, "accuracy": 2, "parallelism": f"replicas{world}", "tile": info,
                        "l2": "batch state (~1.2 GB) larger than L2"},
             "shots_per_s": world * len(waves) * args.steps / (ms * 1e-3),
+            "sequential": {"value": whole_job_value(world, cells, nt, 1, seq_ms), "unit": "Gcell-updates/s",
+                           "shots_per_s": world * len(waves) / (seq_ms * 1e-3),
+                           "what": "the same shots one after the other, each from its own cached CUDA graph"},
             "fwi_step": {"ms": fwi_ms, "checkpoint_every": 100,
                          "what": "batched forward with checkpoints + 64 per-shot adjoints + gradient chain, "
                                  "observed traces from pinned host memory, gradients back to the host"},

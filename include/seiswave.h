@@ -172,6 +172,16 @@ SW_API int sw3d_plan_create(const sw3d_desc* desc, sw_plan** plan);
  * (the autotuner's knob; the plan picks a default from the grid and SM count). */
 SW_API int sw_plan_set_tile(sw_plan* plan, int32_t x_chunk);
 
+/* No reference counterpart (a self-check of this library's exact division).
+ * Counts the finite float numerators x (all 2^32 bit patterns) for which the
+ * kernels' quotient by `divisor` differs from IEEE division x/divisor: mode 0
+ * the constant-spacing quotient (Markstein's correction with r = RN(1/d), its
+ * scaled form below 2^-100), which a plan enables for a spacing only when
+ * this count is zero; mode 1 the per-cell quotient (density, kappa) with its
+ * scaled route for numerators below 2^-100.  Blocks on the stream; about a
+ * millisecond on a B200.  Allocates one 8-byte counter. */
+SW_API int sw_check_division(float divisor, int32_t mode, uint64_t* mismatches, void* stream);
+
 /* Block until the stream is idle and report a device-side failure recorded
  * by the plan's kernels since the previous status read (SW_ERR_TIMEOUT: a
  * bounded wait for TMA data, or a grid barrier of the 2D persistent run, gave

@@ -29,7 +29,7 @@ SW_SRC_NONE, SW_SRC_FORCE, SW_SRC_MOMENT, SW_SRC_RSG4 = 0, 1, 2, 3
 EXPORTS = (
     "sw_version", "sw_last_error", "sw2d_plan_create", "sw3d_plan_create",
     "sw_plan_set_tile", "sw_abi_sizeof", "sw_plan_destroy", "sw_step", "sw_step_amp",
-    "sw_run", "sw_check_finite", "sw_plan_status", "sw_plan_info", "sw_plan_set_path",
+    "sw_run", "sw_check_finite", "sw_check_division", "sw_plan_status", "sw_plan_info", "sw_plan_set_path",
     "sw_plan_set_exact", "sw_count_nonfinite_noalloc", "sw2d_snapshot_elems", "sw2d_record",
     "sw2d_adjoint_run", "sw2d_batch_create", "sw_batch_set_tile", "sw_batch_info", "sw_batch_run",
     "sw_batch_destroy", "sw2d_abc_correct", "sw2d_abc_features", "sw_mlp_grad", "sw_mlp_forward",
@@ -149,6 +149,7 @@ def load() -> C.CDLL:
         "sw_step_amp": (C.c_int, [vp, C.c_int32, C.c_double, vp]),
         "sw_run": (C.c_int, [vp, C.c_int32, C.c_int32, C.c_int32, vp]),
         "sw_check_finite": (C.c_int, [vp, vp, C.POINTER(C.c_int64)]),
+        "sw_check_division": (C.c_int, [C.c_float, C.c_int32, C.POINTER(C.c_uint64), vp]),
         "sw_plan_status": (C.c_int, [vp, vp]),
         "sw_plan_info": (C.c_int, [vp, C.POINTER(C.c_int32)]),
         "sw_plan_set_path": (C.c_int, [vp, C.c_int32, C.c_int32]),
@@ -241,6 +242,15 @@ def count_nonfinite_noalloc(tensors, stream: int | None = None) -> list[int]:
     if rc not in (SW_OK, SW_ERR_NONFINITE):
         check(rc)
     return [int(out[a]) for a in range(n)]
+
+
+def check_division(divisor: float, mode: int, stream: int = 0) -> int:
+    """Numerators (of all 2^32 floats) where the kernels' quotient by divisor
+    differs from IEEE division: mode 0 the constant-spacing path, mode 1 the
+    per-cell path (sw_check_division)."""
+    out = C.c_uint64(0)
+    check(load().sw_check_division(C.c_float(divisor), int(mode), C.byref(out), C.c_void_p(stream)))
+    return int(out.value)
 
 
 class SeisWaveError(RuntimeError):

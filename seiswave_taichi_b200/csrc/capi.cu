@@ -774,6 +774,20 @@ int sw_plan_set_tile(sw_plan* pl, int32_t x_chunk) {
   return SW_OK;
 }
 
+int sw_check_division(float divisor, int32_t mode, uint64_t* mismatches, void* stream) {
+  if (!mismatches || (mode != 0 && mode != 1)) return fail(SW_ERR_ARG, "sw_check_division: mode 0 or 1 and an output");
+  if (!(divisor > 0.f) || !std::isfinite(divisor)) return fail(SW_ERR_ARG, "sw_check_division: positive finite divisor");
+  unsigned long long* d_bad = nullptr;
+  unsigned long long h_bad = 0;
+  cudaError_t e = cudaMalloc(&d_bad, sizeof(unsigned long long));
+  if (e != cudaSuccess) return cuda_fail(e, "sw_check_division");
+  e = sw::sw3_check_divisor(divisor, 1.f / divisor, d_bad, &h_bad, (cudaStream_t)stream, mode);
+  cudaFree(d_bad);
+  if (e != cudaSuccess) return cuda_fail(e, "sw_check_division");
+  *mismatches = h_bad;
+  return SW_OK;
+}
+
 int sw_plan_status(sw_plan* pl, void* stream) {
   if (!pl) return fail(SW_ERR_ARG, "null plan");
   cudaStream_t st = (cudaStream_t)stream;

@@ -621,14 +621,17 @@ k3_fused(const __grid_constant__ P3<float> p, const __grid_constant__ FusedMaps 
 // ---------------------------------------------------------------------------
 // exhaustive check of the constant-divisor path against IEEE division
 // ---------------------------------------------------------------------------
-__global__ void k_check_divc(float d, float r, unsigned long long* bad) {
+// mode 0: the constant-divisor quotient div_c (r = RN(1/d)); mode 1: the
+// per-cell quotient div_v; both against IEEE division, every finite float
+// numerator
+__global__ void k_check_divc(float d, float r, int mode, unsigned long long* bad) {
   unsigned long long local = 0;
   const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
   for (unsigned long long b = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; b < (1ull << 32);
        b += stride) {
     const float xv = __uint_as_float((unsigned)b);
     if (!isfinite(xv)) continue;
-    const float a = div_c(xv, d, r, 1);
+    const float a = mode == 0 ? div_c(xv, d, r, 1) : div_v(xv, d);
     const float e = __fdiv_rn(xv, d);
     if (__float_as_uint(a) != __float_as_uint(e)) ++local;
   }
@@ -636,10 +639,10 @@ __global__ void k_check_divc(float d, float r, unsigned long long* bad) {
 }
 
 cudaError_t sw3_check_divisor(float d, float r, unsigned long long* d_bad, unsigned long long* h_bad,
-                              cudaStream_t st) {
+                              cudaStream_t st, int mode) {
   cudaError_t e = cudaMemsetAsync(d_bad, 0, sizeof(unsigned long long), st);
   if (e != cudaSuccess) return e;
-  k_check_divc<<<148 * 16, 256, 0, st>>>(d, r, d_bad);
+  k_check_divc<<<148 * 16, 256, 0, st>>>(d, r, mode, d_bad);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   e = cudaMemcpyAsync(h_bad, d_bad, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);

@@ -24,6 +24,17 @@
 
 namespace sw {
 
+// SW_OWN_TMA: the plane's own cells (the fields a pass updates) arrive by
+// TMA with the neighbour planes instead of per-thread global loads.
+// SW_ONE_BARRIER: one CTA barrier per plane (the next plane's wait folded
+// into it) instead of two.
+#ifndef SW_OWN_TMA
+#define SW_OWN_TMA 0
+#endif
+#ifndef SW_ONE_BARRIER
+#define SW_ONE_BARRIER 0
+#endif
+
 // z cells per thread: 2 in exact mode, 4 in fast mode.  With two cells per
 // thread the exact velocity pass is bound to three 256-thread CTAs per SM
 // (80 registers, 16/32 bytes of spills: 24 resident warps) and the stress
@@ -73,7 +84,8 @@ struct SG {
   static constexpr int V_YZ = V_YY + R1 * pad(B_Y);
   static constexpr int V_ZZ = V_YZ + R1 * pad(B_YZ);
   static constexpr int V_R = V_ZZ + R1 * pad(B_Z);
-  static constexpr int V_TAB = V_R + R2 * pad(B_R);  // CPML tables of the unit's rows and z cells
+  static constexpr int V_OWN = V_R + R2 * pad(B_R);        // vx vy vz of the plane (own cells)
+  static constexpr int V_TAB = V_OWN + (SW_OWN_TMA ? 3 * R1 * pad(B_XX) : 0);  // CPML tables of the unit
   static constexpr int TAB = pad(6 * (TY + TZ));
   static constexpr int V_FLOATS = V_TAB + TAB;
   // stress pass layout (floats)
@@ -82,7 +94,8 @@ struct SG {
   static constexpr int S_VZ = S_VY + RX * pad(B_YZ);
   static constexpr int S_L = S_VZ + RX * pad(B_YZ);
   static constexpr int S_M = S_L + R2 * pad(B_L);
-  static constexpr int S_TAB = S_M + R2 * pad(B_M);
+  static constexpr int S_OWN = S_M + R2 * pad(B_M);         // the six stresses of the plane (own cells)
+  static constexpr int S_TAB = S_OWN + (SW_OWN_TMA ? 6 * R1 * pad(B_L) : 0);
   static constexpr int S_FLOATS = S_TAB + TAB;
   static constexpr size_t V_BYTES = (size_t)V_FLOATS * 4 + 8 * (D + 1) + 128;
   static constexpr size_t S_BYTES = (size_t)S_FLOATS * 4 + 8 * (D + 1) + 128;
@@ -280,18 +293,12 @@ __device__ __forceinline__ void div_group(Vq<Q> (&v)[K], const float (&d)[K], co
     }
   } else {
     // some lane of the group is tiny, huge or the path is unverified: each
-    // value takes its own route, and only the lanes that need it enter the
-    // out-of-line double-precision quotient
+    // value takes its own route through div_c (the scaled correction for tiny
+    // values, the double-precision quotient for huge ones)
 #pragma unroll
     for (int k = 0; k < K; ++k)
 #pragma unroll
-      for (int e = 0; e < Q; ++e) {
-        const float x = g4(v[k], e);
-        float y;
-        if (fast != 0 && mk_ok(x)) y = mk_div(x, d[k], r[k]);
-        else y = div_rare(x, d[k]);
-        s4(v[k], e, y);
-      }
+      for (int e = 0; e < Q; ++e) s4(v[k], e, div_c(g4(v[k], e), d[k], r[k], fast));
   }
 }
 
@@ -577,7 +584,8 @@ k3s_velocity(const __grid_constant__ P3<float> p, const __grid_constant__ Staged
   auto syz_p = [&](int pl) { return sm + G::V_YZ + rslot(pl, G::R1) * PYZ; };
   auto szz_p = [&](int pl) { return sm + G::V_ZZ + rslot(pl, G::R1) * PZ; };
   auto rho_p = [&](int pl) { return sm + G::V_R + rslot(pl, G::R2) * PR; };
-  const int o_xx = r * G::TZ + Q * cq;                 // sxx, rho boxes
+  auto own_p = [&](int a, int pl) { return sm + G::V_OWN + (a * G::R1 + rslot(pl, G::R1)) * PXX; };
+  const int o_xx = r * G::TZ + Q * cq;                 // sxx, rho, own-cell boxes
   const int o_y = (r + N) * G::TZ + Q * cq;            // sxy, syy boxes
   const int o_z = r * G::WZ + G::H4 + Q * cq;          // sxz, szz boxes
   const int o_yz = (r + N) * G::WZ + G::H4 + Q * cq;   // syz box
@@ -621,8 +629,8 @@ k3s_velocity(const __grid_constant__ P3<float> p, const __grid_constant__ Staged
 
     auto issue = [&](int s, bool first, uint32_t stage) {
       uint64_t* bar = &bars[stage];
-      // sxx + sxy + sxz + syy + syz + szz + rho
-      uint32_t bytes = (G::B_XX + 2 * G::B_Y + 2 * G::B_Z + G::B_YZ + G::B_R) * 4;
+      // sxx + sxy + sxz + syy + syz + szz + rho + the plane's own vx vy vz
+      uint32_t bytes = ((SW_OWN_TMA ? 4 : 1) * G::B_XX + 2 * G::B_Y + 2 * G::B_Z + G::B_YZ + G::B_R) * 4;
       if (first) bytes += ((2 * N - 1) * (G::B_XX + G::B_Y + G::B_Z) + G::B_R) * 4;
       mbar_expect_tx(bar, bytes);
       const int zh = k0 - G::H4, yh = j0 - N;
@@ -633,6 +641,8 @@ k3s_velocity(const __grid_constant__ P3<float> p, const __grid_constant__ Staged
       tma_load3(syz_p(s), &maps.m[4], zh, yh, s, bar);
       tma_load3(szz_p(s), &maps.m[5], zh, j0, s, bar);
       tma_load3(rho_p(s + 1), &maps.m[6], k0, j0, s + 1, bar);
+      if (SW_OWN_TMA)
+        for (int c = 0; c < 3; ++c) tma_load3(own_p(c, s), &maps.m[7 + c], k0, j0, s, bar);
       if (first) {
         for (int q = 1 - N; q < N; ++q) tma_load3(sxx_p(s + q), &maps.m[0], k0, j0, s + q, bar);
         for (int q = -N; q < N - 1; ++q) {
@@ -645,13 +655,27 @@ k3s_velocity(const __grid_constant__ P3<float> p, const __grid_constant__ Staged
     if (tid == 0)
       for (int s = x0; s <= min(x0 + D, x1 - 1); ++s) issue(s, s == x0, (g + (s - x0)) % (D + 1));
 
+#if SW_ONE_BARRIER
+    // the first plane's data (bounded wait); the barrier also publishes the
+    // unit's tables
+    {
+      const bool landed = mbar_wait(&bars[g % (D + 1)], (g / (D + 1)) & 1);
+      if (__syncthreads_or(!landed)) {
+        if (tid == 0) atomicOr(a.err, 1);
+        ok = false;
+      }
+    }
+    for (int i = x0; i < x1 && ok; ++i, ++g) {
+#else
     for (int i = x0; i < x1; ++i, ++g) {
+      // this plane's data (bounded wait); the CTA agrees on the outcome
       const bool landed = mbar_wait(&bars[g % (D + 1)], (g / (D + 1)) & 1);
       if (__syncthreads_or(!landed)) {
         if (tid == 0) atomicOr(a.err, 1);
         ok = false;
         break;
       }
+#endif
       const int xi = SCH == SCH_CPML ? slab_index(i, nx, p.lo[0], p.hi[0]) : -1;
       if (jin && kin) {
         const float* pxx[2 * N];
@@ -683,7 +707,12 @@ k3s_velocity(const __grid_constant__ P3<float> p, const __grid_constant__ Staged
         }
         Vq<Q> a1 = dv[0], a2 = dv[1], a3 = dv[2], b1 = dv[3], b2 = dv[4], b3 = dv[5], c1 = dv[6], c2 = dv[7],
                c3 = dv[8];
-        Vq<Q> vx = ldgq<Q>(p.f[0] + gi), vy = ldgq<Q>(p.f[1] + gi), vz = ldgq<Q>(p.f[2] + gi);
+        Vq<Q> vx, vy, vz;
+        if (SW_OWN_TMA) {
+          vx = ldq<Q>(own_p(0, i) + o_xx), vy = ldq<Q>(own_p(1, i) + o_xx), vz = ldq<Q>(own_p(2, i) + o_xx);
+        } else {
+          vx = ldgq<Q>(p.f[0] + gi), vy = ldgq<Q>(p.f[1] + gi), vz = ldgq<Q>(p.f[2] + gi);
+        }
         // update masks: vx i in [N, nx-N-1), vy and vz i in [N+1, nx-N)
         const bool ix = i < nx - N - 1, iyz = i >= N + 1;
         bool mx[Q], my[Q], mz[Q];
@@ -793,11 +822,7 @@ k3s_velocity(const __grid_constant__ P3<float> p, const __grid_constant__ Staged
               for (int q = 0; q < 3 * Q; ++q) tn[q] = tn[q] == 0.f ? tn[q] : __fdiv_rn(tn[q], td[q]);
             } else {
 #pragma unroll
-              for (int q = 0; q < 3 * Q; ++q) {
-                const float x = tn[q];
-                if (mk_ok(x)) tn[q] = x == 0.f ? x : __fdiv_rn(x, td[q]);
-                else tn[q] = div_rare(x, td[q]);
-              }
+              for (int q = 0; q < 3 * Q; ++q) tn[q] = div_v(tn[q], td[q]);
             }
           } else {
 #pragma unroll
@@ -821,7 +846,20 @@ k3s_velocity(const __grid_constant__ P3<float> p, const __grid_constant__ Staged
         stq<Q>(p.f[1] + gi, vy);
         stq<Q>(p.f[2] + gi, vz);
       }
+#if SW_ONE_BARRIER
+      // one barrier per plane: every thread is done with plane i's ring slots
+      // (which plane i+D+1 refills) and has seen plane i+1's data land
+      const bool landed = i + 1 >= x1 || mbar_wait(&bars[(g + 1) % (D + 1)], ((g + 1) / (D + 1)) & 1);
+      if (__syncthreads_or(!landed)) {
+        if (tid == 0) atomicOr(a.err, 1);
+        ok = false;
+        ++g;  // the stage that gave up; the drain at the end waits from there
+        break;
+      }
+#else
+      // every thread is done with plane i's ring slots, which plane i+D+1 refills
       __syncthreads();
+#endif
       if (tid == 0 && i + D + 1 < x1) issue(i + D + 1, false, g % (D + 1));
     }
   }
@@ -873,6 +911,7 @@ k3s_stress(const __grid_constant__ P3<float> p, const __grid_constant__ StagedMa
   auto vz_p = [&](int pl) { return sm + G::S_VZ + rslot(pl, G::RX) * PYZ; };
   auto lam_p = [&](int pl) { return sm + G::S_L + rslot(pl, G::R2) * PL; };
   auto mu_p = [&](int pl) { return sm + G::S_M + rslot(pl, G::R2) * PM; };
+  auto own_p = [&](int a, int pl) { return sm + G::S_OWN + (a * G::R1 + rslot(pl, G::R1)) * PL; };
   const int o_v = (r + N) * G::WZ + G::H4 + Q * cq;
   const int o_l = r * G::TZ + Q * cq;
   const int o_m = r * G::WM + Q * cq;
@@ -916,7 +955,8 @@ k3s_stress(const __grid_constant__ P3<float> p, const __grid_constant__ StagedMa
 
     auto issue = [&](int s, bool first, uint32_t stage) {
       uint64_t* bar = &bars[stage];
-      uint32_t bytes = (3 * G::B_YZ + G::B_L + G::B_M) * 4;
+      // vx vy vz + lam + mu + the plane's own six stresses
+      uint32_t bytes = (3 * G::B_YZ + (SW_OWN_TMA ? 7 : 1) * G::B_L + G::B_M) * 4;
       if (first) bytes += ((2 * N - 1) * 3 * G::B_YZ + G::B_L + G::B_M) * 4;
       mbar_expect_tx(bar, bytes);
       const int zh = k0 - G::H4, yh = j0 - N;
@@ -926,6 +966,8 @@ k3s_stress(const __grid_constant__ P3<float> p, const __grid_constant__ StagedMa
       tma_load3(vz_p(s + N), &maps.m[2], zh, yh, s + N, bar);
       tma_load3(lam_p(s + 1), &maps.m[3], k0, j0, s + 1, bar);
       tma_load3(mu_p(s + 1), &maps.m[4], k0, j0, s + 1, bar);
+      if (SW_OWN_TMA)
+        for (int c = 0; c < 6; ++c) tma_load3(own_p(c, s), &maps.m[5 + c], k0, j0, s, bar);
       if (first) {
         for (int q = -N; q < N - 1; ++q) tma_load3(vx_p(s + q), &maps.m[0], zh, yh, s + q, bar);
         for (int q = 1 - N; q < N; ++q) {
@@ -939,13 +981,27 @@ k3s_stress(const __grid_constant__ P3<float> p, const __grid_constant__ StagedMa
     if (tid == 0)
       for (int s = x0; s <= min(x0 + D, x1 - 1); ++s) issue(s, s == x0, (g + (s - x0)) % (D + 1));
 
+#if SW_ONE_BARRIER
+    // the first plane's data (bounded wait); the barrier also publishes the
+    // unit's tables
+    {
+      const bool landed = mbar_wait(&bars[g % (D + 1)], (g / (D + 1)) & 1);
+      if (__syncthreads_or(!landed)) {
+        if (tid == 0) atomicOr(a.err, 1);
+        ok = false;
+      }
+    }
+    for (int i = x0; i < x1 && ok; ++i, ++g) {
+#else
     for (int i = x0; i < x1; ++i, ++g) {
+      // this plane's data (bounded wait); the CTA agrees on the outcome
       const bool landed = mbar_wait(&bars[g % (D + 1)], (g / (D + 1)) & 1);
       if (__syncthreads_or(!landed)) {
         if (tid == 0) atomicOr(a.err, 1);
         ok = false;
         break;
       }
+#endif
       const int xi = SCH == SCH_CPML ? slab_index(i, nx, p.lo[0], p.hi[0]) : -1;
       const bool src = inject_next && i == p.si && p.sj == j && p.sk >= k && p.sk < k + Q;
       if (jin && kin) {
@@ -979,8 +1035,14 @@ k3s_stress(const __grid_constant__ P3<float> p, const __grid_constant__ StagedMa
         }
         Vq<Q> e1 = dv[0], e2 = dv[1], e3 = dv[2], f1 = dv[3], f2 = dv[4], h1 = dv[5], h2 = dv[6], q1 = dv[7],
                q2 = dv[8];
-        Vq<Q> sxx = ldgq<Q>(p.f[3] + gi), syy = ldgq<Q>(p.f[4] + gi), szz = ldgq<Q>(p.f[5] + gi);
-        Vq<Q> sxy = ldgq<Q>(p.f[6] + gi), sxz = ldgq<Q>(p.f[7] + gi), syz = ldgq<Q>(p.f[8] + gi);
+        Vq<Q> sxx, syy, szz, sxy, sxz, syz;
+        if (SW_OWN_TMA) {
+          sxx = ldq<Q>(own_p(0, i) + o_l), syy = ldq<Q>(own_p(1, i) + o_l), szz = ldq<Q>(own_p(2, i) + o_l);
+          sxy = ldq<Q>(own_p(3, i) + o_l), sxz = ldq<Q>(own_p(4, i) + o_l), syz = ldq<Q>(own_p(5, i) + o_l);
+        } else {
+          sxx = ldgq<Q>(p.f[3] + gi), syy = ldgq<Q>(p.f[4] + gi), szz = ldgq<Q>(p.f[5] + gi);
+          sxy = ldgq<Q>(p.f[6] + gi), sxz = ldgq<Q>(p.f[7] + gi), syz = ldgq<Q>(p.f[8] + gi);
+        }
         // update masks: normal stresses and sxy i in [N+1, nx-N), sxz i in
         // [N, nx-N-1), syz every plane of the loop
         const bool in_ = i >= N + 1, ixz = i < nx - N - 1;
@@ -1132,7 +1194,20 @@ k3s_stress(const __grid_constant__ P3<float> p, const __grid_constant__ StagedMa
         stq<Q>(p.f[7] + gi, sxz);
         stq<Q>(p.f[8] + gi, syz);
       }
+#if SW_ONE_BARRIER
+      // one barrier per plane: every thread is done with plane i's ring slots
+      // (which plane i+D+1 refills) and has seen plane i+1's data land
+      const bool landed = i + 1 >= x1 || mbar_wait(&bars[(g + 1) % (D + 1)], ((g + 1) / (D + 1)) & 1);
+      if (__syncthreads_or(!landed)) {
+        if (tid == 0) atomicOr(a.err, 1);
+        ok = false;
+        ++g;  // the stage that gave up; the drain at the end waits from there
+        break;
+      }
+#else
+      // every thread is done with plane i's ring slots, which plane i+D+1 refills
       __syncthreads();
+#endif
       if (tid == 0 && i + D + 1 < x1) issue(i + D + 1, false, g % (D + 1));
     }
   }
@@ -1180,12 +1255,14 @@ static bool staged_maps_t(const P3<float>& p, StagedMaps* vm, StagedMaps* sm_) {
   ok = ok && map3(&vm->m[4], p.f[8], nx, ny, nz, G::WZ, G::HY);
   ok = ok && map3(&vm->m[5], p.f[5], nx, ny, nz, G::WZ, TY);
   ok = ok && map3(&vm->m[6], p.rho, nx, ny, nz, G::TZ, TY + 1);
-  // stress pass: vx vy vz lam mu
+  for (int c = 0; c < 3; ++c) ok = ok && map3(&vm->m[7 + c], p.f[c], nx, ny, nz, G::TZ, TY);
+  // stress pass: vx vy vz lam mu, then the six stresses
   ok = ok && map3(&sm_->m[0], p.f[0], nx, ny, nz, G::WZ, G::HY);
   ok = ok && map3(&sm_->m[1], p.f[1], nx, ny, nz, G::WZ, G::HY);
   ok = ok && map3(&sm_->m[2], p.f[2], nx, ny, nz, G::WZ, G::HY);
   ok = ok && map3(&sm_->m[3], p.lam, nx, ny, nz, G::TZ, TY);
   ok = ok && map3(&sm_->m[4], p.mu, nx, ny, nz, G::WM, TY + 1);
+  for (int c = 0; c < 6; ++c) ok = ok && map3(&sm_->m[5 + c], p.f[3 + c], nx, ny, nz, G::TZ, TY);
   return ok;
 }
 

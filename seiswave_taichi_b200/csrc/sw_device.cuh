@@ -170,32 +170,76 @@ static __device__ __noinline__ float div_rare(float x, float d) {
   return __double2float_rn(__ddiv_rn((double)x, (double)d));
 }
 
+// The quotient x/d from xs = x*2^64 (exact) and ys = RN(xs/d) for d > 0,
+// ys normal: scaled back while normal; in the subnormal range rounded again
+// to the 2^-149 grid (2^-85 after the scaling), where only a scaled quotient
+// exactly on a midpoint of that grid can round differently from x/d itself;
+// the exact residual xs - ys*d (representable because ys is the correctly
+// rounded quotient) tells on which side x/d lies.
+__device__ __forceinline__ float tiny_finish(float xs, float ys, float d) {
+  if (fabsf(ys) >= 0x1p-62f) return __fmul_rn(ys, 0x1p-64f);
+  const float t = __fmul_rn(ys, 0x1p85f);  // |t| < 2^23: units of the subnormal grid
+  float n = rintf(t);
+  if (fabsf(__fadd_rn(t, -truncf(t))) == 0.5f) {
+    const float res = __fmaf_rn(-ys, d, xs);
+    if (res > 0.f) n = __fadd_rn(floorf(t), 1.f);
+    else if (res < 0.f) n = floorf(t);
+  }
+  return __fmul_rn(n, 0x1p-149f);
+}
+
+// x / d for 0 < |x| < 2^-100 and a per-cell divisor: the scaled numerator
+// goes through IEEE division's fast path (a tiny numerator sends the float
+// division routine to its slow path); divisors outside [2^-60, 2^60] take
+// the double-precision quotient.
+static __device__ __noinline__ float div_tiny_v(float x, float d) {
+  if (!(d >= 0x1p-60f && d <= 0x1p60f)) return div_rare(x, d);
+  const float xs = __fmul_rn(x, 0x1p64f);
+  return tiny_finish(xs, __fdiv_rn(xs, d), d);
+}
+
 template <>
 __device__ __forceinline__ float div_v<float>(float x, float d) {
   const unsigned ex = (__float_as_uint(x) >> 23) & 0xffu;  // biased exponent
   if (ex - 27u < 200u) return __fdiv_rn(x, d);                // |x| in [2^-100, 2^100)
   if ((__float_as_uint(x) << 1) == 0u) return x;              // +-0/d = +-0 for d > 0
+  if (ex < 27u) return div_tiny_v(x, d);                      // 0 < |x| < 2^-100
   return div_rare(x, d);
+}
+
+// Markstein's correction of x * r towards x / d, r = RN(1/d)
+__device__ __forceinline__ float mk_core(float x, float d, float r) {
+  const float q = __fmul_rn(x, r);
+  const float e = __fmaf_rn(-q, d, x);
+  return __fmaf_rn(e, r, q);
+}
+
+// x / d for 0 < |x| < 2^-100 (the numerical precursor ahead of a wavefront)
+// with the constant divisor's correction: the numerator is scaled by 2^64
+// (exact) into the corrected range and the quotient scaled back, exact while
+// it stays normal.  A quotient below the normal range is rounded again to
+// the subnormal grid (2^-149, i.e. 2^-85 after the scaling); that second
+// rounding can only differ from rounding x/d directly when the scaled
+// quotient lies exactly on a midpoint of the grid, and there the exact
+// residual xs - ys*d tells on which side x/d lies.
+__device__ __forceinline__ float mk_div_tiny(float x, float d, float r) {
+  const float xs = __fmul_rn(x, 0x1p64f);
+  return tiny_finish(xs, mk_core(xs, d, r), d);
 }
 
 // x / d for a divisor fixed for the run (dx, dy, dz), r = RN(1/d).  With
 // fast != 0 (float only) numerators of magnitude in [2^-100, 2^100) use
 // Markstein's correction
 //   q = RN(x*r), e = fma(-q, d, x), result = fma(e, r, q)
-// (P. Markstein, IBM J. Res. Dev. 34(1), 1990); zeros, denormals and huge
-// values take div_v.  The plan enables the fast path only after checking
-// that the whole function equals IEEE division x/d for every finite float x.
+// (P. Markstein, IBM J. Res. Dev. 34(1), 1990), smaller nonzero ones
+// mk_div_tiny; zeros pass through and huge values take div_rare.  The plan
+// enables the fast path only after checking that the whole function equals
+// IEEE division x/d for every finite float x (the 2^32 bit patterns).
 __device__ __forceinline__ float div_c(float x, float d, float r, int fast) {
   const unsigned ex = (__float_as_uint(x) >> 23) & 0xffu;  // biased exponent
-  if (ex - 27u < 200u) {
-    if (fast) {
-      const float q = __fmul_rn(x, r);
-      const float e = __fmaf_rn(-q, d, x);
-      return __fmaf_rn(e, r, q);
-    }
-    return __fdiv_rn(x, d);
-  }
+  if (ex - 27u < 200u) return fast ? mk_core(x, d, r) : __fdiv_rn(x, d);
   if ((__float_as_uint(x) << 1) == 0u) return x;  // +-0/d = +-0 for d > 0
+  if (fast && ex < 27u) return mk_div_tiny(x, d, r);
   return div_rare(x, d);
 }
 __device__ __forceinline__ double div_c(double x, double d, double, int) { return div_v(x, d); }

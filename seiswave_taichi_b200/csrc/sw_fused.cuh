@@ -38,6 +38,6 @@ cudaError_t sw3_fused_step(int N, bool tensor, const P3<float>& p, const FusedMa
 // exhaustive comparison of the constant-divisor path (div_c) with IEEE
 // division for every finite float numerator; *h_bad = number of differing results
 cudaError_t sw3_check_divisor(float d, float r, unsigned long long* d_bad, unsigned long long* h_bad,
-                              cudaStream_t st);
+                              cudaStream_t st, int mode = 0);
 
 }  // namespace sw

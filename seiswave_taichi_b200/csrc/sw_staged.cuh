@@ -8,9 +8,10 @@
 
 namespace sw {
 
-// velocity pass maps: sxx sxy sxz syy syz szz rho; stress pass: vx vy vz lam mu
+// velocity pass maps: sxx sxy sxz syy syz szz rho vx vy vz; stress pass:
+// vx vy vz lam mu sxx syy szz sxy sxz syz
 struct StagedMaps {
-  CUtensorMap m[7];
+  CUtensorMap m[11];
 };
 
 struct StagedArgs {

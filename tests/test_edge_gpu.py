@@ -116,3 +116,29 @@ def test_2d_receiver_component_selector(cuda, comp, mt):
         vp, vs, rho = (torch.as_tensor(c[k], device="cuda") for k in ("vp", "vs", "rho"))
         with pytest.raises(RuntimeError, match="own component"):
             make().forward_op(vp, vs, rho, checkpoint_every=10)
+
+
+@pytest.mark.parametrize("h", [10.0, 12.5, 2.5])
+def test_constant_divisor_path_verified(cuda, h):
+    """The plan enables the corrected quotient by the grid spacing (Markstein's
+    correction, and its scaled form for numerators below 2^-100) only after
+    an exhaustive check against IEEE division over every float numerator;
+    the spacings of the workloads pass that check."""
+    c = case3d(shape=(24, 22, 20), N=2, scheme="TENSOR", nt=4, dx=h, dy=h, dz=h, dt=2e-4)
+    w = product3d(c)
+    assert w._build_plan().info()["fast_div"] is True
+
+
+@pytest.mark.parametrize("d", [2000.0, 1741.3, 2155.25, 1.0, 1.7319, 3.3, 0.62])
+def test_per_cell_quotient_equals_ieee_for_every_numerator(cuda, d):
+    """The per-cell quotient (density averages, CPML kappa, split-PML
+    denominators), including its scaled route for numerators below 2^-100,
+    equals IEEE division for all 2^32 float numerators."""
+    from seiswave_taichi_b200 import _native as N
+    assert N.check_division(d, 1) == 0
+
+
+@pytest.mark.parametrize("h", [10.0, 12.5, 2.5])
+def test_spacing_quotient_equals_ieee_for_every_numerator(cuda, h):
+    from seiswave_taichi_b200 import _native as N
+    assert N.check_division(h, 0) == 0
