@@ -21,7 +21,7 @@
  * Threading: work is enqueued on the caller's stream (a cudaStream_t passed as
  * void*, NULL = legacy default stream).  A plan is not thread-safe; use one plan
  * per stream.  No call blocks the host except sw_check_finite,
- * sw_count_nonfinite_noalloc and sw_plan_status.
+ * sw_count_nonfinite_noalloc, sw_check_division and sw_plan_status.
  */
 #ifndef SEISWAVE_H
 #define SEISWAVE_H
