@@ -41,12 +41,12 @@ sys.path.insert(0, str(ROOT))
 
 FALLBACK_HBM_GBS = 6650.0
 
-# DRAM bytes per time step (velocity + stress launch pair, default path and
-# numerics) from one ncu capture of the full workload (profiles/).
 # dram__bytes_read.sum + dram__bytes_write.sum of one k_segy_decode<1> launch
 # at 8192 x 16000 IBM samples
 SEGY_NCU_TRAFFIC = (525.916672 + 482.566656) * 1e6
-NCU_TRAFFIC_PER_STEP = {"3d-ssg-cpml-tensor-200^3-nt1000": (421.792512 + 127.147008 + 516.385536 + 223.332864) * 1e6}
+# DRAM bytes per time step (velocity + stress launch pair at step 700, default
+# path and exact numerics) from one ncu capture of the full workload (profiles/).
+NCU_TRAFFIC_PER_STEP = {"3d-ssg-cpml-tensor-200^3-nt1000": (418.751744 + 123.215104 + 460.371968 + 207.120384) * 1e6}
 
 
 def peaks():
