@@ -178,8 +178,12 @@ SW_API int sw_plan_set_tile(sw_plan* plan, int32_t x_chunk);
  * the constant-spacing quotient (Markstein's correction with r = RN(1/d), its
  * scaled form below 2^-100), which a plan enables for a spacing only when
  * this count is zero; mode 1 the per-cell quotient (density, kappa) with its
- * scaled route for numerators below 2^-100.  Blocks on the stream; about a
- * millisecond on a B200.  Allocates one 8-byte counter. */
+ * scaled route for numerators below 2^-100; modes 2 and 3 the branch-free
+ * forms of modes 0 and 1 that quotient groups holding numerators below
+ * 2^-100 use, over the numerators of magnitude below 2^100 (mode 2 is also
+ * checked before a plan enables a spacing; mode 3 takes divisors in
+ * [2^-60, 2^60]).  Blocks on the stream; about a millisecond on a B200.
+ * Allocates one 8-byte counter. */
 SW_API int sw_check_division(float divisor, int32_t mode, uint64_t* mismatches, void* stream);
 
 /* Block until the stream is idle and report a device-side failure recorded

@@ -247,7 +247,8 @@ def count_nonfinite_noalloc(tensors, stream: int | None = None) -> list[int]:
 def check_division(divisor: float, mode: int, stream: int = 0) -> int:
     """Numerators (of all 2^32 floats) where the kernels' quotient by divisor
     differs from IEEE division: mode 0 the constant-spacing path, mode 1 the
-    per-cell path (sw_check_division)."""
+    per-cell path, modes 2 and 3 their branch-free group forms over the
+    numerators below 2^100 (sw_check_division)."""
     out = C.c_uint64(0)
     check(load().sw_check_division(C.c_float(divisor), int(mode), C.byref(out), C.c_void_p(stream)))
     return int(out.value)

@@ -257,7 +257,9 @@ bool verified_divisor(float d, float r, cudaStream_t st) {
   unsigned long long hbad = 1;
   bool ok = false;
   if (cudaMalloc(&dbad, sizeof(unsigned long long)) == cudaSuccess) {
-    ok = sw::sw3_check_divisor(d, r, dbad, &hbad, st) == cudaSuccess && hbad == 0;
+    // the per-lane route and the staged kernels' branch-free group route
+    ok = sw::sw3_check_divisor(d, r, dbad, &hbad, st, 0) == cudaSuccess && hbad == 0 &&
+         sw::sw3_check_divisor(d, r, dbad, &hbad, st, 2) == cudaSuccess && hbad == 0;
     cudaFree(dbad);
   }
   cudaGetLastError();
@@ -775,8 +777,10 @@ int sw_plan_set_tile(sw_plan* pl, int32_t x_chunk) {
 }
 
 int sw_check_division(float divisor, int32_t mode, uint64_t* mismatches, void* stream) {
-  if (!mismatches || (mode != 0 && mode != 1)) return fail(SW_ERR_ARG, "sw_check_division: mode 0 or 1 and an output");
+  if (!mismatches || mode < 0 || mode > 3) return fail(SW_ERR_ARG, "sw_check_division: mode 0..3 and an output");
   if (!(divisor > 0.f) || !std::isfinite(divisor)) return fail(SW_ERR_ARG, "sw_check_division: positive finite divisor");
+  if (mode == 3 && !(divisor >= 0x1p-60f && divisor <= 0x1p60f))
+    return fail(SW_ERR_ARG, "sw_check_division: mode 3 needs a divisor in [2^-60, 2^60]");
   unsigned long long* d_bad = nullptr;
   unsigned long long h_bad = 0;
   cudaError_t e = cudaMalloc(&d_bad, sizeof(unsigned long long));

@@ -242,21 +242,22 @@ __device__ __forceinline__ Vq<Q> dzq(const float* s, int off, const float* c) {
   return o;
 }
 
-// Exact division of a group of stencil sums by the constant spacings.  When
-// the spacings' Markstein path is verified (fast != 0) and every lane is zero
-// or of magnitude in [2^-100, 2^100), the whole group runs as one branch-free
-// block: the same correction div_c applies to such lanes, with zeros passed
-// through unchanged (so the sign of zero is kept).  Otherwise every lane is
-// divided in double precision and rounded once to float -- the correctly
-// rounded float quotient for every finite float input (innocuous double
-// rounding, 53 >= 2*24+2), the same result div_c gives -- again without a
-// per-lane branch.  Keeping range tests off the per-lane path leaves the
-// group's independent lanes free to interleave.
+// Exact division of a group of stencil sums by the constant spacings, in
+// three tiers chosen once per group (the lanes of a tier run one branch-free
+// block, so the group's independent values interleave):
+//  * every lane zero or of magnitude in [2^-100, 2^100), the spacings'
+//    correction verified (fast != 0): Markstein's correction, zeros passed
+//    through unchanged (so the sign of zero is kept) -- the steady state;
+//  * some lane below 2^-100 (the numerical precursor ahead of a wavefront),
+//    none huge: mk_div_any, which gives every lane div_c's bits with the
+//    scaled-numerator route selected per lane instead of branched to;
+//  * otherwise (a huge value, or the correction unverified) each value
+//    takes its own route through div_c.
 // The group test, the same predicate as mk_ok on every lane, in three
 // instructions per value: the smallest of 2*bits - 2 (unsigned; a zero of
 // either sign maps to 0xfffffffe, a magnitude below 2^-100 below
 // 2*0x0d800000 - 2) and the largest |x| (NaN is ignored by fmaxf; it stays
-// NaN on either path).
+// NaN on every path).
 struct RangeAcc {
   unsigned lo = 0xffffffffu;
   float hi = 0.f;
@@ -265,6 +266,7 @@ struct RangeAcc {
     hi = fmaxf(hi, fabsf(x));
   }
   __device__ __forceinline__ bool ok() const { return lo >= 2u * 0x0D800000u - 2u && hi < 0x1p100f; }
+  __device__ __forceinline__ bool below_huge() const { return hi < 0x1p100f; }
 };
 
 template <int K, int Q>
@@ -291,14 +293,46 @@ __device__ __forceinline__ void div_group(Vq<Q> (&v)[K], const float (&d)[K], co
 #pragma unroll
         for (int e = 0; e < Q; ++e) s4(v[k], e, mk_div(g4(v[k], e), d[k], r[k]));
     }
+  } else if (fast != 0 && acc.below_huge()) {
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+#pragma unroll
+      for (int e = 0; e < Q; ++e) s4(v[k], e, mk_div_any(g4(v[k], e), d[k], r[k]));
   } else {
-    // some lane of the group is tiny, huge or the path is unverified: each
-    // value takes its own route through div_c (the scaled correction for tiny
-    // values, the double-precision quotient for huge ones)
 #pragma unroll
     for (int k = 0; k < K; ++k)
 #pragma unroll
       for (int e = 0; e < Q; ++e) s4(v[k], e, div_c(g4(v[k], e), d[k], r[k], fast));
+  }
+}
+
+// Exact quotients by per-value positive divisors (densities, CPML kappas) in
+// the same three tiers: IEEE division when every numerator is zero or in
+// [2^-100, 2^100); dv_div_any (div_v's bits, the scaled route selected per
+// lane) when some numerator is smaller, none huge and every divisor lies in
+// [2^-60, 2^60]; otherwise div_v per value.
+template <int K>
+__device__ __forceinline__ void dv_group(float (&x)[K], const float (&d)[K]) {
+  RangeAcc acc;
+#pragma unroll
+  for (int k = 0; k < K; ++k) acc.add(x[k]);
+  if (acc.ok()) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) x[k] = x[k] == 0.f ? x[k] : __fdiv_rn(x[k], d[k]);
+    return;
+  }
+  float dlo = d[0], dhi = d[0];
+#pragma unroll
+  for (int k = 1; k < K; ++k) {
+    dlo = fminf(dlo, d[k]);
+    dhi = fmaxf(dhi, d[k]);
+  }
+  if (acc.below_huge() && dlo >= 0x1p-60f && dhi <= 0x1p60f) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) x[k] = dv_div_any(x[k], d[k]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < K; ++k) x[k] = div_v(x[k], d[k]);
   }
 }
 
@@ -329,12 +363,64 @@ __device__ __forceinline__ float cpml1(float& d, float psi, float b, float aa, f
 // pair's cells (x and y), memory variables o, update mask m
 template <bool EX, int Q>
 __device__ __forceinline__ void cpml_pair(Vq<Q>& d, Vq<Q>& o, const bool (&m)[Q], float b, float aa, float kk) {
+  if constexpr (EX) {
+    // cpml1's arithmetic with the Q quotients by kappa as one group
+    float np[Q], x[Q], kd[Q];
+#pragma unroll
+    for (int e = 0; e < Q; ++e) {
+      const float de = g4(d, e);
+      np[e] = b * g4(o, e) + aa * de;
+      x[e] = m[e] ? de : 0.f;
+      kd[e] = kk;
+    }
+    dv_group<Q>(x, kd);
+#pragma unroll
+    for (int e = 0; e < Q; ++e)
+      if (m[e]) {
+        s4(o, e, np[e]);
+        s4(d, e, x[e] + np[e]);
+      }
+  } else {
+#pragma unroll
+    for (int e = 0; e < Q; ++e)
+      if (m[e]) {
+        float de = g4(d, e);
+        s4(o, e, cpml1<EX>(de, g4(o, e), b, aa, kk));
+        s4(d, e, de);
+      }
+  }
+}
+
+// the z-slab memory variables of one component: the thread's cells e with
+// on[e] (in the z slab and inside the component's update range) advance
+// psi (at m2[zk[e] + off]) with the unit's z table row set at integer (HALF
+// = false) or half points; the quotients by kappa form one group
+template <bool EX, bool HALF, int Q, int TZ>
+__device__ __forceinline__ void cpml_z(Vq<Q>& d, float* m2, long long off, const int (&zk)[Q], const bool (&m)[Q],
+                                       const float* tzt, int kq) {
+  float np[Q], x[Q], kd[Q];
+  bool on[Q];
+#pragma unroll
+  for (int e = 0; e < Q; ++e) {
+    on[e] = zk[e] >= 0 && m[e];
+    const float b = tab(tzt, HALF ? CBH : CB, TZ, kq + e), aa = tab(tzt, HALF ? CAH : CA, TZ, kq + e);
+    const float psi = on[e] ? m2[zk[e] + off] : 0.f;
+    const float de = g4(d, e);
+    np[e] = b * psi + aa * de;
+    x[e] = on[e] ? de : 0.f;
+    kd[e] = on[e] ? tab(tzt, HALF ? CKH : CK, TZ, kq + e) : 1.f;
+  }
+  if constexpr (EX) {
+    dv_group<Q>(x, kd);
+  } else {
+#pragma unroll
+    for (int e = 0; e < Q; ++e) x[e] = __fdividef(x[e], kd[e]);
+  }
 #pragma unroll
   for (int e = 0; e < Q; ++e)
-    if (m[e]) {
-      float de = g4(d, e);
-      s4(o, e, cpml1<EX>(de, g4(o, e), b, aa, kk));
-      s4(d, e, de);
+    if (on[e]) {
+      m2[zk[e] + off] = np[e];
+      s4(d, e, x[e] + np[e]);
     }
 }
 
@@ -761,31 +847,9 @@ k3s_velocity(const __grid_constant__ P3<float> p, const __grid_constant__ Staged
           if (zany) {
             float* m2 = p.mem[2] + ((size_t)i * ny + j) * p.sn[2];
             const long long mc = p.mcomp[2];
-#pragma unroll
-            for (int e = 0; e < Q; ++e)
-              if (zk[e] >= 0) {
-                const int kk = Q * cq + e;
-                const float bi = tab(tzt, CB, G::TZ, kk), ai = tab(tzt, CA, G::TZ, kk),
-                            ki = tab(tzt, CK, G::TZ, kk);
-                const float bh = tab(tzt, CBH, G::TZ, kk), ah = tab(tzt, CAH, G::TZ, kk),
-                            kh = tab(tzt, CKH, G::TZ, kk);
-                float* q0 = m2 + zk[e];
-                if (mx[e]) {
-                  float d = g4(a3, e);
-                  *q0 = cpml1<EX>(d, *q0, bi, ai, ki);
-                  s4(a3, e, d);
-                }
-                if (my[e]) {
-                  float d = g4(b3, e);
-                  q0[mc] = cpml1<EX>(d, q0[mc], bi, ai, ki);
-                  s4(b3, e, d);
-                }
-                if (mz[e]) {
-                  float d = g4(c3, e);
-                  q0[2 * mc] = cpml1<EX>(d, q0[2 * mc], bh, ah, kh);
-                  s4(c3, e, d);
-                }
-              }
+            cpml_z<EX, false, Q, G::TZ>(a3, m2, 0, zk, mx, tzt, Q * cq);
+            cpml_z<EX, false, Q, G::TZ>(b3, m2, mc, zk, my, tzt, Q * cq);
+            cpml_z<EX, true, Q, G::TZ>(c3, m2, 2 * mc, zk, mz, tzt, Q * cq);
           }
           // numerators and densities of the 3Q updates, then their quotients
           // as one group (no per-lane range branch); masked cells keep their value
@@ -814,16 +878,7 @@ k3s_velocity(const __grid_constant__ P3<float> p, const __grid_constant__ Staged
             }
           }
           if (EX) {
-            RangeAcc acc;
-#pragma unroll
-            for (int q = 0; q < 3 * Q; ++q) acc.add(tn[q]);
-            if (acc.ok()) {
-#pragma unroll
-              for (int q = 0; q < 3 * Q; ++q) tn[q] = tn[q] == 0.f ? tn[q] : __fdiv_rn(tn[q], td[q]);
-            } else {
-#pragma unroll
-              for (int q = 0; q < 3 * Q; ++q) tn[q] = div_v(tn[q], td[q]);
-            }
+            dv_group<3 * Q>(tn, td);
           } else {
 #pragma unroll
             for (int q = 0; q < 3 * Q; ++q) tn[q] = __fdividef(tn[q], td[q]);
@@ -1097,31 +1152,9 @@ k3s_stress(const __grid_constant__ P3<float> p, const __grid_constant__ StagedMa
           if (zany) {
             const long long mc = p.mcomp[2];
             float* m2 = p.mem[2] + 3 * mc + ((size_t)i * ny + j) * p.sn[2];
-#pragma unroll
-            for (int e = 0; e < Q; ++e)
-              if (zk[e] >= 0) {
-                const int kk = Q * cq + e;
-                const float bi = tab(tzt, CB, G::TZ, kk), ai = tab(tzt, CA, G::TZ, kk),
-                            ki = tab(tzt, CK, G::TZ, kk);
-                const float bh = tab(tzt, CBH, G::TZ, kk), ah = tab(tzt, CAH, G::TZ, kk),
-                            khz = tab(tzt, CKH, G::TZ, kk);
-                float* q0 = m2 + zk[e];
-                if (mn[e]) {  // dvz_dz
-                  float d = g4(e3, e);
-                  *q0 = cpml1<EX>(d, *q0, bi, ai, ki);
-                  s4(e3, e, d);
-                }
-                if (mxz[e]) {  // dvx_dz
-                  float d = g4(h2, e);
-                  q0[mc] = cpml1<EX>(d, q0[mc], bh, ah, khz);
-                  s4(h2, e, d);
-                }
-                if (myz[e]) {  // dvy_dz
-                  float d = g4(q2, e);
-                  q0[2 * mc] = cpml1<EX>(d, q0[2 * mc], bh, ah, khz);
-                  s4(q2, e, d);
-                }
-              }
+            cpml_z<EX, false, Q, G::TZ>(e3, m2, 0, zk, mn, tzt, Q * cq);      // dvz_dz
+            cpml_z<EX, true, Q, G::TZ>(h2, m2, mc, zk, mxz, tzt, Q * cq);     // dvx_dz
+            cpml_z<EX, true, Q, G::TZ>(q2, m2, 2 * mc, zk, myz, tzt, Q * cq); // dvy_dz
           }
           if constexpr (packed<EX, Q>()) {
             const float2 dt2 = sp2(dt), half = sp2(0.5f), quarter = sp2(0.25f);

@@ -227,6 +227,42 @@ __device__ __forceinline__ float mk_div_tiny(float x, float d, float r) {
   return tiny_finish(xs, mk_core(xs, d, r), d);
 }
 
+// tiny_finish without branches (both outcomes computed, one selected), for
+// groups whose lanes take different routes
+__device__ __forceinline__ float tiny_finish_sel(float xs, float ys, float d) {
+  const float t = __fmul_rn(ys, 0x1p85f);
+  const float fl = floorf(t);
+  const bool mid = fabsf(__fadd_rn(t, -truncf(t))) == 0.5f;
+  const float res = __fmaf_rn(-ys, d, xs);
+  float n = rintf(t);
+  n = mid && res > 0.f ? __fadd_rn(fl, 1.f) : n;
+  n = mid && res < 0.f ? fl : n;
+  return fabsf(ys) >= 0x1p-62f ? __fmul_rn(ys, 0x1p-64f) : __fmul_rn(n, 0x1p-149f);
+}
+
+// div_c's result with a verified correction (fast != 0) for any |x| < 2^100
+// -- zero, below 2^-100 or in [2^-100, 2^100) -- without a branch
+__device__ __forceinline__ float mk_div_any(float x, float d, float r) {
+  const unsigned u = __float_as_uint(x) & 0x7fffffffu;
+  const bool tiny = u < 0x0D800000u;  // |x| < 2^-100, zero included
+  const float xs = tiny ? __fmul_rn(x, 0x1p64f) : x;
+  const float q = mk_core(xs, d, r);
+  const float y = tiny ? tiny_finish_sel(xs, q, d) : q;
+  return u == 0u ? x : y;
+}
+
+// div_v's result for |x| < 2^100 and d in [2^-60, 2^60] without a branch (a
+// zero numerator divides 1 instead, so the division stays on its fast path,
+// and passes through)
+__device__ __forceinline__ float dv_div_any(float x, float d) {
+  const unsigned u = __float_as_uint(x) & 0x7fffffffu;
+  const bool tiny = u < 0x0D800000u;
+  const float xs = u == 0u ? 1.f : (tiny ? __fmul_rn(x, 0x1p64f) : x);
+  const float q = __fdiv_rn(xs, d);
+  const float y = tiny ? tiny_finish_sel(xs, q, d) : q;
+  return u == 0u ? x : y;
+}
+
 // x / d for a divisor fixed for the run (dx, dy, dz), r = RN(1/d).  With
 // fast != 0 (float only) numerators of magnitude in [2^-100, 2^100) use
 // Markstein's correction

@@ -136,9 +136,11 @@ def test_per_cell_quotient_equals_ieee_for_every_numerator(cuda, d):
     equals IEEE division for all 2^32 float numerators."""
     from seiswave_taichi_b200 import _native as N
     assert N.check_division(d, 1) == 0
+    assert N.check_division(d, 3) == 0
 
 
 @pytest.mark.parametrize("h", [10.0, 12.5, 2.5])
 def test_spacing_quotient_equals_ieee_for_every_numerator(cuda, h):
     from seiswave_taichi_b200 import _native as N
     assert N.check_division(h, 0) == 0
+    assert N.check_division(h, 2) == 0

@@ -57,6 +57,17 @@ def test_bad_descriptors_fail_before_any_device_call():
     assert lib.sw_plan_destroy(None) == N.SW_OK
 
 
+def test_division_check_arguments_fail_before_any_device_call():
+    lib = N.load()
+    out = C.c_uint64(7)
+    for divisor, mode, what in ((10.0, 4, b"mode"), (10.0, -1, b"mode"), (0.0, 0, b"positive"),
+                                (float("inf"), 1, b"positive"), (2.0 ** 70, 3, b"2^60")):
+        assert lib.sw_check_division(C.c_float(divisor), mode, C.byref(out), None) == N.SW_ERR_ARG
+        assert what in lib.sw_last_error()
+    assert lib.sw_check_division(C.c_float(10.0), 0, None, None) == N.SW_ERR_ARG
+    assert out.value == 7
+
+
 def test_check_raises_with_message():
     lib = N.load()
     lib.sw3d_plan_create(None, C.byref(C.c_void_p()))
