@@ -599,7 +599,9 @@ def run_thin_layer(args, rank, world, local):
     vp, vs, rho = layered((n, n, n), 2000.0, 5000.0, nlayers=8, seed=rank, anomaly=0.05)
     h, dt, f0 = 10.0, 8e-4, 12.0
     out = {}
-    for tag, P, npml in (("cpml20", pad20, 20), ("learned6", pad6, 6)):
+    # thin6: the 6-cell layer without its network corrections, which bounds
+    # what any correction kernel could reach (its cost taken as zero)
+    for tag, P, npml in (("cpml20", pad20, 20), ("learned6", pad6, 6), ("thin6", pad6, 6)):
         m = [np.pad(a, P, mode="edge") for a in (vp, vs, rho)]
         c = m[0].shape[0] // 2
         w = LA.solver3d(*m, h, dt, c, c, c, nt, npml=npml, freq=f0)
@@ -646,10 +648,13 @@ def run_thin_layer(args, rank, world, local):
                        "grids": {"cpml20": n + 2 * pad20, "learned6": n + 2 * pad6}, "time_steps": nt},
             "shots_per_s": {"learned6": 1e3 / out["learned6"], "cpml20": 1e3 / out["cpml20"]},
             "learned_over_cpml20": out["cpml20"] / out["learned6"],
+            "bound_free_correction": {"thin6_shots_per_s": 1e3 / out["thin6"],
+                                      "cpml20_over_thin6": out["cpml20"] / out["thin6"],
+                                      "what": "the 6-cell grid stepped without the network corrections"},
             "fp64_error": out.get("fp64"),
             "note": "shots run one after the other (no 3D shot batching); error gate measured on small grids "
                     "in tests/test_learned_abc3d.py",
-            "gpu_launches": args.steps * (2 * nt + 2 * nt + 1),
+            "gpu_launches": args.steps * (2 * nt + 2 * nt + 1 + 2 * nt),
         }
         print(json.dumps(line), flush=True)
     return 0

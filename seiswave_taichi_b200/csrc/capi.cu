@@ -147,7 +147,7 @@ struct sw_plan {
   bool staged = false;
   sw::StagedMaps svm{}, ssm{};
   sw::StagedArgs sa{};
-  int staged_grid = 0, staged_N = 0, staged_tz = 32;
+  int staged_N = 0, staged_tz = 32;
   // 0: register-queue two-pass kernels (2D: two launches per step), 1: staged
   // two-pass, 2: fused single pass, 3: 2D persistent (one cooperative launch
   // per run)
@@ -544,13 +544,6 @@ void staged_chunks(sw_plan* pl, int len) {
   if (len < 2 * pl->staged_N + 2) len = 2 * pl->staged_N + 2;
   a.chunk_len = len;
   a.chunks = (p.nx + len - 1) / len;
-  int dev = 0, maxsm = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
-  const size_t big = sc.vel_smem > sc.str_smem ? sc.vel_smem : sc.str_smem;
-  int per_sm = (int)((size_t)maxsm / (big + 1024));
-  if (per_sm < 1) per_sm = 1;
-  pl->staged_grid = units_grid(a.tiles_y * a.tiles_z * a.chunks, per_sm);
 }
 
 void setup_staged(sw_plan* pl) {
@@ -818,7 +811,16 @@ int sw_plan_info(sw_plan* pl, int32_t* info) {
   info[0] = pl->path;
   info[1] = pl->dim == 3 ? (pl->dtype == SW_F32 ? pl->p3f.fast_div : 0) : (pl->dtype == SW_F32 ? pl->p2f.fast_div : 0);
   info[2] = pl->staged ? 1 : 0;
-  info[3] = pl->staged ? pl->staged_grid : 0;
+  info[3] = 0;
+  if (pl->staged) {
+    // the velocity pass's grid (the occupancy of the numerics in use)
+    int gv = 0, gs = 0;
+    const bool spml = pl->scheme == SW3D_SPML, tensor = pl->scheme == SW3D_CPML_TENSOR;
+    if (sw::sw3_staged_grid(pl->staged_N, pl->staged_tz, spml, tensor, pl->sa.exact != 0,
+                            pl->sa.tiles_y * pl->sa.tiles_z * pl->sa.chunks, &gv, &gs) == cudaSuccess)
+      info[3] = gv;
+    cudaGetLastError();
+  }
   info[4] = pl->staged ? pl->sa.chunk_len : 0;
   info[5] = pl->fused ? 1 : 0;
   info[6] = pl->fused ? pl->fused_grid : 0;

@@ -1439,4 +1439,26 @@ cudaError_t sw3_staged_step(int N, int tz, bool spml, bool tensor, const P3<floa
   return cudaErrorInvalidValue;
 }
 
+template <int N, int TY, int D, int TZ, bool EX, int SCH>
+static cudaError_t staged_grid_t(bool tensor, int units, int* vel, int* str) {
+  StagedOcc o;
+  cudaError_t e = staged_setup<N, TY, D, TZ, EX, SCH>(tensor, &o);
+  if (e != cudaSuccess) return e;
+  *vel = units < o.sms * o.vel ? units : o.sms * o.vel;
+  *str = units < o.sms * o.str ? units : o.sms * o.str;
+  return cudaSuccess;
+}
+
+cudaError_t sw3_staged_grid(int N, int tz, bool spml, bool tensor, bool exact, int units, int* vel, int* str) {
+#define SW_GRID(a_, b, c, d)                                                                \
+  {                                                                                         \
+    if (spml) return staged_grid_t<a_, b, c, d, true, SCH_SPML>(false, units, vel, str);    \
+    return exact ? staged_grid_t<a_, b, c, d, true, SCH_CPML>(tensor, units, vel, str)      \
+                 : staged_grid_t<a_, b, c, d, false, SCH_CPML>(tensor, units, vel, str);    \
+  }
+  SW_STAGED_SWITCH(N, tz, SW_GRID)
+#undef SW_GRID
+  return cudaErrorInvalidValue;
+}
+
 }  // namespace sw

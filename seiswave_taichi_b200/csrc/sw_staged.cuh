@@ -34,5 +34,7 @@ bool sw3_staged_maps(int N, int tz, const P3<float>& p, StagedMaps* vel, StagedM
 cudaError_t sw3_staged_step(int N, int tz, bool spml, bool tensor, const P3<float>& p, const StagedMaps& vel,
                             const StagedMaps& str, const StagedArgs& a, int it, bool force_here, bool inject_next,
                             bool gather, cudaStream_t st);
+// the CTAs sw3_staged_step launches for each pass over `units` work units
+cudaError_t sw3_staged_grid(int N, int tz, bool spml, bool tensor, bool exact, int units, int* vel, int* str);
 
 }  // namespace sw
