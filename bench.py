@@ -46,7 +46,7 @@ FALLBACK_HBM_GBS = 6650.0
 SEGY_NCU_TRAFFIC = (525.916672 + 482.566656) * 1e6
 # DRAM bytes per time step (velocity + stress launch pair at step 700, default
 # path and exact numerics) from one ncu capture of the full workload (profiles/).
-NCU_TRAFFIC_PER_STEP = {"3d-ssg-cpml-tensor-200^3-nt1000": (418.751744 + 123.215104 + 460.371968 + 207.120384) * 1e6}
+NCU_TRAFFIC_PER_STEP = {"3d-ssg-cpml-tensor-200^3-nt1000": (406.525952 + 122.243584 + 450.126080 + 207.585792) * 1e6}
 
 
 def peaks():
