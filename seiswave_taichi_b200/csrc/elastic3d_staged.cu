@@ -424,6 +424,28 @@ __device__ __forceinline__ void cpml_z(Vq<Q>& d, float* m2, long long off, const
     }
 }
 
+// L2 prefetch of the memory variables (components c0 .. c0+2 of each slab
+// axis) that cell quad (j, k) updates in plane i: issued one plane ahead,
+// these loads are the slab cells' longest waits
+template <int Q>
+__device__ __forceinline__ void prefetch_memvars(const P3<float>& p, int i, int j, int k, int c0, int yj,
+                                                 const int (&zk)[Q], bool zany) {
+  const int xn = slab_index(i, p.nx, p.lo[0], p.hi[0]);
+  if (xn >= 0) {
+    const float* b = p.mem[0] + c0 * p.mcomp[0] + ((size_t)xn * p.ny + j) * p.nz + k;
+    for (int c = 0; c < 3; ++c) prefetch_l2(b + c * p.mcomp[0]);
+  }
+  if (yj >= 0) {
+    const float* b = p.mem[1] + c0 * p.mcomp[1] + ((size_t)i * p.sn[1] + yj) * p.nz + k;
+    for (int c = 0; c < 3; ++c) prefetch_l2(b + c * p.mcomp[1]);
+  }
+  if (zany) {
+    const int ze = zk[0] >= 0 ? zk[0] : zk[Q - 1];
+    const float* b = p.mem[2] + c0 * p.mcomp[2] + ((size_t)i * p.ny + j) * p.sn[2] + ze;
+    for (int c = 0; c < 3; ++c) prefetch_l2(b + c * p.mcomp[2]);
+  }
+}
+
 // per-unit CPML table of the tile's rows (y) or z cells: row q of the axis
 // coefficient table (b, a, kappa at integer points, then at half points)
 __device__ __forceinline__ float tab(const float* t, int row, int len, int at) { return t[row * len + at]; }
@@ -763,6 +785,8 @@ k3s_velocity(const __grid_constant__ P3<float> p, const __grid_constant__ Staged
       }
 #endif
       const int xi = SCH == SCH_CPML ? slab_index(i, nx, p.lo[0], p.hi[0]) : -1;
+      if constexpr (SCH == SCH_CPML)
+        if (jin && kin && i + 1 < x1) prefetch_memvars(p, i + 1, j, k, 0, yj, zk, zany);
       if (jin && kin) {
         const float* pxx[2 * N];
         const float* pxy[2 * N];
@@ -1058,6 +1082,8 @@ k3s_stress(const __grid_constant__ P3<float> p, const __grid_constant__ StagedMa
       }
 #endif
       const int xi = SCH == SCH_CPML ? slab_index(i, nx, p.lo[0], p.hi[0]) : -1;
+      if constexpr (SCH == SCH_CPML)
+        if (jin && kin && i + 1 < x1) prefetch_memvars(p, i + 1, j, k, 3, yj, zk, zany);
       const bool src = inject_next && i == p.si && p.sj == j && p.sk >= k && p.sk < k + Q;
       if (jin && kin) {
         const float* pvx[2 * N];  // vx planes i-N .. i+N-1  (Dx3bm)
