@@ -46,7 +46,7 @@ FALLBACK_HBM_GBS = 6650.0
 SEGY_NCU_TRAFFIC = (525.916672 + 482.566656) * 1e6
 # DRAM bytes per time step (velocity + stress launch pair at step 700, default
 # path and exact numerics) from one ncu capture of the full workload (profiles/).
-NCU_TRAFFIC_PER_STEP = {"3d-ssg-cpml-tensor-200^3-nt1000": (406.525952 + 122.243584 + 450.126080 + 207.585792) * 1e6}
+NCU_TRAFFIC_PER_STEP = {"3d-ssg-cpml-tensor-200^3-nt1000": (435.430144 + 125.214464 + 483.239680 + 209.421568) * 1e6}
 
 
 def peaks():
@@ -733,7 +733,8 @@ def main(argv=None):
     alg = algorithmic_bytes(cfg)
     ms_per_tstep = ms_step / nt
     achieved = alg / (ms_per_tstep * 1e-3) / 1e9
-    traffic = NCU_TRAFFIC_PER_STEP.get(cfg["name"])
+    # the captured traffic belongs to the plan's default path (the staged passes)
+    traffic = NCU_TRAFFIC_PER_STEP.get(cfg["name"]) if not args.path else None
 
     # end to end through the public API with host buffers
     pin = {k: torch.from_numpy(np.ascontiguousarray(cfg[k])).pin_memory() for k in ("vp", "vs", "rho")}
