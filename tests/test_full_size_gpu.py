@@ -2,10 +2,13 @@
 
 * 2D homogeneous P-SV, 400^2, 1000 steps (explosive source, 200 receivers):
   the whole loop equals the oracle bit for bit.
-* 3D double couple, 200^3, 1000 steps, and 3D heterogeneous thrust belt,
-  400x400x200, 2000 steps: the oracle cannot run these loops in a test's
-  time, so the first steps on the full grid are compared with it bit for bit
-  (all host cores), and the whole loop by exact and by tolerance properties:
+* 3D double couple, 200^3, 1000 steps: the whole loop against the oracle
+  bit for bit (about a minute on 16 host cores), fields and traces.
+* 3D heterogeneous thrust belt, 400x400x200, 2000 steps: the oracle cannot
+  run this loop in a test's time, so its first 160 steps on the full grid
+  are compared with it bit for bit (all host cores).
+* For both 3D workloads the whole loop is also checked by exact and by
+  tolerance properties:
   - the TMA-staged kernels (the default path) equal the plain two-pass
     kernels, an independent implementation of the same IEEE operations that
     the small-grid tests check against the oracle, bit for bit over the whole
@@ -96,7 +99,7 @@ def test_2d_full_loop_equals_oracle(cuda):
     assert np.abs(o.data).max() > 0
 
 
-@pytest.mark.parametrize("which,steps", [("config2", 120), ("config3", 24)])
+@pytest.mark.parametrize("which,steps", [("config2", 1000), ("config3", 160)])
 def test_3d_full_grid(cuda, which, steps):
     from seiswave_taichi_b200 import synthetic as S
     cfg = getattr(S, which)()
@@ -114,7 +117,8 @@ def test_3d_full_grid(cuda, which, steps):
     _eq("data", _np(w.data)[:steps], o.data[:steps])
     del o
     # the whole loop on the staged path
-    w.run(nt - steps, it0=steps)
+    if nt > steps:
+        w.run(nt - steps, it0=steps)
     plan.status()
     ref = {f: _np(getattr(w, f)) for f in F3}
     ref["data"] = _np(w.data)
