@@ -448,9 +448,11 @@ __device__ __forceinline__ void prefetch_memvars(const P3<float>& p, int i, int 
   }
 }
 
-// L2 prefetch of the split fields (components c0 .. c0+nc-1) of cell quad
+// L1 prefetch of the split fields (components c0 .. c0+nc-1) of cell quad
 // (j, k) in plane i, where the quad's first or last cell lies in the PML
-// shell (the split-field scheme's counterpart of prefetch_memvars)
+// shell, issued one plane ahead (the split-field scheme's counterpart of
+// prefetch_memvars; measured at 200^3: 6.37 Gcell/s against 6.03 with an L2
+// prefetch two planes ahead and 5.85 without)
 template <int Q>
 __device__ __forceinline__ void prefetch_split(const P3<float>& p, int i, int j, int k, int c0, int nc, uint8_t fy,
                                                const uint8_t (&fz)[Q]) {
@@ -458,7 +460,7 @@ __device__ __forceinline__ void prefetch_split(const P3<float>& p, int i, int j,
   const int e = (fx | fy | fz[0]) ? 0 : Q - 1;
   if (fx | fy | fz[e]) {
     const float* b = p.split + c0 * p.scomp + shell_index(p, i, j, k + e);
-    for (int c = 0; c < nc; ++c) prefetch_l2(b + c * p.scomp);
+    for (int c = 0; c < nc; ++c) prefetch_l1(b + c * p.scomp);
   }
 }
 
@@ -804,7 +806,7 @@ k3s_velocity(const __grid_constant__ P3<float> p, const __grid_constant__ Staged
       if constexpr (SCH == SCH_CPML)
         if (jin && kin && i + 2 < x1) prefetch_memvars(p, i + 2, j, k, 0, yj, zk, zany);
       if constexpr (SCH == SCH_SPML)
-        if (jin && kin && i + 2 < x1) prefetch_split(p, i + 2, j, k, PVX_X, 9, fy, fz);
+        if (jin && kin && i + 1 < x1) prefetch_split(p, i + 1, j, k, PVX_X, 9, fy, fz);
       if (jin && kin) {
         const float* pxx[2 * N];
         const float* pxy[2 * N];
@@ -1103,7 +1105,7 @@ k3s_stress(const __grid_constant__ P3<float> p, const __grid_constant__ StagedMa
       if constexpr (SCH == SCH_CPML)
         if (jin && kin && i + 2 < x1) prefetch_memvars(p, i + 2, j, k, 3, yj, zk, zany);
       if constexpr (SCH == SCH_SPML)
-        if (jin && kin && i + 2 < x1) prefetch_split(p, i + 2, j, k, PSXX_X, 15, fy, fz);
+        if (jin && kin && i + 1 < x1) prefetch_split(p, i + 1, j, k, PSXX_X, 15, fy, fz);
       const bool src = inject_next && i == p.si && p.sj == j && p.sk >= k && p.sk < k + Q;
       if (jin && kin) {
         const float* pvx[2 * N];  // vx planes i-N .. i+N-1  (Dx3bm)
