@@ -303,14 +303,26 @@ __device__ __forceinline__ float mk_div(float x, float d, float r) {
   const float y = __fmaf_rn(e, r, q);
   return x == 0.f ? x : y;
 }
+// Three tiers, chosen once per group: every lane zero or in [2^-100, 2^100)
+// (the steady state); some lane smaller, none of magnitude 2^100 or more
+// (the numerical precursor ahead of a wavefront): every lane runs the scaled
+// float route and selects its result (mk_div_any, dv_div_any); otherwise the
+// double-precision quotient.  Each tier gives every lane div_c's / div_v's
+// bits.
 template <int K>
 __device__ __forceinline__ void divc_group(float (&x)[K], const float (&d)[K], const float (&r)[K], int fast) {
-  bool ok = fast != 0;
+  bool ok = fast != 0, small = fast != 0;
 #pragma unroll
-  for (int k = 0; k < K; ++k) ok = ok & mk_ok(x[k]);
+  for (int k = 0; k < K; ++k) {
+    ok = ok & mk_ok(x[k]);
+    small = small & (fabsf(x[k]) < 0x1p100f);
+  }
   if (ok) {
 #pragma unroll
     for (int k = 0; k < K; ++k) x[k] = mk_div(x[k], d[k], r[k]);
+  } else if (small) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) x[k] = mk_div_any(x[k], d[k], r[k]);
   } else {
 #pragma unroll
     for (int k = 0; k < K; ++k) x[k] = dd_div(x[k], d[k]);
@@ -324,12 +336,18 @@ __device__ __forceinline__ void divc_group(double (&x)[K], const double (&d)[K],
 // quotients by per-cell positive divisors (densities), grouped likewise
 template <int K>
 __device__ __forceinline__ void divv_group(float (&x)[K], const float (&d)[K]) {
-  bool ok = true;
+  bool ok = true, small = true;
 #pragma unroll
-  for (int k = 0; k < K; ++k) ok = ok & mk_ok(x[k]);
+  for (int k = 0; k < K; ++k) {
+    ok = ok & mk_ok(x[k]);
+    small = small & (fabsf(x[k]) < 0x1p100f) & (d[k] >= 0x1p-60f) & (d[k] <= 0x1p60f);
+  }
   if (ok) {
 #pragma unroll
     for (int k = 0; k < K; ++k) x[k] = x[k] == 0.f ? x[k] : __fdiv_rn(x[k], d[k]);
+  } else if (small) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) x[k] = dv_div_any(x[k], d[k]);
   } else {
 #pragma unroll
     for (int k = 0; k < K; ++k) x[k] = dd_div(x[k], d[k]);
