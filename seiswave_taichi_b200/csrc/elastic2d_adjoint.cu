@@ -105,6 +105,10 @@ k2a_stress_mid(const __grid_constant__ P2<T> p, const __grid_constant__ A2<T> a)
   if (i >= nx || j >= nz) return;
   const long long idx = (long long)i * nz + j;
   const T dx = p.dx, dz = p.dz, dt = p.dt;
+  // quotients by the spacings: the verified constant-divisor route (the
+  // forward pass's bits, IEEE division's bits)
+  auto qdx = [&](T v) { return div_c(v, dx, p.rd[0], p.fast_div & 1); };
+  auto qdz = [&](T v) { return div_c(v, dz, p.rd[1], p.fast_div & 1); };
   T c[N];
 #pragma unroll
   for (int m = 0; m < N; ++m) c[m] = p.c[m];
@@ -122,8 +126,8 @@ k2a_stress_mid(const __grid_constant__ P2<T> p, const __grid_constant__ A2<T> a)
     const T lhx = (T)0.5 * (p.lam[idx] + p.lam[idx + nz]);
     const T mhx = (T)0.5 * (p.mu[idx] + p.mu[idx + nz]);
     const T lpm = lhx + (T)2 * mhx;
-    T pv = dx_fm<T, N>(vx, idx, nz, c) / dx;
-    T qv = dz_bm<T, N>(vz, idx, c) / dz;
+    T pv = qdx(dx_fm<T, N>(vx, idx, nz, c));
+    T qv = qdz(dz_bm<T, N>(vz, idx, c));
     const bool P = (fx & 2) || (fz & 1);
     const T bxh = cfx[CBH * nx + i], axh = cfx[CAH * nx + i], kxh = cfx[CKH * nx + i];
     const T bz = cfz[CB * nz + j], az = cfz[CA * nz + j], kz = cfz[CK * nz + j];
@@ -136,14 +140,14 @@ k2a_stress_mid(const __grid_constant__ P2<T> p, const __grid_constant__ A2<T> a)
     T qb = dt * (lhx * sb + lpm * zb);
     if (P && xi >= 0) pb = pml_adj(pb, amx(p, a, 2, xi, j), bxh, axh, kxh);
     if (P && zj >= 0) qb = pml_adj(qb, amz(p, a, 2, i, zj), bz, az, kz);
-    t0 = pb / dx;
-    t1 = qb / dz;
+    t0 = qdx(pb);
+    t1 = qdz(qb);
   }
   // sxz at (i, j+1/2)
   if (i >= N + 1 && i < nx - N && j >= N && j < nz - N - 1) {
     const T mhz = (T)0.5 * (p.mu[idx + 1] + p.mu[idx]);
-    T rv = dx_bm<T, N>(vz, idx, nz, c) / dx;
-    T uv = dz_fm<T, N>(vx, idx, c) / dz;
+    T rv = qdx(dx_bm<T, N>(vz, idx, nz, c));
+    T uv = qdz(dz_fm<T, N>(vx, idx, c));
     const bool P = (fx & 1) || (fz & 2);
     const T bx = cfx[CB * nx + i], ax = cfx[CA * nx + i], kx = cfx[CK * nx + i];
     const T bzh = cfz[CBH * nz + j], azh = cfz[CAH * nz + j], kzh = cfz[CKH * nz + j];
@@ -155,8 +159,8 @@ k2a_stress_mid(const __grid_constant__ P2<T> p, const __grid_constant__ A2<T> a)
     T ub = sb, rb = sb;
     if (P && xi >= 0) rb = pml_adj(rb, amx(p, a, 3, xi, j), bx, ax, kx);
     if (P && zj >= 0) ub = pml_adj(ub, amz(p, a, 3, i, zj), bzh, azh, kzh);
-    t2 = ub / dz;
-    t3 = rb / dx;
+    t2 = qdz(ub);
+    t3 = qdx(rb);
   }
   a.tmp[0][idx] = t0;
   a.tmp[1][idx] = t1;
@@ -196,6 +200,10 @@ k2a_vel_mid(const __grid_constant__ P2<T> p, const __grid_constant__ A2<T> a) {
   if (i >= nx || j >= nz) return;
   const long long idx = (long long)i * nz + j;
   const T dx = p.dx, dz = p.dz, dt = p.dt;
+  // quotients by the spacings: the verified constant-divisor route (the
+  // forward pass's bits, IEEE division's bits)
+  auto qdx = [&](T v) { return div_c(v, dx, p.rd[0], p.fast_div & 1); };
+  auto qdz = [&](T v) { return div_c(v, dz, p.rd[1], p.fast_div & 1); };
   T c[N];
 #pragma unroll
   for (int m = 0; m < N; ++m) c[m] = p.c[m];
@@ -212,8 +220,8 @@ k2a_vel_mid(const __grid_constant__ P2<T> p, const __grid_constant__ A2<T> a) {
   T t0 = 0, t1 = 0, t2 = 0, t3 = 0;
   // vx at (i, j)
   if (i >= N + 1 && i < nx - N && j >= N + 1 && j < nz - N) {
-    T av = dx_bm<T, N>(sxx, idx, nz, c) / dx;
-    T bv = dz_bm<T, N>(sxz, idx, c) / dz;
+    T av = qdx(dx_bm<T, N>(sxx, idx, nz, c));
+    T bv = qdz(dz_bm<T, N>(sxz, idx, c));
     const bool P = (fx & 1) || (fz & 1);
     const T bx = cfx[CB * nx + i], ax = cfx[CA * nx + i], kx = cfx[CK * nx + i];
     const T bz = cfz[CB * nz + j], az = cfz[CA * nz + j], kz = cfz[CK * nz + j];
@@ -225,14 +233,14 @@ k2a_vel_mid(const __grid_constant__ P2<T> p, const __grid_constant__ A2<T> a) {
     T ab = sb, bb = sb;
     if (P && xi >= 0) ab = pml_adj(ab, amx(p, a, 0, xi, j), bx, ax, kx);
     if (P && zj >= 0) bb = pml_adj(bb, amz(p, a, 0, i, zj), bz, az, kz);
-    t0 = ab / dx;
-    t1 = bb / dz;
+    t0 = qdx(ab);
+    t1 = qdz(bb);
   }
   // vz at (i+1/2, j+1/2)
   if (i >= N && i < nx - N - 1 && j >= N && j < nz - N - 1) {
     const T rh = (T)0.25 * (rho[idx] + rho[idx + 1] + rho[idx + nz + 1] + rho[idx + nz]);
-    T av = dx_fm<T, N>(sxz, idx, nz, c) / dx;
-    T bv = dz_fm<T, N>(szz, idx, c) / dz;
+    T av = qdx(dx_fm<T, N>(sxz, idx, nz, c));
+    T bv = qdz(dz_fm<T, N>(szz, idx, c));
     const bool P = (fx & 2) || (fz & 2);
     const T bxh = cfx[CBH * nx + i], axh = cfx[CAH * nx + i], kxh = cfx[CKH * nx + i];
     const T bzh = cfz[CBH * nz + j], azh = cfz[CAH * nz + j], kzh = cfz[CKH * nz + j];
@@ -244,8 +252,8 @@ k2a_vel_mid(const __grid_constant__ P2<T> p, const __grid_constant__ A2<T> a) {
     T ab = sb, bb = sb;
     if (P && xi >= 0) ab = pml_adj(ab, amx(p, a, 1, xi, j), bxh, axh, kxh);
     if (P && zj >= 0) bb = pml_adj(bb, amz(p, a, 1, i, zj), bzh, azh, kzh);
-    t2 = ab / dx;
-    t3 = bb / dz;
+    t2 = qdx(ab);
+    t3 = qdz(bb);
   }
   a.tmp[0][idx] = t0;
   a.tmp[1][idx] = t1;
@@ -298,6 +306,10 @@ k2a_sv_stress_mid(const __grid_constant__ P2<T> p, const __grid_constant__ A2<T>
   if (i >= nx || j >= nz) return;
   const long long idx = (long long)i * nz + j;
   const T dx = p.dx, dz = p.dz, dt = p.dt;
+  // quotients by the spacings: the verified constant-divisor route (the
+  // forward pass's bits, IEEE division's bits)
+  auto qdx = [&](T v) { return div_c(v, dx, p.rd[0], p.fast_div & 1); };
+  auto qdz = [&](T v) { return div_c(v, dz, p.rd[1], p.fast_div & 1); };
   T c[N];
 #pragma unroll
   for (int m = 0; m < N; ++m) c[m] = p.c[m];
@@ -315,8 +327,8 @@ k2a_sv_stress_mid(const __grid_constant__ P2<T> p, const __grid_constant__ A2<T>
     {
       const T lm = p.lam[idx];
       const T lpm = p.lam[idx] + (T)2 * p.mu[idx];
-      T pv = dx_bm<T, N>(vx, idx, nz, c) / dx;
-      T qv = dz_bm<T, N>(vz, idx, c) / dz;
+      T pv = qdx(dx_bm<T, N>(vx, idx, nz, c));
+      T qv = qdz(dz_bm<T, N>(vz, idx, c));
       const bool P = (fx & 1) || (fz & 1);
       const T bx = cfx[CB * nx + i], ax = cfx[CA * nx + i], kx = cfx[CK * nx + i];
       const T bz = cfz[CB * nz + j], az = cfz[CA * nz + j], kz = cfz[CK * nz + j];
@@ -329,14 +341,14 @@ k2a_sv_stress_mid(const __grid_constant__ P2<T> p, const __grid_constant__ A2<T>
       T qb = dt * (lm * sb + lpm * zb);
       if (P && xi >= 0) pb = pml_adj(pb, amx(p, a, 2, xi, j), bx, ax, kx);
       if (P && zj >= 0) qb = pml_adj(qb, amz(p, a, 2, i, zj), bz, az, kz);
-      t0 = pb / dx;
-      t1 = qb / dz;
+      t0 = qdx(pb);
+      t1 = qdz(qb);
     }
     // sxz at (i+1/2, j+1/2)
     {
       const T m4 = (T)0.25 * (p.mu[idx + 1] + p.mu[idx] + p.mu[idx + nz + 1] + p.mu[idx + nz]);
-      T rv = dx_fm<T, N>(vz, idx, nz, c) / dx;
-      T uv = dz_fm<T, N>(vx, idx, c) / dz;
+      T rv = qdx(dx_fm<T, N>(vz, idx, nz, c));
+      T uv = qdz(dz_fm<T, N>(vx, idx, c));
       const bool P = (fx & 2) || (fz & 2);
       const T bxh = cfx[CBH * nx + i], axh = cfx[CAH * nx + i], kxh = cfx[CKH * nx + i];
       const T bzh = cfz[CBH * nz + j], azh = cfz[CAH * nz + j], kzh = cfz[CKH * nz + j];
@@ -348,8 +360,8 @@ k2a_sv_stress_mid(const __grid_constant__ P2<T> p, const __grid_constant__ A2<T>
       T ub = sb, rb = sb;
       if (P && xi >= 0) rb = pml_adj(rb, amx(p, a, 3, xi, j), bxh, axh, kxh);
       if (P && zj >= 0) ub = pml_adj(ub, amz(p, a, 3, i, zj), bzh, azh, kzh);
-      t2 = ub / dz;
-      t3 = rb / dx;
+      t2 = qdz(ub);
+      t3 = qdx(rb);
     }
   }
   a.tmp[0][idx] = t0;
@@ -389,6 +401,10 @@ k2a_sv_vel_mid(const __grid_constant__ P2<T> p, const __grid_constant__ A2<T> a)
   if (i >= nx || j >= nz) return;
   const long long idx = (long long)i * nz + j;
   const T dx = p.dx, dz = p.dz, dt = p.dt;
+  // quotients by the spacings: the verified constant-divisor route (the
+  // forward pass's bits, IEEE division's bits)
+  auto qdx = [&](T v) { return div_c(v, dx, p.rd[0], p.fast_div & 1); };
+  auto qdz = [&](T v) { return div_c(v, dz, p.rd[1], p.fast_div & 1); };
   T c[N];
 #pragma unroll
   for (int m = 0; m < N; ++m) c[m] = p.c[m];
@@ -405,8 +421,8 @@ k2a_sv_vel_mid(const __grid_constant__ P2<T> p, const __grid_constant__ A2<T> a)
   T t0 = 0, t1 = 0, t2 = 0, t3 = 0;
   // vx at (i+1/2, j)
   if (i >= N && i < nx - N - 1 && j >= N + 1 && j < nz - N) {
-    T av = dx_fm<T, N>(sxx, idx, nz, c) / dx;
-    T bv = dz_bm<T, N>(sxz, idx, c) / dz;
+    T av = qdx(dx_fm<T, N>(sxx, idx, nz, c));
+    T bv = qdz(dz_bm<T, N>(sxz, idx, c));
     const bool P = (fx & 2) || (fz & 1);
     const T bxh = cfx[CBH * nx + i], axh = cfx[CAH * nx + i], kxh = cfx[CKH * nx + i];
     const T bz = cfz[CB * nz + j], az = cfz[CA * nz + j], kz = cfz[CK * nz + j];
@@ -419,13 +435,13 @@ k2a_sv_vel_mid(const __grid_constant__ P2<T> p, const __grid_constant__ A2<T> a)
     T ab = sb, bb = sb;
     if (P && xi >= 0) ab = pml_adj(ab, amx(p, a, 0, xi, j), bxh, axh, kxh);
     if (P && zj >= 0) bb = pml_adj(bb, amz(p, a, 0, i, zj), bz, az, kz);
-    t0 = ab / dx;
-    t1 = bb / dz;
+    t0 = qdx(ab);
+    t1 = qdz(bb);
   }
   // vz at (i, j+1/2)
   if (i >= N + 1 && i < nx - N && j >= N && j < nz - N - 1) {
-    T av = dx_bm<T, N>(sxz, idx, nz, c) / dx;
-    T bv = dz_fm<T, N>(szz, idx, c) / dz;
+    T av = qdx(dx_bm<T, N>(sxz, idx, nz, c));
+    T bv = qdz(dz_fm<T, N>(szz, idx, c));
     const bool P = (fx & 1) || (fz & 2);
     const T bx = cfx[CB * nx + i], ax = cfx[CA * nx + i], kx = cfx[CK * nx + i];
     const T bzh = cfz[CBH * nz + j], azh = cfz[CAH * nz + j], kzh = cfz[CKH * nz + j];
@@ -438,8 +454,8 @@ k2a_sv_vel_mid(const __grid_constant__ P2<T> p, const __grid_constant__ A2<T> a)
     T ab = sb, bb = sb;
     if (P && xi >= 0) ab = pml_adj(ab, amx(p, a, 1, xi, j), bx, ax, kx);
     if (P && zj >= 0) bb = pml_adj(bb, amz(p, a, 1, i, zj), bzh, azh, kzh);
-    t2 = ab / dx;
-    t3 = bb / dz;
+    t2 = qdx(ab);
+    t3 = qdz(bb);
   }
   a.tmp[0][idx] = t0;
   a.tmp[1][idx] = t1;
