@@ -19,6 +19,14 @@ namespace sw {
 
 // single-shot tile: 32 (z) x 4 (x) cells, one per thread (config 1, 400^2:
 // 13.3 Gcell/s against 12.8 with 32 x 8 on B200)
+// Resident blocks per SM the float batched kernels are compiled for: a full
+// SM (2048 threads).  Their loads of many shots' taps are latency bound, and
+// full occupancy (4x32 tiles: 16 blocks, 32 registers with a few spills)
+// measured 28.9 against 20.3 Gcell/s with the compiler's own register count
+// (50: 9 blocks) on 64 ragged shots.  The single-shot kernels keep theirs
+// (full occupancy made them slower: 12.6 against 13.3 Gcell/s at 400^2), and
+// so do the double ones.
+#define SW_BATCH_MINB (sizeof(T) == 4 ? 2048 / (BX * BZ) : 1)
 constexpr int T2Z = 32;
 constexpr int T2X = 4;
 
@@ -591,7 +599,7 @@ template cudaError_t sw2_persistent<double>(const P2<double>&, int, int, int, in
 // batched ragged shots: one launch per phase covers every tile of every shot
 // ---------------------------------------------------------------------------
 template <typename T, int N, int S, int BX, int BZ>
-__global__ void __launch_bounds__(BX * BZ) k2b_velocity(const __grid_constant__ Batch2<T> bt, int it) {
+__global__ void __launch_bounds__(BX * BZ, SW_BATCH_MINB) k2b_velocity(const __grid_constant__ Batch2<T> bt, int it) {
   const int2 wk = bt.work[blockIdx.x];
   const P2<T>& p = bt.shots[wk.x - bt.first];
   const int j = (wk.y & 0xffff) * BZ + threadIdx.x, i = (wk.y >> 16) * BX + threadIdx.y;
@@ -600,7 +608,7 @@ __global__ void __launch_bounds__(BX * BZ) k2b_velocity(const __grid_constant__ 
 }
 
 template <typename T, int N, int S, int BX, int BZ>
-__global__ void __launch_bounds__(BX * BZ) k2b_stress(const __grid_constant__ Batch2<T> bt, int it, int inject_next) {
+__global__ void __launch_bounds__(BX * BZ, SW_BATCH_MINB) k2b_stress(const __grid_constant__ Batch2<T> bt, int it, int inject_next) {
   const int2 wk = bt.work[blockIdx.x];
   const P2<T>& p = bt.shots[wk.x - bt.first];
   const int tx = wk.y >> 16, tz = wk.y & 0xffff;
