@@ -84,15 +84,28 @@ __device__ __forceinline__ T drz_bm(const T* f, long long idx, int nz, const T* 
 // a thread's loads are all in flight together; rows / columns are clamped to
 // the grid (the values of clamped taps only feed cells that are not updated).
 // taps_x: f[i0 + q, j], q = 0 .. 2N-1; taps_z: f[i, j0 + q] (row base given).
+// Taps wholly inside the grid (every cell away from the edges) skip the clamps.
 template <typename T, int N>
 __device__ __forceinline__ void taps_x(T (&t)[2 * N], const T* f, int i0, int j, int nx, int nz) {
+  if (i0 >= 0 && i0 + 2 * N <= nx) {
+    const T* b = f + (long long)i0 * nz + j;
 #pragma unroll
-  for (int q = 0; q < 2 * N; ++q) t[q] = ldg(f + (long long)min(max(i0 + q, 0), nx - 1) * nz + j);
+    for (int q = 0; q < 2 * N; ++q) t[q] = ldg(b + (long long)q * nz);
+  } else {
+#pragma unroll
+    for (int q = 0; q < 2 * N; ++q) t[q] = ldg(f + (long long)min(max(i0 + q, 0), nx - 1) * nz + j);
+  }
 }
 template <typename T, int N>
 __device__ __forceinline__ void taps_z(T (&t)[2 * N], const T* f, long long row, int j0, int nz) {
+  if (j0 >= 0 && j0 + 2 * N <= nz) {
+    const T* b = f + row + j0;
 #pragma unroll
-  for (int q = 0; q < 2 * N; ++q) t[q] = ldg(f + row + min(max(j0 + q, 0), nz - 1));
+    for (int q = 0; q < 2 * N; ++q) t[q] = ldg(b + q);
+  } else {
+#pragma unroll
+    for (int q = 0; q < 2 * N; ++q) t[q] = ldg(f + row + min(max(j0 + q, 0), nz - 1));
+  }
 }
 // sum_m c_m (t[N+m] - t[N-1-m]) from m = 0: with i0 = i - N this is the
 // backward difference at i, with i0 = i - N + 1 the forward one (the order of
