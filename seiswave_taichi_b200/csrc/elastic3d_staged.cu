@@ -6,16 +6,18 @@
 //   k3s_stress    sxx syy szz sxy sxz syz (+ receivers,  reference :245-310
 //                 + next step's moment-tensor source)
 //
-// Each CTA owns a TY x 32 (y x z) column tile and streams x planes.  One
-// elected thread issues cp.async.bulk.tensor loads of whole plane tiles (with
-// the halo each array needs) into shared-memory rings, D planes ahead,
-// completing on mbarriers; x taps come from the ring planes, y and z taps from
-// the halo.  Every thread updates Q consecutive z cells (a "quad", Q = 2 or
-// 4, moved with 8- or 16-byte shared and global accesses).  A tile plane that lies inside every update range and
-// outside every CPML slab takes a branch-free path; the others evaluate the
-// update ranges per cell and the CPML memory variables on their slabs.
-// Arithmetic follows the reference's operation order with -fmad=false, exact
-// division (div_c / div_v), so results equal the CPU oracle bit for bit.
+// Each CTA owns a TY x TZ (y x z) column tile (TZ = 32 or 40) and streams x
+// planes.  One elected thread issues cp.async.bulk.tensor loads of whole plane
+// tiles (with the halo each array needs) into shared-memory rings, D planes
+// ahead, completing on mbarriers; x taps come from the ring planes, y and z
+// taps from the halo.  Every thread updates Q consecutive z cells (a "quad",
+// Q = 2 or 4, moved with 8- or 16-byte shared and global accesses), and
+// prefetches the CPML memory variables (split fields, in the split-PML
+// scheme) of the planes ahead.  Update ranges are evaluated per cell and the
+// CPML memory variables on their slabs; exact quotients run in range-tested
+// groups.  Arithmetic follows the reference's operation order with
+// -fmad=false and exact division, so results equal the CPU oracle bit for
+// bit.
 #include <cudaTypedefs.h>
 
 #include "sw_device.cuh"
@@ -26,25 +28,17 @@ namespace sw {
 
 // SW_OWN_TMA: the plane's own cells (the fields a pass updates) arrive by
 // TMA with the neighbour planes instead of per-thread global loads.
-// SW_ONE_BARRIER: one CTA barrier per plane (the next plane's wait folded
-// into it) instead of two.
 #ifndef SW_OWN_TMA
 #define SW_OWN_TMA 0
 #endif
-#ifndef SW_ONE_BARRIER
-#define SW_ONE_BARRIER 0
-#endif
 
-// z cells per thread: 2 in exact mode, 4 in fast mode.  With two cells per
-// thread the exact velocity pass is bound to three 256-thread CTAs per SM
-// (80 registers, 16/32 bytes of spills: 24 resident warps) and the stress
-// pass to two (128 registers, no spills: 16 warps), against 12 warps for
-// four cells (three 128-thread CTAs at 160-168 registers); the extra warps
-// hide more of the exact arithmetic's dependent chains.  Measured on B200 at
-// 200^3 (exact, steps 300-500 / 600-800 us per step): 793 / 601, against
-// 835 / 626 with both passes at three CTAs, 823 / 664 with both at two,
-// 774 / 691 with one cell per thread and 1215 / 746 with four.  The fast
-// kernels, with shorter chains, keep four cells (482 us; 594 with two).
+// z cells per thread: 2 in exact mode, 4 in fast mode.  Two cells per thread
+// give the exact passes more resident warps to hide the exact arithmetic's
+// dependent chains (at 40-cell tiles: two 320-thread CTAs per SM, 96
+// registers, 20 warps); when this was chosen on 256-thread CTAs it measured,
+// on B200 at 200^3 (exact, steps 300-500 / 600-800 us per step), 793 / 601
+// against 774 / 691 with one cell per thread and 1215 / 746 with four.  The
+// fast kernels, with shorter chains, keep four cells (482 us; 594 with two).
 constexpr int staged_q(bool exact) { return exact ? 2 : 4; }
 
 // TZ: z cells of a tile, 32 or 40 (the plan takes the width that covers nz
@@ -781,18 +775,6 @@ k3s_velocity(const __grid_constant__ P3<float> p, const __grid_constant__ Staged
     if (tid == 0)
       for (int s = x0; s <= min(x0 + D, x1 - 1); ++s) issue(s, s == x0, (g + (s - x0)) % (D + 1));
 
-#if SW_ONE_BARRIER
-    // the first plane's data (bounded wait); the barrier also publishes the
-    // unit's tables
-    {
-      const bool landed = mbar_wait(&bars[g % (D + 1)], (g / (D + 1)) & 1);
-      if (__syncthreads_or(!landed)) {
-        if (tid == 0) atomicOr(a.err, 1);
-        ok = false;
-      }
-    }
-    for (int i = x0; i < x1 && ok; ++i, ++g) {
-#else
     for (int i = x0; i < x1; ++i, ++g) {
       // this plane's data (bounded wait); the CTA agrees on the outcome
       const bool landed = mbar_wait(&bars[g % (D + 1)], (g / (D + 1)) & 1);
@@ -801,7 +783,6 @@ k3s_velocity(const __grid_constant__ P3<float> p, const __grid_constant__ Staged
         ok = false;
         break;
       }
-#endif
       const int xi = SCH == SCH_CPML ? slab_index(i, nx, p.lo[0], p.hi[0]) : -1;
       if constexpr (SCH == SCH_CPML)
         if (jin && kin && i + 2 < x1) prefetch_memvars(p, i + 2, j, k, 0, yj, zk, zany);
@@ -945,20 +926,8 @@ k3s_velocity(const __grid_constant__ P3<float> p, const __grid_constant__ Staged
         stq<Q>(p.f[1] + gi, vy);
         stq<Q>(p.f[2] + gi, vz);
       }
-#if SW_ONE_BARRIER
-      // one barrier per plane: every thread is done with plane i's ring slots
-      // (which plane i+D+1 refills) and has seen plane i+1's data land
-      const bool landed = i + 1 >= x1 || mbar_wait(&bars[(g + 1) % (D + 1)], ((g + 1) / (D + 1)) & 1);
-      if (__syncthreads_or(!landed)) {
-        if (tid == 0) atomicOr(a.err, 1);
-        ok = false;
-        ++g;  // the stage that gave up; the drain at the end waits from there
-        break;
-      }
-#else
       // every thread is done with plane i's ring slots, which plane i+D+1 refills
       __syncthreads();
-#endif
       if (tid == 0 && i + D + 1 < x1) issue(i + D + 1, false, g % (D + 1));
     }
   }
@@ -1080,18 +1049,6 @@ k3s_stress(const __grid_constant__ P3<float> p, const __grid_constant__ StagedMa
     if (tid == 0)
       for (int s = x0; s <= min(x0 + D, x1 - 1); ++s) issue(s, s == x0, (g + (s - x0)) % (D + 1));
 
-#if SW_ONE_BARRIER
-    // the first plane's data (bounded wait); the barrier also publishes the
-    // unit's tables
-    {
-      const bool landed = mbar_wait(&bars[g % (D + 1)], (g / (D + 1)) & 1);
-      if (__syncthreads_or(!landed)) {
-        if (tid == 0) atomicOr(a.err, 1);
-        ok = false;
-      }
-    }
-    for (int i = x0; i < x1 && ok; ++i, ++g) {
-#else
     for (int i = x0; i < x1; ++i, ++g) {
       // this plane's data (bounded wait); the CTA agrees on the outcome
       const bool landed = mbar_wait(&bars[g % (D + 1)], (g / (D + 1)) & 1);
@@ -1100,7 +1057,6 @@ k3s_stress(const __grid_constant__ P3<float> p, const __grid_constant__ StagedMa
         ok = false;
         break;
       }
-#endif
       const int xi = SCH == SCH_CPML ? slab_index(i, nx, p.lo[0], p.hi[0]) : -1;
       if constexpr (SCH == SCH_CPML)
         if (jin && kin && i + 2 < x1) prefetch_memvars(p, i + 2, j, k, 3, yj, zk, zany);
@@ -1275,20 +1231,8 @@ k3s_stress(const __grid_constant__ P3<float> p, const __grid_constant__ StagedMa
         stq<Q>(p.f[7] + gi, sxz);
         stq<Q>(p.f[8] + gi, syz);
       }
-#if SW_ONE_BARRIER
-      // one barrier per plane: every thread is done with plane i's ring slots
-      // (which plane i+D+1 refills) and has seen plane i+1's data land
-      const bool landed = i + 1 >= x1 || mbar_wait(&bars[(g + 1) % (D + 1)], ((g + 1) / (D + 1)) & 1);
-      if (__syncthreads_or(!landed)) {
-        if (tid == 0) atomicOr(a.err, 1);
-        ok = false;
-        ++g;  // the stage that gave up; the drain at the end waits from there
-        break;
-      }
-#else
       // every thread is done with plane i's ring slots, which plane i+D+1 refills
       __syncthreads();
-#endif
       if (tid == 0 && i + D + 1 < x1) issue(i + D + 1, false, g % (D + 1));
     }
   }
