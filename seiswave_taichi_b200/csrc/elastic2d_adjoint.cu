@@ -37,6 +37,9 @@ struct A2 {
   const T* snap1;   // slot k+1
 };
 
+// Resident blocks per SM the float adjoint kernels are compiled for (a full
+// SM): one thread per cell waits on its loads, as in the batched forward.
+#define SW_ADJ_MINB (sizeof(T) == 4 ? 2048 / (A2Z * A2X) : 1)
 constexpr int A2Z = 32;
 constexpr int A2X = 8;
 
@@ -97,7 +100,7 @@ __global__ void k2a_record(const __grid_constant__ P2<T> p, const __grid_constan
 
 // ---- stress phase: mids and lam/mu gradients ---------------------------------
 template <typename T, int N>
-__global__ void __launch_bounds__(A2Z * A2X)
+__global__ void __launch_bounds__(A2Z * A2X, SW_ADJ_MINB)
 k2a_stress_mid(const __grid_constant__ P2<T> p, const __grid_constant__ A2<T> a) {
   const int j = blockIdx.x * A2Z + threadIdx.x;
   const int i = blockIdx.y * A2X + threadIdx.y;
@@ -170,7 +173,7 @@ k2a_stress_mid(const __grid_constant__ P2<T> p, const __grid_constant__ A2<T> a)
 
 // vx_bar += Dfx^T t0 + Dfz^T t2;  vz_bar += Dbz^T t1 + Dbx^T t3
 template <typename T, int N>
-__global__ void __launch_bounds__(A2Z * A2X)
+__global__ void __launch_bounds__(A2Z * A2X, SW_ADJ_MINB)
 k2a_vel_gather(const __grid_constant__ P2<T> p, const __grid_constant__ A2<T> a) {
   const int j = blockIdx.x * A2Z + threadIdx.x;
   const int i = blockIdx.y * A2X + threadIdx.y;
@@ -192,7 +195,7 @@ k2a_vel_gather(const __grid_constant__ P2<T> p, const __grid_constant__ A2<T> a)
 
 // ---- velocity phase: mids and rho gradients ---------------------------------
 template <typename T, int N>
-__global__ void __launch_bounds__(A2Z * A2X)
+__global__ void __launch_bounds__(A2Z * A2X, SW_ADJ_MINB)
 k2a_vel_mid(const __grid_constant__ P2<T> p, const __grid_constant__ A2<T> a) {
   const int j = blockIdx.x * A2Z + threadIdx.x;
   const int i = blockIdx.y * A2X + threadIdx.y;
@@ -263,7 +266,7 @@ k2a_vel_mid(const __grid_constant__ P2<T> p, const __grid_constant__ A2<T> a) {
 
 // sxx_bar += Dbx^T t0;  sxz_bar += Dbz^T t1 + Dfx^T t2;  szz_bar += Dfz^T t3
 template <typename T, int N>
-__global__ void __launch_bounds__(A2Z * A2X)
+__global__ void __launch_bounds__(A2Z * A2X, SW_ADJ_MINB)
 k2a_str_gather(const __grid_constant__ P2<T> p, const __grid_constant__ A2<T> a) {
   const int j = blockIdx.x * A2Z + threadIdx.x;
   const int i = blockIdx.y * A2X + threadIdx.y;
@@ -298,7 +301,7 @@ k2a_str_gather(const __grid_constant__ P2<T> p, const __grid_constant__ A2<T> a)
 // G_vx (rho2), G_vz (rhoz), G_lpm, G_lm, G_m4.
 // ============================================================================
 template <typename T, int N>
-__global__ void __launch_bounds__(A2Z * A2X)
+__global__ void __launch_bounds__(A2Z * A2X, SW_ADJ_MINB)
 k2a_sv_stress_mid(const __grid_constant__ P2<T> p, const __grid_constant__ A2<T> a) {
   const int j = blockIdx.x * A2Z + threadIdx.x;
   const int i = blockIdx.y * A2X + threadIdx.y;
@@ -372,7 +375,7 @@ k2a_sv_stress_mid(const __grid_constant__ P2<T> p, const __grid_constant__ A2<T>
 
 // vx_bar += Dbx^T t0 + Dfz^T t2;  vz_bar += Dbz^T t1 + Dfx^T t3
 template <typename T, int N>
-__global__ void __launch_bounds__(A2Z * A2X)
+__global__ void __launch_bounds__(A2Z * A2X, SW_ADJ_MINB)
 k2a_sv_vel_gather(const __grid_constant__ P2<T> p, const __grid_constant__ A2<T> a) {
   const int j = blockIdx.x * A2Z + threadIdx.x;
   const int i = blockIdx.y * A2X + threadIdx.y;
@@ -393,7 +396,7 @@ k2a_sv_vel_gather(const __grid_constant__ P2<T> p, const __grid_constant__ A2<T>
 }
 
 template <typename T, int N>
-__global__ void __launch_bounds__(A2Z * A2X)
+__global__ void __launch_bounds__(A2Z * A2X, SW_ADJ_MINB)
 k2a_sv_vel_mid(const __grid_constant__ P2<T> p, const __grid_constant__ A2<T> a) {
   const int j = blockIdx.x * A2Z + threadIdx.x;
   const int i = blockIdx.y * A2X + threadIdx.y;
@@ -465,7 +468,7 @@ k2a_sv_vel_mid(const __grid_constant__ P2<T> p, const __grid_constant__ A2<T> a)
 
 // sxx_bar += Dfx^T t0;  sxz_bar += Dbz^T t1 + Dbx^T t2;  szz_bar += Dfz^T t3
 template <typename T, int N>
-__global__ void __launch_bounds__(A2Z * A2X)
+__global__ void __launch_bounds__(A2Z * A2X, SW_ADJ_MINB)
 k2a_sv_str_gather(const __grid_constant__ P2<T> p, const __grid_constant__ A2<T> a) {
   const int j = blockIdx.x * A2Z + threadIdx.x;
   const int i = blockIdx.y * A2X + threadIdx.y;
