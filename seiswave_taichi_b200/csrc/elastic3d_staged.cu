@@ -123,47 +123,6 @@ template <int Q>
 __device__ __forceinline__ Vq<Q> ldgq(const float* p) {
   return __ldg(reinterpret_cast<const Vq<Q>*>(p));
 }
-// Exact mode with two z cells per thread computes on cell pairs with the
-// packed two-lane FP32 instructions of sm_100 (add/mul/fma .rn.f32x2): each
-// lane is one IEEE round-to-nearest operation, the same bits as the scalar
-// instruction, at half the instruction count.  They are written as inline
-// PTX with the explicit .rn modifier, which the optimizer never contracts
-// (a multiply and an add fused into one fma would round once instead of
-// twice and leave the reference's operation order).
-#ifndef SW_STAGED_PACKED
-#define SW_STAGED_PACKED 0
-#endif
-template <bool EX, int Q>
-constexpr bool packed() { return SW_STAGED_PACKED && EX && Q == 2; }
-__device__ __forceinline__ float2 sp2(float c) { return make_float2(c, c); }
-__device__ __forceinline__ float2 add2(float2 a, float2 b) {
-  float2 d;
-  asm("{\n .reg .b64 ra, rb, rd;\n mov.b64 ra, {%2, %3};\n mov.b64 rb, {%4, %5};\n"
-      " add.rn.f32x2 rd, ra, rb;\n mov.b64 {%0, %1}, rd;\n}"
-      : "=f"(d.x), "=f"(d.y)
-      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
-  return d;
-}
-__device__ __forceinline__ float2 mul2(float2 a, float2 b) {
-  float2 d;
-  asm("{\n .reg .b64 ra, rb, rd;\n mov.b64 ra, {%2, %3};\n mov.b64 rb, {%4, %5};\n"
-      " mul.rn.f32x2 rd, ra, rb;\n mov.b64 {%0, %1}, rd;\n}"
-      : "=f"(d.x), "=f"(d.y)
-      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
-  return d;
-}
-// a * b + c with one rounding
-__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
-  float2 d;
-  asm("{\n .reg .b64 ra, rb, rc, rd;\n mov.b64 ra, {%2, %3};\n mov.b64 rb, {%4, %5};\n"
-      " mov.b64 rc, {%6, %7};\n fma.rn.f32x2 rd, ra, rb, rc;\n mov.b64 {%0, %1}, rd;\n}"
-      : "=f"(d.x), "=f"(d.y)
-      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
-  return d;
-}
-// a - b with one rounding: fma(b, -1, a)
-__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return fma2(b, sp2(-1.f), a); }
-
 __device__ __forceinline__ float g4(const float4& v, int e) { return e == 0 ? v.x : e == 1 ? v.y : e == 2 ? v.z : v.w; }
 __device__ __forceinline__ void s4(float4& v, int e, float x) {
   if (e == 0) v.x = x; else if (e == 1) v.y = x; else if (e == 2) v.z = x; else v.w = x;
@@ -181,13 +140,9 @@ __device__ __forceinline__ int rslot(int plane, int R) { return (int)((unsigned)
 // mode), or acc = fma(c, a - b, acc) with the spacing folded into c (fast mode)
 template <bool EX, int Q>
 __device__ __forceinline__ void tapq(Vq<Q>& acc, float c, const Vq<Q>& a, const Vq<Q>& b) {
-  if constexpr (packed<EX, Q>()) {
-    acc = add2(acc, mul2(sp2(c), sub2(a, b)));
-  } else {
 #pragma unroll
-    for (int e = 0; e < Q; ++e)
-      s4(acc, e, EX ? g4(acc, e) + c * (g4(a, e) - g4(b, e)) : __fmaf_rn(c, g4(a, e) - g4(b, e), g4(acc, e)));
-  }
+  for (int e = 0; e < Q; ++e)
+    s4(acc, e, EX ? g4(acc, e) + c * (g4(a, e) - g4(b, e)) : __fmaf_rn(c, g4(a, e) - g4(b, e), g4(acc, e)));
 }
 
 // derivative across ring planes: pl[q] is the plane (centre - N + q + FWD)
@@ -271,22 +226,10 @@ __device__ __forceinline__ void div_group(Vq<Q> (&v)[K], const float (&d)[K], co
 #pragma unroll
     for (int e = 0; e < Q; ++e) acc.add(g4(v[k], e));
   if (fast != 0 && acc.ok()) {
-    if constexpr (packed<true, Q>()) {
-      // Markstein's correction on pairs; a zero numerator gives +0 like
-      // mk_div (a stencil sum, which starts from +0 + c*(a-b), is never -0)
 #pragma unroll
-      for (int k = 0; k < K; ++k) {
-        const float2 rr = sp2(r[k]);
-        const float2 q = mul2(v[k], rr);
-        const float2 e = fma2(q, sp2(-d[k]), v[k]);
-        v[k] = fma2(e, rr, q);
-      }
-    } else {
+    for (int k = 0; k < K; ++k)
 #pragma unroll
-      for (int k = 0; k < K; ++k)
-#pragma unroll
-        for (int e = 0; e < Q; ++e) s4(v[k], e, mk_div(g4(v[k], e), d[k], r[k]));
-    }
+      for (int e = 0; e < Q; ++e) s4(v[k], e, mk_div(g4(v[k], e), d[k], r[k]));
   } else if (fast != 0 && acc.below_huge()) {
 #pragma unroll
     for (int k = 0; k < K; ++k)
@@ -879,28 +822,17 @@ k3s_velocity(const __grid_constant__ P3<float> p, const __grid_constant__ Staged
           // numerators and densities of the 3Q updates, then their quotients
           // as one group (no per-lane range branch); masked cells keep their value
           float tn[3 * Q], td[3 * Q];
-          if constexpr (packed<EX, Q>()) {
-            const float2 dt2 = sp2(dt), rcn = add2(rc, rn);
-            const float2 n0 = mul2(add2(add2(a1, a3), a2), dt2);
-            const float2 n1 = mul2(add2(add2(b1, b2), b3), dt2);
-            const float2 n2 = mul2(TENSOR ? add2(add2(c1, c2), c3) : add2(add2(c3, c1), c2), dt2);
-            const float2 d1 = mul2(sp2(0.5f), rcn);
-            const float2 d2 = mul2(sp2(0.25f), add2(add2(rcn, r1n), r1c));
-            tn[0] = n0.x; tn[1] = n0.y; tn[2] = n1.x; tn[3] = n1.y; tn[4] = n2.x; tn[5] = n2.y;
-            td[0] = rc.x; td[1] = rc.y; td[2] = d1.x; td[3] = d1.y; td[4] = d2.x; td[5] = d2.y;
-          } else {
 #pragma unroll
-            for (int e = 0; e < Q; ++e) {
-              const float rce = g4(rc, e), rne = g4(rn, e);
-              tn[e] = (g4(a1, e) + g4(a3, e) + g4(a2, e)) * dt;
-              td[e] = rce;
-              tn[Q + e] = (g4(b1, e) + g4(b2, e) + g4(b3, e)) * dt;
-              td[Q + e] = 0.5f * (rce + rne);
-              const float sum =
-                  TENSOR ? (g4(c1, e) + g4(c2, e) + g4(c3, e)) : (g4(c3, e) + g4(c1, e) + g4(c2, e));
-              tn[2 * Q + e] = sum * dt;
-              td[2 * Q + e] = 0.25f * (rce + rne + g4(r1n, e) + g4(r1c, e));
-            }
+          for (int e = 0; e < Q; ++e) {
+            const float rce = g4(rc, e), rne = g4(rn, e);
+            tn[e] = (g4(a1, e) + g4(a3, e) + g4(a2, e)) * dt;
+            td[e] = rce;
+            tn[Q + e] = (g4(b1, e) + g4(b2, e) + g4(b3, e)) * dt;
+            td[Q + e] = 0.5f * (rce + rne);
+            const float sum =
+                TENSOR ? (g4(c1, e) + g4(c2, e) + g4(c3, e)) : (g4(c3, e) + g4(c1, e) + g4(c2, e));
+            tn[2 * Q + e] = sum * dt;
+            td[2 * Q + e] = 0.25f * (rce + rne + g4(r1n, e) + g4(r1c, e));
           }
           if (EX) {
             dv_group<3 * Q>(tn, td);
@@ -1160,57 +1092,29 @@ k3s_stress(const __grid_constant__ P3<float> p, const __grid_constant__ StagedMa
             cpml_z<EX, true, Q, G::TZ>(h2, m2, mc, zk, mxz, tzt, Q * cq);     // dvx_dz
             cpml_z<EX, true, Q, G::TZ>(q2, m2, 2 * mc, zk, myz, tzt, Q * cq); // dvy_dz
           }
-          if constexpr (packed<EX, Q>()) {
-            const float2 dt2 = sp2(dt), half = sp2(0.5f), quarter = sp2(0.25f);
-            const float2 lhx = mul2(half, add2(l0, l1));
-            const float2 mhx = mul2(half, add2(u0, u1));
-            const float2 lpm = add2(lhx, mul2(sp2(2.0f), mhx));
-            const float2 nxx = add2(sxx, mul2(add2(mul2(lpm, e1), mul2(lhx, add2(e3, e2))), dt2));
-            const float2 nyy = add2(syy, mul2(add2(mul2(lpm, e2), mul2(lhx, add2(e1, e3))), dt2));
-            const float2 nzz = add2(szz, mul2(add2(mul2(lpm, e3), mul2(lhx, add2(e1, e2))), dt2));
-            const float2 uu = add2(unj, u0);
-            const float2 mxy4 = mul2(quarter, add2(add2(uu, u0), u1));
-            const float2 nxy = add2(sxy, mul2(mul2(mxy4, add2(f2, f1)), dt2));
-            const float2 mxz4 = mul2(quarter, add2(add2(add2(u0, u1), u0), unj));
-            const float2 nxz = add2(sxz, mul2(mul2(mxz4, add2(h2, h1)), dt2));
-            const float2 myz4 = mul2(quarter, add2(add2(uu, make_float2(unk[0], unk[1])), u0));
-            const float2 nyz = add2(syz, mul2(mul2(myz4, add2(q1, q2)), dt2));
 #pragma unroll
-            for (int e = 0; e < Q; ++e) {
-              if (mn[e]) {
-                s4(sxx, e, g4(nxx, e));
-                s4(syy, e, g4(nyy, e));
-                s4(szz, e, g4(nzz, e));
-              }
-              if (mxy[e]) s4(sxy, e, g4(nxy, e));
-              if (mxz[e]) s4(sxz, e, g4(nxz, e));
-              if (myz[e]) s4(syz, e, g4(nyz, e));
+          for (int e = 0; e < Q; ++e) {
+            const float u = g4(u0, e);
+            if (mn[e]) {
+              const float lhx = 0.5f * (g4(l0, e) + g4(l1, e));
+              const float mhx = 0.5f * (u + g4(u1, e));
+              const float lpm = lhx + 2.0f * mhx;
+              const float A = g4(e1, e), B = g4(e2, e), Cc = g4(e3, e);
+              s4(sxx, e, g4(sxx, e) + (lpm * A + lhx * (Cc + B)) * dt);
+              s4(syy, e, g4(syy, e) + (lpm * B + lhx * (A + Cc)) * dt);
+              s4(szz, e, g4(szz, e) + (lpm * Cc + lhx * (A + B)) * dt);
             }
-          } else {
-#pragma unroll
-            for (int e = 0; e < Q; ++e) {
-              const float u = g4(u0, e);
-              if (mn[e]) {
-                const float lhx = 0.5f * (g4(l0, e) + g4(l1, e));
-                const float mhx = 0.5f * (u + g4(u1, e));
-                const float lpm = lhx + 2.0f * mhx;
-                const float A = g4(e1, e), B = g4(e2, e), Cc = g4(e3, e);
-                s4(sxx, e, g4(sxx, e) + (lpm * A + lhx * (Cc + B)) * dt);
-                s4(syy, e, g4(syy, e) + (lpm * B + lhx * (A + Cc)) * dt);
-                s4(szz, e, g4(szz, e) + (lpm * Cc + lhx * (A + B)) * dt);
-              }
-              if (mxy[e]) {
-                const float m4 = 0.25f * (g4(unj, e) + u + u + g4(u1, e));
-                s4(sxy, e, g4(sxy, e) + m4 * (g4(f2, e) + g4(f1, e)) * dt);
-              }
-              if (mxz[e]) {
-                const float m4 = 0.25f * (u + g4(u1, e) + u + g4(unj, e));
-                s4(sxz, e, g4(sxz, e) + m4 * (g4(h2, e) + g4(h1, e)) * dt);
-              }
-              if (myz[e]) {
-                const float m4 = 0.25f * (g4(unj, e) + u + unk[e] + u);
-                s4(syz, e, g4(syz, e) + m4 * (g4(q1, e) + g4(q2, e)) * dt);
-              }
+            if (mxy[e]) {
+              const float m4 = 0.25f * (g4(unj, e) + u + u + g4(u1, e));
+              s4(sxy, e, g4(sxy, e) + m4 * (g4(f2, e) + g4(f1, e)) * dt);
+            }
+            if (mxz[e]) {
+              const float m4 = 0.25f * (u + g4(u1, e) + u + g4(unj, e));
+              s4(sxz, e, g4(sxz, e) + m4 * (g4(h2, e) + g4(h1, e)) * dt);
+            }
+            if (myz[e]) {
+              const float m4 = 0.25f * (g4(unj, e) + u + unk[e] + u);
+              s4(syz, e, g4(syz, e) + m4 * (g4(q1, e) + g4(q2, e)) * dt);
             }
           }
         }
